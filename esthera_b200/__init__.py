@@ -1,0 +1,413 @@
+"""esthera_b200 -- B200-native particle-filter engine (Python mirror of the C ABI).
+
+The compute path is the CUDA library ``libesthera_b200.so`` built in-tree by
+``esthera_b200.build``; this module only binds it with ctypes.  There is no
+CPU fallback: importing works without a GPU, but every call that needs one
+raises ``PFError`` carrying the library's status and message.
+
+The Python surface mirrors the reference's driver and model hooks
+(src/partfilt/cuda/pf_generic_soa.cu:686 ``particle_filter``; model hooks in
+src/models/robotarm/cuda/pf_model_soa.cuh) -- see ``ParticleFilter`` and
+``particle_filter``.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libesthera_b200.so"
+
+# enums (include/esthera_b200.h)
+PF_OK, PF_ERR_INVALID, PF_ERR_CUDA, PF_ERR_NOMEM, PF_ERR_UNSUPPORTED, PF_ERR_IO = 0, 1, 2, 3, 4, 5
+PF_ERR_ADMISSION, PF_ERR_TIMEOUT, PF_ERR_NOT_FOUND, PF_ERR_BUSY = 6, 7, 8, 9
+MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM = 0, 1, 2
+EXCHANGE_NONE, EXCHANGE_RING, EXCHANGE_TORUS, EXCHANGE_ALL2ALL = 0, 1, 2, 3
+RESAMPLE_REFERENCE, RESAMPLE_SYSTEMATIC, RESAMPLE_VOSE = 0, 1, 2
+RNG_SUBFILTER, RNG_REFLAYOUT = 0, 1
+PIPELINE_FUSED, PIPELINE_PHASED = 0, 1
+MTGP_MASK_PARAMS, MTGP_MASK_CUDA_REF = 0, 0xFF800000
+MAX_STATE, MAX_CONTROL, MAX_MEAS = 16, 8, 16
+
+
+class PFConfig(C.Structure):
+    _fields_ = [("particles_per_subfilter", C.c_int32), ("num_subfilters", C.c_int32),
+                ("num_transfer", C.c_int32), ("exchange", C.c_int32), ("resampler", C.c_int32),
+                ("resampling_freq", C.c_float), ("seed", C.c_uint32), ("rng", C.c_int32),
+                ("mtgp_streams", C.c_int32), ("mtgp_mask", C.c_uint32), ("log_weights", C.c_int32),
+                ("pipeline", C.c_int32), ("particles_per_thread", C.c_int32), ("device", C.c_int32)]
+
+
+class StepInput(C.Structure):
+    _fields_ = [("dt", C.c_float), ("control", C.c_float * MAX_CONTROL), ("meas", C.c_float * MAX_MEAS),
+                ("pad", C.c_float * 7)]
+
+
+class Estimate(C.Structure):
+    _fields_ = [("mean", C.c_double * MAX_STATE), ("log_norm", C.c_double), ("best", C.c_float * MAX_STATE),
+                ("best_key", C.c_float), ("best_subfilter", C.c_int32), ("step", C.c_int32),
+                ("flags", C.c_int32)]
+
+
+class UnicycleParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("sigma_q", C.c_float * 3), ("sigma_range", C.c_float),
+                ("sigma_bearing", C.c_float), ("num_landmarks", C.c_int32), ("landmarks", (C.c_float * 2) * 8),
+                ("init_state", C.c_float * 3)]
+
+
+class DhArmParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("sigma_qd", C.c_float), ("sigma_pos", C.c_float), ("sigma_ang", C.c_float),
+                ("a", C.c_float * 6), ("alpha", C.c_float * 6), ("d", C.c_float * 6), ("init_state", C.c_float * 12)]
+
+
+class RefArmParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("init_state", C.c_float * 9)]
+
+
+STEP_INPUT_DTYPE = np.dtype([("dt", np.float32), ("control", np.float32, MAX_CONTROL),
+                             ("meas", np.float32, MAX_MEAS), ("pad", np.float32, 7)])
+ESTIMATE_DTYPE = np.dtype([("mean", np.float64, MAX_STATE), ("log_norm", np.float64),
+                           ("best", np.float32, MAX_STATE), ("best_key", np.float32),
+                           ("best_subfilter", np.int32), ("step", np.int32), ("flags", np.int32)])
+assert STEP_INPUT_DTYPE.itemsize == C.sizeof(StepInput) == 128
+assert ESTIMATE_DTYPE.itemsize == C.sizeof(Estimate)
+
+PARAMS_TYPE = {MODEL_UNICYCLE: UnicycleParams, MODEL_DHARM: DhArmParams, MODEL_REFARM: RefArmParams}
+
+
+class PFError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (status_string(status), msg))
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError("libesthera_b200.so not built; run `python -m esthera_b200.build`")
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    P = C.c_void_p
+    fp, ip, up = C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_uint32)
+    sig = {
+        "pf_status_string": (C.c_char_p, [C.c_int]),
+        "pf_last_error": (C.c_char_p, []),
+        "pf_version": (C.c_int32, []),
+        "pf_device_count": (C.c_int32, []),
+        "pf_model_info": (C.c_int, [C.c_int, ip, ip, ip, ip]),
+        "pf_config_default": (C.c_int, [C.POINTER(PFConfig)]),
+        "pf_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, P, C.c_size_t, C.POINTER(P)]),
+        "pf_destroy": (C.c_int, [P]),
+        "pf_set_initial_state": (C.c_int, [P, fp]),
+        "pf_set_particles": (C.c_int, [P, fp]),
+        "pf_get_particles": (C.c_int, [P, fp]),
+        "pf_get_sorted": (C.c_int, [P, fp, fp]),
+        "pf_get_selection": (C.c_int, [P, ip]),
+        "pf_record_selection": (C.c_int, [P, C.c_int32]),
+        "pf_step": (C.c_int, [P, C.POINTER(StepInput), C.POINTER(Estimate)]),
+        "pf_run_device": (C.c_int, [P, P, C.c_int32, P]),
+        "pf_run_device_continue": (C.c_int, [P, C.c_int32]),
+        "pf_synchronize": (C.c_int, [P]),
+        "pf_stream": (P, [P]),
+        "pf_set_timing": (C.c_int, [P, C.c_int32]),
+        "pf_last_step_timing": (C.c_int, [P, fp, C.c_int32, ip]),
+        "pf_phase_name": (C.c_char_p, [P, C.c_int32]),
+        "pf_get_info": (C.c_int, [P, ip, ip, ip, C.POINTER(C.c_int64)]),
+        "pf_snapshot_size": (C.c_int64, [P]),
+        "pf_snapshot": (C.c_int, [P, P]),
+        "pf_restore": (C.c_int, [P, P]),
+        "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
+        "pfk_boxmuller": (C.c_int, [fp, C.c_int64]),
+        "pfk_bitonic_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32]),
+        "pfk_resample": (C.c_int, [C.c_int32, fp, fp, C.c_int32, C.c_int32, C.c_int32, ip]),
+        "pfk_vose_build": (C.c_int, [fp, C.c_int32, C.c_int32, C.c_int32, fp, up]),
+        "pfk_exchange_sources": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, ip]),
+        "pfk_model_step": (C.c_int, [C.c_int, P, C.c_size_t, C.POINTER(StepInput), C.c_int32, fp, fp, fp]),
+        "pf_unicycle_default_params": (C.c_int, [C.c_uint32, C.c_int32, C.POINTER(UnicycleParams)]),
+        "pf_dharm_default_params": (C.c_int, [C.c_uint32, C.POINTER(DhArmParams)]),
+        "pf_make_trace": (C.c_int, [C.c_int, P, C.c_uint32, C.c_int32, P, fp]),
+        "pf_read_trace_line": (C.c_int, [P, C.c_int, C.POINTER(StepInput), fp]),
+        "pf_refarm_estimate_error": (C.c_float, [fp, fp]),
+        "pf_particle_filter": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_char_p, fp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def status_string(s):
+    try:
+        return lib().pf_status_string(s).decode()
+    except Exception:  # library missing: still format the error
+        return "status %d" % s
+
+
+def check(status):
+    if status != PF_OK:
+        raise PFError(status, lib().pf_last_error().decode())
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _uptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def device_count():
+    return int(lib().pf_device_count())
+
+
+def model_info(model):
+    v = [C.c_int32() for _ in range(4)]
+    check(lib().pf_model_info(model, *[C.byref(x) for x in v]))
+    return tuple(x.value for x in v)  # num_state, num_noise, num_control, num_meas
+
+
+def default_config(**kw):
+    c = PFConfig()
+    check(lib().pf_config_default(C.byref(c)))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise AttributeError("pf_config has no field %r" % k)
+        setattr(c, k, v)
+    return c
+
+
+# ---- synthetic traces --------------------------------------------------------
+def unicycle_params(seed, num_landmarks=4):
+    p = UnicycleParams()
+    check(lib().pf_unicycle_default_params(seed, num_landmarks, C.byref(p)))
+    return p
+
+
+def dharm_params(seed):
+    p = DhArmParams()
+    check(lib().pf_dharm_default_params(seed, C.byref(p)))
+    return p
+
+
+def refarm_params(dt=1.0):
+    p = RefArmParams()
+    p.dt = dt
+    for i in range(5):
+        p.init_state[i] = 0.75 * np.pi
+    p.init_state[5] = 7.0
+    return p
+
+
+def make_trace(model, params, seed, steps):
+    """(inputs: structured array of STEP_INPUT_DTYPE, truth: steps x num_state float32)."""
+    S = model_info(model)[0]
+    inputs = np.zeros(steps, dtype=STEP_INPUT_DTYPE)
+    truth = np.zeros((steps, S), dtype=np.float32)
+    check(lib().pf_make_trace(model, C.byref(params), seed, steps, inputs.ctypes.data_as(C.c_void_p),
+                              _fptr(truth)))
+    return inputs, truth
+
+
+def step_input(rec):
+    """A StepInput from one STEP_INPUT_DTYPE record."""
+    s = StepInput()
+    C.memmove(C.byref(s), np.ascontiguousarray(rec).ctypes.data, 128)
+    return s
+
+
+def estimate_to_numpy(e):
+    a = np.zeros(1, dtype=ESTIMATE_DTYPE)
+    C.memmove(a.ctypes.data, C.byref(e), ESTIMATE_DTYPE.itemsize)
+    return a[0]
+
+
+# ---- filter ----------------------------------------------------------------------
+class ParticleFilter:
+    """One distributed particle filter on one GPU (wraps pf_create / pf_step)."""
+
+    def __init__(self, model, params, config=None, **cfg):
+        self.model = model
+        self.params = params
+        self.config = config if config is not None else default_config(**cfg)
+        self.num_state, self.num_noise, _, _ = model_info(model)
+        h = C.c_void_p()
+        check(lib().pf_create(C.byref(self.config), model, C.byref(params), C.sizeof(params), C.byref(h)))
+        self._h = h
+        self.m = self.config.particles_per_subfilter
+        self.N = self.config.num_subfilters
+        self.T = self.m * self.N
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        e, dx, dy, b = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib().pf_get_info(self._h, C.byref(e), C.byref(dx), C.byref(dy), C.byref(b)))
+        return {"particles_per_thread": e.value, "torus": (dx.value, dy.value), "device_bytes": b.value}
+
+    def set_initial_state(self, state):
+        check(lib().pf_set_initial_state(self._h, _fptr(_f32(state))))
+
+    def set_particles(self, soa):
+        a = _f32(soa).reshape(self.num_state, self.T)
+        check(lib().pf_set_particles(self._h, _fptr(a)))
+
+    def particles(self):
+        a = np.zeros((self.num_state, self.T), np.float32)
+        check(lib().pf_get_particles(self._h, _fptr(a)))
+        return a
+
+    def sorted(self):
+        s = np.zeros((self.num_state, self.T), np.float32)
+        k = np.zeros(self.T, np.float32)
+        check(lib().pf_get_sorted(self._h, _fptr(s), _fptr(k)))
+        return s, k
+
+    def record_selection(self, on=True):
+        check(lib().pf_record_selection(self._h, 1 if on else 0))
+
+    def selection(self):
+        a = np.zeros(self.T, np.int32)
+        check(lib().pf_get_selection(self._h, _iptr(a)))
+        return a
+
+    def step(self, inp):
+        """One filter step; inp is a STEP_INPUT_DTYPE record or a StepInput."""
+        s = inp if isinstance(inp, StepInput) else step_input(inp)
+        e = Estimate()
+        check(lib().pf_step(self._h, C.byref(s), C.byref(e)))
+        return estimate_to_numpy(e)
+
+    def run_device(self, d_inputs_ptr, steps, d_estimates_ptr):
+        check(lib().pf_run_device(self._h, C.c_void_p(d_inputs_ptr), steps, C.c_void_p(d_estimates_ptr)))
+
+    def run_continue(self, steps):
+        check(lib().pf_run_device_continue(self._h, steps))
+
+    def synchronize(self):
+        check(lib().pf_synchronize(self._h))
+
+    def stream(self):
+        return lib().pf_stream(self._h)
+
+    def set_timing(self, on=True):
+        check(lib().pf_set_timing(self._h, 1 if on else 0))
+
+    def last_step_timing(self):
+        """[(phase name, ms)] of the launches of the last step (timing must be on)."""
+        ms = np.zeros(8, np.float32)
+        n = C.c_int32()
+        check(lib().pf_last_step_timing(self._h, _fptr(ms), 8, C.byref(n)))
+        return [(lib().pf_phase_name(self._h, i).decode(), float(ms[i])) for i in range(n.value)]
+
+    def snapshot(self):
+        n = lib().pf_snapshot_size(self._h)
+        buf = np.zeros(n, np.uint8)
+        check(lib().pf_snapshot(self._h, buf.ctypes.data_as(C.c_void_p)))
+        return buf
+
+    def restore(self, buf):
+        b = np.ascontiguousarray(buf, np.uint8)
+        check(lib().pf_restore(self._h, b.ctypes.data_as(C.c_void_p)))
+
+
+def particle_filter(num_particles, num_blocks, num_transfer, resampling_freq, input_file):
+    """Drop-in for the reference driver call (pf_generic_soa.cu:686): robot-arm
+    model over a reference trace file; returns the mean estimate error."""
+    e = C.c_float()
+    check(lib().pf_particle_filter(num_particles, num_blocks, num_transfer, resampling_freq,
+                                   str(input_file).encode(), C.byref(e)))
+    return e.value
+
+
+# ---- kernel-level entry points (parity tests) --------------------------------------
+def mtgp_generate(G, seed, per_stream, kind=1, mask=MTGP_MASK_PARAMS, calls=1):
+    out = np.zeros(calls * G * per_stream, np.uint32)
+    check(lib().pfk_mtgp_generate(G, seed, mask, kind, per_stream, calls, _uptr(out)))
+    return out
+
+
+def boxmuller(data, n=None):
+    n = len(data) if n is None else n
+    a = np.array(data, dtype=np.float32, copy=True)
+    if len(a) < 2 * ((n + 1) // 2):
+        a = np.concatenate([a, np.zeros(2 * ((n + 1) // 2) - len(a), np.float32)])
+    check(lib().pfk_boxmuller(_fptr(a), n))
+    return a
+
+
+def bitonic_sort(keys, m, ppt=0):
+    k = np.array(keys, dtype=np.float32, copy=True)
+    idx = np.zeros(len(k), np.int32)
+    check(lib().pfk_bitonic_sort(_fptr(k), _iptr(idx), m, len(k) // m, ppt))
+    return k, idx
+
+
+def resample(resampler, w, u, m, ppt=0):
+    w = _f32(w)
+    u = _f32(u)
+    sel = np.zeros(len(w), np.int32)
+    check(lib().pfk_resample(resampler, _fptr(w), _fptr(u), m, len(w) // m, ppt, _iptr(sel)))
+    return sel
+
+
+def vose_build(w, m, ppt=0):
+    w = _f32(w)
+    prob = np.zeros(len(w), np.float32)
+    alias = np.zeros(len(w), np.uint32)
+    check(lib().pfk_vose_build(_fptr(w), m, len(w) // m, ppt, _fptr(prob), _uptr(alias)))
+    return prob, alias
+
+
+def exchange_sources(mode, N, m, t, sorted_keys=None):
+    src = np.zeros(N * m, np.int32)
+    k = None if sorted_keys is None else _f32(sorted_keys)
+    check(lib().pfk_exchange_sources(mode, N, m, t, None if k is None else _fptr(k), _iptr(src)))
+    return src
+
+
+def model_step(model, params, inp, state, noise):
+    st = np.array(state, dtype=np.float32, copy=True)
+    nz = _f32(noise)
+    n = st.shape[1]
+    ll = np.zeros(n, np.float32)
+    s = inp if isinstance(inp, StepInput) else step_input(inp)
+    check(lib().pfk_model_step(model, C.byref(params), C.sizeof(params), C.byref(s), n, _fptr(st), _fptr(nz),
+                               _fptr(ll)))
+    return st, ll

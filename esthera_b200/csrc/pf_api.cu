@@ -1,0 +1,946 @@
+// pf_api.cu -- the C ABI (include/esthera_b200.h): filter lifecycle, device
+// memory, the per-step launch sequence, CUDA-graph replay, snapshot/restore
+// and the kernel-level entry points used by the parity tests.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "pf_launch.cuh"
+
+using namespace pfdev;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static pf_status fail(pf_status s, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define CU(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? PF_ERR_NOMEM : PF_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+
+extern "C" const char* pf_last_error(void) { return g_err.c_str(); }
+
+extern "C" const char* pf_status_string(pf_status s)
+{
+    switch (s) {
+    case PF_OK: return "ok";
+    case PF_ERR_INVALID: return "invalid argument";
+    case PF_ERR_CUDA: return "CUDA error";
+    case PF_ERR_NOMEM: return "out of memory";
+    case PF_ERR_UNSUPPORTED: return "unsupported configuration";
+    case PF_ERR_IO: return "I/O error";
+    case PF_ERR_ADMISSION: return "admission rejected";
+    case PF_ERR_TIMEOUT: return "timeout";
+    case PF_ERR_NOT_FOUND: return "not found";
+    case PF_ERR_BUSY: return "busy";
+    }
+    return "unknown";
+}
+
+extern "C" int32_t pf_version(void) { return 100; }
+
+extern "C" int32_t pf_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+static pf_status require_gpu(int device)
+{
+    const int n = pf_device_count();
+    if (n <= 0) return fail(PF_ERR_CUDA, "no CUDA device available (this engine has no CPU path)");
+    if (device < 0 || device >= n) return fail(PF_ERR_INVALID, "device %d out of range (%d devices)", device, n);
+    CU(cudaSetDevice(device));
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// model table
+// ---------------------------------------------------------------------------
+struct ModelInfo {
+    int S, K, C, Z;
+    size_t psize;
+};
+
+static bool model_info(int model, ModelInfo* mi)
+{
+    switch (model) {
+    case PF_MODEL_UNICYCLE: *mi = {Unicycle::S, Unicycle::K, 2, 16, sizeof(pf_unicycle_params)}; return true;
+    case PF_MODEL_DHARM: *mi = {DhArm::S, DhArm::K, 0, 6, sizeof(pf_dharm_params)}; return true;
+    case PF_MODEL_REFARM: *mi = {RefArm::S, RefArm::K, 5, 7, sizeof(pf_refarm_params)}; return true;
+    }
+    return false;
+}
+
+extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, int32_t* C, int32_t* Z)
+{
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    if (S) *S = mi.S;
+    if (K) *K = mi.K;
+    if (C) *C = mi.C;
+    if (Z) *Z = mi.Z;
+    return PF_OK;
+}
+
+static const float* init_state_of(int model, const ModelParams& mp)
+{
+    switch (model) {
+    case PF_MODEL_UNICYCLE: return mp.uni.init_state;
+    case PF_MODEL_DHARM: return mp.arm.init_state;
+    default: return mp.ref.init_state;
+    }
+}
+
+// Launch dispatch over the model template.
+struct ModelOps {
+    cudaError_t (*sample_sort)(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
+    cudaError_t (*sample_weight)(int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
+    cudaError_t (*block_sort)(int, int, int, cudaStream_t, const FilterDesc*, const int2*);
+    cudaError_t (*exchange_resample)(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, int32_t*,
+                                     int);
+    cudaError_t (*exchange_inplace)(int, int, cudaStream_t, const FilterDesc*, const int2*);
+    cudaError_t (*estimate)(int, cudaStream_t, const FilterDesc*, InputRef);
+    cudaError_t (*test_model)(const ModelParams&, const pf_step_input*, int, float*, const float*, float*,
+                              cudaStream_t);
+};
+
+template <class Mdl>
+static ModelOps ops_of()
+{
+    return {Launch<Mdl>::sample_sort,       Launch<Mdl>::sample_weight,    Launch<Mdl>::block_sort,
+            Launch<Mdl>::exchange_resample, Launch<Mdl>::exchange_inplace, Launch<Mdl>::estimate,
+            Launch<Mdl>::test_model};
+}
+
+static ModelOps model_ops(int model)
+{
+    if (model == PF_MODEL_UNICYCLE) return ops_of<Unicycle>();
+    if (model == PF_MODEL_DHARM) return ops_of<DhArm>();
+    return ops_of<RefArm>();
+}
+
+// ---------------------------------------------------------------------------
+// MTGP32 stream initialisation on the host (mtgp32_init_state,
+// src/partfilt/cuda/mtgp/mtgp32-fast.c:119-137): the same 351 words the
+// reference seeds stream g with (seed + g + 1).
+// ---------------------------------------------------------------------------
+static const uint32_t kHostParams[200 * 52] = {
+#include "mtgp32_params_11213.inc"
+};
+
+static void mtgp_init_state_host(uint32_t* st, int set, uint32_t seed)
+{
+    const uint32_t* tbl = kHostParams + set * 52 + 4;
+    const uint32_t hidden = tbl[4] ^ (tbl[8] << 16);
+    uint32_t tmp = hidden;
+    tmp += tmp >> 16;
+    tmp += tmp >> 8;
+    const uint32_t b = tmp & 0xffu;
+    const uint32_t fill = b | (b << 8) | (b << 16) | (b << 24);
+    for (int i = 0; i < kMtgpN; ++i) st[i] = fill;
+    st[0] = seed;
+    st[1] = hidden;
+    for (int i = 1; i < kMtgpN; ++i) st[i] ^= 1812433253u * (st[i - 1] ^ (st[i - 1] >> 30)) + (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------
+// filter
+// ---------------------------------------------------------------------------
+struct pf_filter {
+    pf_config cfg;
+    int model;
+    ModelParams mp;
+    ModelInfo mi;
+    ModelOps ops;
+    int M, E, N, t, dx, dy, streams;
+    int64_t T, rtotal, draws, nbm;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    float *state = nullptr, *tmp = nullptr, *tkey = nullptr, *key = nullptr, *winner = nullptr, *ru = nullptr,
+          *rbuf = nullptr;
+    double* part = nullptr;
+    uint32_t* mtgp = nullptr;
+    int32_t *a2a = nullptr, *sel = nullptr, *ctr = nullptr;
+    pf_estimate* d_est = nullptr;
+    pf_step_input* d_in = nullptr;
+    FilterDesc* d_desc = nullptr;  // [0]: pf_step, [1]: pf_run_device
+    FilterDesc h_desc;
+    pf_estimate* h_est = nullptr;
+    pf_step_input* h_in = nullptr;
+    int64_t dev_bytes = 0;
+    int32_t steps_done = 0;
+    cudaGraphExec_t graph = nullptr;
+    const pf_step_input* graph_inputs = nullptr;
+    pf_estimate* graph_est = nullptr;
+    // per-phase timing: events recorded between the launches of a step
+    int timing = 0;
+    cudaEvent_t ev[8] = {};
+    const char* phase[8] = {};
+    int nphase = 0;
+};
+
+template <class T>
+static pf_status dalloc(pf_filter* f, T** p, size_t count)
+{
+    void* q = nullptr;
+    const size_t bytes = count * sizeof(T);
+    if (bytes == 0) {
+        *p = nullptr;
+        return PF_OK;
+    }
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PF_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    f->allocs.push_back(q);
+    f->dev_bytes += (int64_t)bytes;
+    *p = static_cast<T*>(q);
+    return PF_OK;
+}
+
+static void release(pf_filter* f)
+{
+    if (!f) return;
+    if (f->graph) cudaGraphExecDestroy(f->graph);
+    for (cudaEvent_t e : f->ev)
+        if (e) cudaEventDestroy(e);
+    for (void* p : f->allocs) cudaFree(p);
+    if (f->h_est) cudaFreeHost(f->h_est);
+    if (f->h_in) cudaFreeHost(f->h_in);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+}
+
+extern "C" pf_status pf_config_default(pf_config* c)
+{
+    if (!c) return fail(PF_ERR_INVALID, "null config");
+    memset(c, 0, sizeof(*c));
+    c->particles_per_subfilter = 512;
+    c->num_subfilters = 16;
+    c->num_transfer = 1;
+    c->exchange = PF_EXCHANGE_RING;
+    c->resampler = PF_RESAMPLE_SYSTEMATIC;
+    c->resampling_freq = 1.0f;
+    c->seed = 0xF000000Du;
+    c->rng = PF_RNG_SUBFILTER;
+    c->mtgp_streams = 96;
+    c->mtgp_mask = PF_MTGP_MASK_PARAMS;
+    c->log_weights = 1;
+    c->pipeline = PF_PIPELINE_FUSED;
+    c->particles_per_thread = 0;
+    c->device = 0;
+    return PF_OK;
+}
+
+static int default_ppt(int M)
+{
+    if (M <= 32) return 1;
+    if (M <= 64) return 2;
+    return 2;
+}
+
+static void torus_dims(int N, int* dx, int* dy)
+{
+    int x = 1;
+    while ((int64_t)(2 * x) * (2 * x) <= N) x *= 2;
+    *dx = x;
+    *dy = N / x;
+}
+
+static void torus_dims(int N, int* dx, int* dy);
+
+static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, int* E)
+{
+    const int M = c->particles_per_subfilter;
+    if (M < 32 || M > 1024 || (M & (M - 1)))
+        return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
+    if (c->num_subfilters < 1) return fail(PF_ERR_INVALID, "num_subfilters must be >= 1");
+    if ((int64_t)M * c->num_subfilters > (int64_t)1 << 30) return fail(PF_ERR_INVALID, "too many particles");
+    if (c->num_transfer < 0) return fail(PF_ERR_INVALID, "num_transfer must be >= 0");
+    if (c->exchange < PF_EXCHANGE_NONE || c->exchange > PF_EXCHANGE_ALL2ALL)
+        return fail(PF_ERR_INVALID, "unknown exchange %d", c->exchange);
+    if (c->exchange == PF_EXCHANGE_TORUS && 5 * c->num_transfer > M)
+        return fail(PF_ERR_INVALID, "torus exchange needs 5*t <= m (t=%d, m=%d)", c->num_transfer, M);
+    if (c->exchange == PF_EXCHANGE_TORUS) {
+        int dx, dy;
+        torus_dims(c->num_subfilters, &dx, &dy);
+        if (dx * dy != c->num_subfilters)
+            return fail(PF_ERR_INVALID, "torus exchange needs N = dx*dy with dx = 2^floor(log2 sqrt N) (N=%d)",
+                        c->num_subfilters);
+    }
+    if ((c->exchange == PF_EXCHANGE_RING || c->exchange == PF_EXCHANGE_ALL2ALL) && 2 * c->num_transfer > M)
+        return fail(PF_ERR_INVALID, "exchange needs 2*t <= m (t=%d, m=%d)", c->num_transfer, M);
+    if (c->exchange == PF_EXCHANGE_ALL2ALL && (c->num_subfilters > 8192 || c->num_transfer > c->num_subfilters * M))
+        return fail(PF_ERR_UNSUPPORTED, "all-to-all exchange supports at most 8192 sub-filters");
+    if (c->resampler < PF_RESAMPLE_REFERENCE || c->resampler > PF_RESAMPLE_VOSE)
+        return fail(PF_ERR_INVALID, "unknown resampler %d", c->resampler);
+    if (!(c->resampling_freq >= 0.0f && c->resampling_freq <= 1.0f))
+        return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
+    if (c->rng != PF_RNG_SUBFILTER && c->rng != PF_RNG_REFLAYOUT) return fail(PF_ERR_INVALID, "unknown rng layout");
+    if (c->rng == PF_RNG_REFLAYOUT && (c->mtgp_streams < 1 || c->mtgp_streams > 200))
+        return fail(PF_ERR_INVALID, "mtgp_streams must be in [1, 200]");
+    if (c->pipeline == PF_PIPELINE_PHASED && c->rng != PF_RNG_REFLAYOUT)
+        return fail(PF_ERR_INVALID, "the phased pipeline uses the reference RNG layout (rng = PF_RNG_REFLAYOUT)");
+    if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED)
+        return fail(PF_ERR_INVALID, "unknown pipeline");
+    *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M);
+    if (!me_supported(M, *E))
+        return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", *E, M);
+    (void)model;
+    (void)mi;
+    return PF_OK;
+}
+
+static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
+{
+    memset(&D, 0, sizeof(D));
+    D.state = f->state;
+    D.tmp = f->tmp;
+    D.tkey = f->tkey;
+    D.key = f->key;
+    D.winner = f->winner;
+    D.part = f->part;
+    D.mtgp = f->mtgp;
+    D.ru = f->ru;
+    D.rbuf = f->rbuf;
+    D.a2a = f->a2a;
+    D.sel = f->sel;
+    D.est = est;
+    D.T = f->T;
+    D.N = f->N;
+    D.M = f->M;
+    D.t = f->t;
+    D.exchange = f->cfg.exchange;
+    D.resampler = f->cfg.resampler;
+    D.dx = f->dx;
+    D.dy = f->dy;
+    D.log_weights = f->cfg.log_weights ? 1 : 0;
+    D.inplace = (f->cfg.resampling_freq < 1.0f || f->cfg.pipeline == PF_PIPELINE_PHASED) ? 1 : 0;
+    D.rng_fused = f->cfg.rng == PF_RNG_SUBFILTER ? 1 : 0;
+    D.draws = (int32_t)f->draws;
+    D.nbm = (int32_t)f->nbm;
+    D.ru_stride = (int32_t)(f->draws - f->nbm);
+    D.mask = f->cfg.mtgp_mask;
+    D.stream_base = 0;
+    D.freq = f->cfg.resampling_freq;
+    D.nnorm = (int64_t)f->mi.K * f->T;
+    D.mp = f->mp;
+}
+
+static pf_status upload_descs(pf_filter* f, pf_estimate* run_est)
+{
+    FilterDesc d[2];
+    fill_desc(f, d[0], f->d_est);
+    fill_desc(f, d[1], run_est);
+    f->h_desc = d[0];
+    CU(cudaMemcpyAsync(f->d_desc, d, sizeof(d), cudaMemcpyHostToDevice, f->stream));
+    CU(cudaStreamSynchronize(f->stream));
+    return PF_OK;
+}
+
+static int64_t resample_draws(int res, int M)
+{
+    return res == PF_RESAMPLE_REFERENCE ? M : (res == PF_RESAMPLE_VOSE ? 2 * (int64_t)M : 1);
+}
+
+static pf_status init_streams(pf_filter* f)
+{
+    std::vector<uint32_t> st((size_t)f->streams * kMtgpN);
+    for (int g = 0; g < f->streams; ++g)
+        mtgp_init_state_host(st.data() + (size_t)g * kMtgpN, g % kMtgpSets, f->cfg.seed + (uint32_t)g + 1u);
+    CU(cudaMemcpy(f->mtgp, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const void* params, size_t params_size,
+                               pf_filter** out)
+{
+    if (!cfg || !out) return fail(PF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    if (!params || params_size != mi.psize)
+        return fail(PF_ERR_INVALID, "model params size %zu, expected %zu", params_size, mi.psize);
+    int E = 0;
+    pf_status s = validate(cfg, model, mi, &E);
+    if (s != PF_OK) return s;
+    if (model == PF_MODEL_UNICYCLE) {
+        const pf_unicycle_params* p = (const pf_unicycle_params*)params;
+        if (p->num_landmarks < 1 || p->num_landmarks > 8) return fail(PF_ERR_INVALID, "1..8 landmarks");
+        if (!(p->sigma_range > 0) || !(p->sigma_bearing > 0)) return fail(PF_ERR_INVALID, "sigmas must be > 0");
+    } else if (model == PF_MODEL_DHARM) {
+        const pf_dharm_params* p = (const pf_dharm_params*)params;
+        if (!(p->sigma_pos > 0) || !(p->sigma_ang > 0)) return fail(PF_ERR_INVALID, "sigmas must be > 0");
+    }
+    s = require_gpu(cfg->device);
+    if (s != PF_OK) return s;
+
+    pf_filter* f = new pf_filter();
+    f->cfg = *cfg;
+    f->model = model;
+    memset(&f->mp, 0, sizeof(f->mp));
+    memcpy(&f->mp, params, params_size);
+    f->mi = mi;
+    f->ops = model_ops(model);
+    f->M = cfg->particles_per_subfilter;
+    f->E = E;
+    f->N = cfg->num_subfilters;
+    f->t = cfg->exchange == PF_EXCHANGE_NONE ? 0 : cfg->num_transfer;
+    f->T = (int64_t)f->M * f->N;
+    torus_dims(f->N, &f->dx, &f->dy);
+    f->nbm = 2 * (((int64_t)mi.K * f->M + 1) / 2);
+    f->draws = f->nbm + 1 + resample_draws(cfg->resampler, f->M);
+    f->streams = cfg->rng == PF_RNG_SUBFILTER ? f->N : cfg->mtgp_streams;
+    if (cfg->rng == PF_RNG_REFLAYOUT) {
+        const int64_t nn = (int64_t)mi.K * f->T;
+        const int64_t nu = cfg->resampler == PF_RESAMPLE_VOSE ? (int64_t)(2 * f->M + 1) * f->N
+                                                              : (int64_t)(f->M + 1) * f->N;
+        const int64_t unit = 768LL * cfg->mtgp_streams;
+        f->rtotal = ((nn + nu + unit - 1) / unit) * unit;
+        if (f->rtotal / cfg->mtgp_streams > INT32_MAX) {
+            release(f);
+            return fail(PF_ERR_UNSUPPORTED, "random buffer too large for the reference layout");
+        }
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        release(f);
+        return fail(PF_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    const int S = mi.S;
+#define TRY(x)                 \
+    do {                       \
+        pf_status s_ = (x);    \
+        if (s_ != PF_OK) {     \
+            release(f);        \
+            return s_;         \
+        }                      \
+    } while (0)
+    TRY(dalloc(f, &f->state, (size_t)S * f->T));
+    TRY(dalloc(f, &f->tmp, (size_t)S * f->T));
+    TRY(dalloc(f, &f->tkey, (size_t)f->T));
+    if (cfg->pipeline == PF_PIPELINE_PHASED) TRY(dalloc(f, &f->key, (size_t)f->T));
+    TRY(dalloc(f, &f->winner, (size_t)f->N));
+    TRY(dalloc(f, &f->part, (size_t)f->N * kPartStride));
+    TRY(dalloc(f, &f->mtgp, (size_t)f->streams * kMtgpN));
+    if (cfg->rng == PF_RNG_SUBFILTER) TRY(dalloc(f, &f->ru, (size_t)f->N * (f->draws - f->nbm)));
+    else TRY(dalloc(f, &f->rbuf, (size_t)f->rtotal));
+    if (cfg->exchange == PF_EXCHANGE_ALL2ALL) TRY(dalloc(f, &f->a2a, (size_t)(f->t > 0 ? f->t : 1)));
+    TRY(dalloc(f, &f->ctr, 1));
+    TRY(dalloc(f, &f->d_est, 1));
+    TRY(dalloc(f, &f->d_in, 1));
+    TRY(dalloc(f, &f->d_desc, 2));
+    if (cudaMallocHost(&f->h_est, sizeof(pf_estimate)) != cudaSuccess ||
+        cudaMallocHost(&f->h_in, sizeof(pf_step_input)) != cudaSuccess) {
+        cudaGetLastError();
+        release(f);
+        return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
+    }
+    TRY(init_streams(f));
+    TRY(upload_descs(f, nullptr));
+    TRY(pf_set_initial_state(f, init_state_of(model, f->mp)));
+#undef TRY
+    *out = f;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_destroy(pf_filter* f)
+{
+    if (!f) return PF_OK;
+    cudaSetDevice(f->cfg.device);
+    cudaStreamSynchronize(f->stream);
+    release(f);
+    return PF_OK;
+}
+
+extern "C" pf_status pf_set_initial_state(pf_filter* f, const float* state)
+{
+    if (!f || !state) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    std::vector<float> h((size_t)f->mi.S * f->T);
+    for (int v = 0; v < f->mi.S; ++v)
+        for (int64_t i = 0; i < f->T; ++i) h[(size_t)v * f->T + i] = state[v];
+    CU(cudaMemcpy(f->state, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+    f->steps_done = 0;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_set_particles(pf_filter* f, const float* soa)
+{
+    if (!f || !soa) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    CU(cudaMemcpy(f->state, soa, (size_t)f->mi.S * f->T * 4, cudaMemcpyHostToDevice));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_get_particles(pf_filter* f, float* soa)
+{
+    if (!f || !soa) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    CU(cudaMemcpy(soa, f->state, (size_t)f->mi.S * f->T * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_get_sorted(pf_filter* f, float* soa, float* keys)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    if (soa) CU(cudaMemcpy(soa, f->tmp, (size_t)f->mi.S * f->T * 4, cudaMemcpyDeviceToHost));
+    if (keys) CU(cudaMemcpy(keys, f->tkey, (size_t)f->T * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_record_selection(pf_filter* f, int32_t enable)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    if (enable && !f->sel) {
+        pf_status s = dalloc(f, &f->sel, (size_t)f->T);
+        if (s != PF_OK) return s;
+    }
+    if (!enable) f->sel = nullptr;  // the buffer stays allocated until destroy
+    if (f->graph) {
+        cudaGraphExecDestroy(f->graph);
+        f->graph = nullptr;
+    }
+    return upload_descs(f, f->graph_est);
+}
+
+extern "C" pf_status pf_get_selection(pf_filter* f, int32_t* sel)
+{
+    if (!f || !sel) return fail(PF_ERR_INVALID, "null argument");
+    if (!f->sel) return fail(PF_ERR_INVALID, "selection recording is off (pf_record_selection)");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    CU(cudaMemcpy(sel, f->sel, (size_t)f->T * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+// The launch sequence of one step on f->stream.  desc: device descriptor to use.
+// With timing on, an event is recorded before the first and after every launch
+// (also inside a captured graph, as event-record nodes).
+static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in, int32_t* ctr_inc)
+{
+    const int M = f->M, E = f->E, N = f->N;
+    cudaStream_t st = f->stream;
+    const pf_config& c = f->cfg;
+    int np = 0;
+    auto mark = [&](const char* name) -> cudaError_t {
+        if (!f->timing) return cudaSuccess;
+        if (name) f->phase[np - 1] = name;
+        if (np >= 8) return cudaSuccess;
+        return cudaEventRecord(f->ev[np++], st);
+    };
+    CU(mark(nullptr));
+    if (c.rng == PF_RNG_REFLAYOUT) {
+        const int G = c.mtgp_streams;
+        CU(launch_mtgp_blocks(G, f->mtgp, reinterpret_cast<uint32_t*>(f->rbuf), f->rtotal / G, c.mtgp_mask, 1, 0, st));
+        CU(mark("mtgp32"));
+        CU(launch_boxmuller(f->rbuf, (int64_t)f->mi.K * f->T, st));
+        CU(mark("boxmuller"));
+    }
+    if (c.pipeline == PF_PIPELINE_FUSED) {
+        CU(f->ops.sample_sort(M, E, c.rng == PF_RNG_SUBFILTER, N, st, desc, nullptr, in));
+        CU(mark("sample_sort"));
+        if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
+            CU(launch_a2a_merge(1, desc, st));
+            CU(mark("a2a_merge"));
+        }
+        CU(f->ops.estimate(1, st, desc, in));
+        CU(mark("estimate"));
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, ctr_inc, 1));
+        CU(mark("exchange_resample"));
+    } else {
+        CU(f->ops.sample_weight(M, E, N, st, desc, nullptr, in));
+        CU(mark("sample_weight"));
+        CU(f->ops.block_sort(M, E, N, st, desc, nullptr));
+        CU(mark("block_sort"));
+        if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
+            CU(launch_a2a_merge(1, desc, st));
+            CU(mark("a2a_merge"));
+        }
+        CU(f->ops.estimate(1, st, desc, in));
+        CU(mark("estimate"));
+        if (c.exchange != PF_EXCHANGE_NONE && f->t > 0) {
+            const int nx = c.exchange == PF_EXCHANGE_TORUS ? 4 * f->t : f->t;
+            CU(f->ops.exchange_inplace(N, nx < 1024 ? ((nx + 31) / 32) * 32 : 1024, st, desc, nullptr));
+            CU(mark("exchange"));
+        }
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, ctr_inc, 0));
+        CU(mark("resample"));
+    }
+    if (f->timing) f->nphase = np - 1;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_set_timing(pf_filter* f, int32_t enable)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    if (enable && !f->ev[0])
+        for (auto& e : f->ev) CU(cudaEventCreate(&e));
+    if ((enable != 0) != (f->timing != 0) && f->graph) {
+        cudaGraphExecDestroy(f->graph);
+        f->graph = nullptr;
+    }
+    f->timing = enable ? 1 : 0;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_last_step_timing(pf_filter* f, float* ms, int32_t cap, int32_t* n)
+{
+    if (!f || !n) return fail(PF_ERR_INVALID, "null argument");
+    if (!f->timing || f->nphase <= 0) return fail(PF_ERR_INVALID, "timing is off or no step ran");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaEventSynchronize(f->ev[f->nphase]));
+    *n = f->nphase;
+    for (int i = 0; i < f->nphase && i < cap; ++i) CU(cudaEventElapsedTime(&ms[i], f->ev[i], f->ev[i + 1]));
+    return PF_OK;
+}
+
+extern "C" const char* pf_phase_name(pf_filter* f, int32_t i)
+{
+    if (!f || i < 0 || i >= f->nphase) return "";
+    return f->phase[i];
+}
+
+extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate* out)
+{
+    if (!f || !in) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    *f->h_in = *in;
+    CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
+    InputRef ir{f->d_in, 0, nullptr};
+    pf_status s = enqueue_step(f, f->d_desc, ir, nullptr);
+    if (s != PF_OK) return s;
+    CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate), cudaMemcpyDeviceToHost, f->stream));
+    CU(cudaStreamSynchronize(f->stream));
+    f->steps_done++;
+    if (out) {
+        *out = *f->h_est;
+        out->step = f->steps_done;
+    }
+    return PF_OK;
+}
+
+extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, int32_t steps,
+                                   pf_estimate* d_estimates)
+{
+    if (!f || !d_inputs || !d_estimates || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
+    CU(cudaSetDevice(f->cfg.device));
+    if (steps == 0) return PF_OK;
+    if (!f->graph || f->graph_inputs != d_inputs || f->graph_est != d_estimates) {
+        if (f->graph) {
+            cudaGraphExecDestroy(f->graph);
+            f->graph = nullptr;
+        }
+        pf_status s = upload_descs(f, d_estimates);
+        if (s != PF_OK) return s;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
+        InputRef ir{d_inputs, 0, f->ctr};
+        s = enqueue_step(f, f->d_desc + 1, ir, f->ctr);
+        cudaError_t e = cudaStreamEndCapture(f->stream, &g);
+        if (s != PF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) return fail(PF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&f->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            f->graph = nullptr;
+            return fail(PF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        f->graph_inputs = d_inputs;
+        f->graph_est = d_estimates;
+    }
+    CU(cudaMemsetAsync(f->ctr, 0, sizeof(int32_t), f->stream));
+    for (int i = 0; i < steps; ++i) CU(cudaGraphLaunch(f->graph, f->stream));
+    f->steps_done += steps;
+    return PF_OK;
+}
+
+// One step of a run already set up by pf_run_device (graph replay with the
+// counter continuing); used to time steps one by one.
+extern "C" pf_status pf_run_device_continue(pf_filter* f, int32_t steps)
+{
+    if (!f || !f->graph) return fail(PF_ERR_INVALID, "no run set up (call pf_run_device first)");
+    CU(cudaSetDevice(f->cfg.device));
+    for (int i = 0; i < steps; ++i) CU(cudaGraphLaunch(f->graph, f->stream));
+    f->steps_done += steps;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_synchronize(pf_filter* f)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    return PF_OK;
+}
+
+extern "C" void* pf_stream(pf_filter* f) { return f ? (void*)f->stream : nullptr; }
+
+extern "C" pf_status pf_get_info(pf_filter* f, int32_t* ppt, int32_t* dx, int32_t* dy, int64_t* bytes)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    if (ppt) *ppt = f->E;
+    if (dx) *dx = f->dx;
+    if (dy) *dy = f->dy;
+    if (bytes) *bytes = f->dev_bytes;
+    return PF_OK;
+}
+
+// snapshot layout: int64 header[4] = {magic, S, T, streams}, state S*T floats,
+// stream words streams*351, int32 steps_done.
+static const int64_t kSnapMagic = 0x5046534e41503031LL;
+
+extern "C" int64_t pf_snapshot_size(pf_filter* f)
+{
+    if (!f) return -1;
+    return 32 + (int64_t)f->mi.S * f->T * 4 + (int64_t)f->streams * kMtgpN * 4 + 4;
+}
+
+extern "C" pf_status pf_snapshot(pf_filter* f, void* buf)
+{
+    if (!f || !buf) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    char* p = (char*)buf;
+    int64_t hdr[4] = {kSnapMagic, f->mi.S, f->T, f->streams};
+    memcpy(p, hdr, 32);
+    p += 32;
+    const size_t sb = (size_t)f->mi.S * f->T * 4, mb = (size_t)f->streams * kMtgpN * 4;
+    CU(cudaMemcpy(p, f->state, sb, cudaMemcpyDeviceToHost));
+    p += sb;
+    CU(cudaMemcpy(p, f->mtgp, mb, cudaMemcpyDeviceToHost));
+    p += mb;
+    memcpy(p, &f->steps_done, 4);
+    return PF_OK;
+}
+
+extern "C" pf_status pf_restore(pf_filter* f, const void* buf)
+{
+    if (!f || !buf) return fail(PF_ERR_INVALID, "null argument");
+    const char* p = (const char*)buf;
+    int64_t hdr[4];
+    memcpy(hdr, p, 32);
+    if (hdr[0] != kSnapMagic || hdr[1] != f->mi.S || hdr[2] != f->T || hdr[3] != f->streams)
+        return fail(PF_ERR_INVALID, "snapshot does not match this filter");
+    p += 32;
+    CU(cudaSetDevice(f->cfg.device));
+    CU(cudaStreamSynchronize(f->stream));
+    const size_t sb = (size_t)f->mi.S * f->T * 4, mb = (size_t)f->streams * kMtgpN * 4;
+    CU(cudaMemcpy(f->state, p, sb, cudaMemcpyHostToDevice));
+    p += sb;
+    CU(cudaMemcpy(f->mtgp, p, mb, cudaMemcpyHostToDevice));
+    p += mb;
+    memcpy(&f->steps_done, p, 4);
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel-level entry points (host arrays in/out)
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+static pf_status dev_buf(DevBuf& b, size_t bytes)
+{
+    CU(cudaMalloc(&b.p, bytes ? bytes : 4));
+    return PF_OK;
+}
+
+#define TRYS(x)                 \
+    do {                        \
+        pf_status s_ = (x);     \
+        if (s_ != PF_OK) return s_; \
+    } while (0)
+
+extern "C" pf_status pfk_mtgp_generate(int32_t G, uint32_t seed, uint32_t mask, int32_t kind, int64_t per_stream,
+                                       int32_t calls, uint32_t* out)
+{
+    if (G < 1 || G > 200 || per_stream < 0 || per_stream > INT32_MAX || calls < 1 || !out)
+        return fail(PF_ERR_INVALID, "bad argument");
+    TRYS(require_gpu(0));
+    std::vector<uint32_t> st((size_t)G * kMtgpN);
+    for (int g = 0; g < G; ++g) mtgp_init_state_host(st.data() + (size_t)g * kMtgpN, g, seed + (uint32_t)g + 1u);
+    DevBuf ds, dout;
+    TRYS(dev_buf(ds, st.size() * 4));
+    TRYS(dev_buf(dout, (size_t)G * per_stream * 4));
+    CU(cudaMemcpy(ds.p, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+    for (int c = 0; c < calls; ++c) {
+        CU(launch_mtgp_blocks(G, (uint32_t*)ds.p, (uint32_t*)dout.p, per_stream, mask, kind ? 1 : 0, 0, 0));
+        CU(cudaMemcpy(out + (size_t)c * G * per_stream, dout.p, (size_t)G * per_stream * 4, cudaMemcpyDeviceToHost));
+    }
+    return PF_OK;
+}
+
+extern "C" pf_status pfk_boxmuller(float* data, int64_t n)
+{
+    if (!data || n < 0) return fail(PF_ERR_INVALID, "bad argument");
+    TRYS(require_gpu(0));
+    const size_t cnt = (size_t)(2 * ((n + 1) / 2));
+    DevBuf d;
+    TRYS(dev_buf(d, cnt * 4));
+    CU(cudaMemcpy(d.p, data, cnt * 4, cudaMemcpyHostToDevice));
+    CU(launch_boxmuller((float*)d.p, n, 0));
+    CU(cudaMemcpy(data, d.p, cnt * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+static int pick_ppt(int m, int ppt) { return ppt > 0 ? ppt : default_ppt(m); }
+
+extern "C" pf_status pfk_bitonic_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt)
+{
+    if (!keys || !idx || nsub < 1) return fail(PF_ERR_INVALID, "bad argument");
+    const int E = pick_ppt(m, ppt);
+    if (!me_supported(m, E)) return fail(PF_ERR_UNSUPPORTED, "m=%d ppt=%d not built", m, E);
+    TRYS(require_gpu(0));
+    const size_t n = (size_t)m * nsub;
+    DevBuf dk, di;
+    TRYS(dev_buf(dk, n * 4));
+    TRYS(dev_buf(di, n * 4));
+    CU(cudaMemcpy(dk.p, keys, n * 4, cudaMemcpyHostToDevice));
+    CU(launch_test_sort(m, E, nsub, (float*)dk.p, (int32_t*)di.p, 0));
+    CU(cudaMemcpy(keys, dk.p, n * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(idx, di.p, n * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+static pf_status test_resample(int res, const float* w, const float* u, int m, int nsub, int ppt, int32_t* sel,
+                               float* prob, uint32_t* alias)
+{
+    const int E = pick_ppt(m, ppt);
+    if (!me_supported(m, E)) return fail(PF_ERR_UNSUPPORTED, "m=%d ppt=%d not built", m, E);
+    TRYS(require_gpu(0));
+    const size_t n = (size_t)m * nsub;
+    const size_t nu = res == PF_RESAMPLE_SYSTEMATIC ? (size_t)nsub : (res == PF_RESAMPLE_VOSE ? 2 * n : n);
+    DevBuf dw, du, ds, dp, da;
+    TRYS(dev_buf(dw, n * 4));
+    TRYS(dev_buf(du, nu * 4));
+    TRYS(dev_buf(ds, n * 4));
+    CU(cudaMemcpy(dw.p, w, n * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(du.p, u, nu * 4, cudaMemcpyHostToDevice));
+    if (prob) {
+        TRYS(dev_buf(dp, n * 4));
+        TRYS(dev_buf(da, n * 4));
+    }
+    CU(launch_test_resample(res, m, E, nsub, (const float*)dw.p, (const float*)du.p, (int32_t*)ds.p,
+                            (float*)dp.p, (uint32_t*)da.p, 0));
+    if (sel) CU(cudaMemcpy(sel, ds.p, n * 4, cudaMemcpyDeviceToHost));
+    if (prob) {
+        CU(cudaMemcpy(prob, dp.p, n * 4, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(alias, da.p, n * 4, cudaMemcpyDeviceToHost));
+    }
+    return PF_OK;
+}
+
+extern "C" pf_status pfk_resample(int32_t resampler, const float* w, const float* u, int32_t m, int32_t nsub,
+                                  int32_t ppt, int32_t* sel)
+{
+    if (!w || !u || !sel || nsub < 1 || resampler < 0 || resampler > 2) return fail(PF_ERR_INVALID, "bad argument");
+    return test_resample(resampler, w, u, m, nsub, ppt, sel, nullptr, nullptr);
+}
+
+extern "C" pf_status pfk_vose_build(const float* w, int32_t m, int32_t nsub, int32_t ppt, float* prob,
+                                    uint32_t* alias)
+{
+    if (!w || !prob || !alias || nsub < 1) return fail(PF_ERR_INVALID, "bad argument");
+    std::vector<float> u((size_t)2 * m * nsub, 0.0f);
+    return test_resample(PF_RESAMPLE_VOSE, w, u.data(), m, nsub, ppt, nullptr, prob, alias);
+}
+
+extern "C" pf_status pfk_exchange_sources(int32_t mode, int32_t N, int32_t m, int32_t t, const float* sorted_keys,
+                                          int32_t* src)
+{
+    // Routing is evaluated by the same device function the step kernels use.
+    if (!src || N < 1 || m < 1 || t < 0) return fail(PF_ERR_INVALID, "bad argument");
+    if (mode == PF_EXCHANGE_ALL2ALL && (!sorted_keys || N > 8192)) return fail(PF_ERR_INVALID, "bad argument");
+    TRYS(require_gpu(0));
+    const int64_t T = (int64_t)m * N;
+    DevBuf dkeys, da2a, dsrc, ddesc;
+    TRYS(dev_buf(dkeys, (size_t)T * 4));
+    TRYS(dev_buf(da2a, (size_t)(t > 0 ? t : 1) * 4));
+    TRYS(dev_buf(dsrc, (size_t)T * 4));
+    TRYS(dev_buf(ddesc, sizeof(FilterDesc)));
+    if (sorted_keys) CU(cudaMemcpy(dkeys.p, sorted_keys, (size_t)T * 4, cudaMemcpyHostToDevice));
+    FilterDesc D;
+    memset(&D, 0, sizeof(D));
+    D.tkey = (float*)dkeys.p;
+    D.a2a = (int32_t*)da2a.p;
+    D.T = T;
+    D.N = N;
+    D.M = m;
+    D.t = t;
+    D.exchange = mode;
+    torus_dims(N, &D.dx, &D.dy);
+    CU(cudaMemcpy(ddesc.p, &D, sizeof(D), cudaMemcpyHostToDevice));
+    if (mode == PF_EXCHANGE_ALL2ALL && t > 0) CU(launch_a2a_merge(1, (const FilterDesc*)ddesc.p, 0));
+    CU(launch_exchange_sources((const FilterDesc*)ddesc.p, (int32_t*)dsrc.p, 0));
+    CU(cudaMemcpy(src, dsrc.p, (size_t)T * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pfk_model_step(pf_model_id model, const void* params, size_t params_size,
+                                    const pf_step_input* in, int32_t n, float* state, const float* noise,
+                                    float* loglik)
+{
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model");
+    if (!params || params_size != mi.psize || !in || n < 1 || !state || !noise || !loglik)
+        return fail(PF_ERR_INVALID, "bad argument");
+    TRYS(require_gpu(0));
+    ModelParams mp;
+    memset(&mp, 0, sizeof(mp));
+    memcpy(&mp, params, params_size);
+    DevBuf din, ds, dn, dl;
+    TRYS(dev_buf(din, sizeof(pf_step_input)));
+    TRYS(dev_buf(ds, (size_t)mi.S * n * 4));
+    TRYS(dev_buf(dn, (size_t)mi.K * n * 4));
+    TRYS(dev_buf(dl, (size_t)n * 4));
+    CU(cudaMemcpy(din.p, in, sizeof(pf_step_input), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ds.p, state, (size_t)mi.S * n * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(dn.p, noise, (size_t)mi.K * n * 4, cudaMemcpyHostToDevice));
+    CU(model_ops(model).test_model(mp, (const pf_step_input*)din.p, n, (float*)ds.p, (const float*)dn.p,
+                                   (float*)dl.p, 0));
+    CU(cudaMemcpy(state, ds.p, (size_t)mi.S * n * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(loglik, dl.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}

@@ -1,0 +1,693 @@
+// pf_device.cuh -- device building blocks of the particle-filter step (sm_100a).
+//
+// Each block restates one routine of the Esthera step with B200-first data
+// movement: SoA particle state read as float2/float4 per thread, a
+// sub-filter staged in shared memory, warp shuffles for the short sort
+// strides and the scans, one MTGP32 stream per CTA generating straight into
+// shared memory.  Citations are to the Esthera source tree.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "esthera_b200.h"
+
+namespace pfdev {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kTwoPi = 6.28318530717958647692f;
+constexpr float kInvTwoPi = 0.15915494309189533577f;
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// MTGP32-11213 (mtgp32-cuda.cu:82-128, 259-306; mtgp32-fast.h:145-214)
+// ---------------------------------------------------------------------------
+constexpr int kMtgpN = 351;        // state words
+constexpr int kMtgpSets = 200;     // parameter sets
+constexpr int kMtgpLanes = 256;    // outputs per recursion round (N - max(pos) > 256)
+constexpr int kMtgpRing = 1024;    // shared ring; x_j lives at ring[j & 1023]
+
+// The 200 parameter sets, 52 words each (layout in gen_mtgp_params.py).  One
+// copy per translation unit; only 41.6 KB and read once per CTA into smem.
+static __device__ const uint32_t g_mtgp_params[kMtgpSets * 52] = {
+#include "mtgp32_params_11213.inc"
+};
+
+struct MtgpSmem {
+    uint32_t ring[kMtgpRing];
+    uint32_t tbl[16];
+    uint32_t ttb[16];  // flt_tmp_tbl (float output) or tmp_tbl (uint32 output)
+    uint32_t pos, sh1, sh2, mask;
+};
+
+// Stream state words x_0..x_350 -> ring[0..350]; parameter set tables -> smem.
+__device__ __forceinline__ void mtgp_load(MtgpSmem& s, const uint32_t* __restrict__ gstate, int set,
+                                          uint32_t mask, bool float_out)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < kMtgpN; i += nt) s.ring[i] = gstate[i];
+    const uint32_t* P = g_mtgp_params + set * 52;
+    for (int i = tid; i < 16; i += nt) {
+        s.tbl[i] = P[4 + i];
+        s.ttb[i] = float_out ? P[36 + i] : P[20 + i];
+    }
+    if (tid == 0) {
+        s.pos = P[0];
+        s.sh1 = P[1];
+        s.sh2 = P[2];
+        s.mask = mask ? mask : P[3];
+    }
+    __syncthreads();
+}
+
+// Generate n outputs of the stream held in s.ring, in rounds of 256:
+// output k: x_{k+351} = rec(x_k, x_{k+1}, x_{k+pos}); out_k = temper(x_{k+351}, x_{k+pos-1}).
+// Within a round every read index is < base+351 <= every write index, so
+// the 256 lanes are independent; one barrier separates rounds.  emit(k, word)
+// is called for k < n.  Ends with a barrier.
+template <class Emit>
+__device__ __forceinline__ void mtgp_generate(MtgpSmem& s, int n, bool float_out, Emit emit)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t pos = s.pos, sh1 = s.sh1, sh2 = s.sh2, mask = s.mask;
+    for (int base = 0; base < n; base += kMtgpLanes) {
+        for (int l = tid; l < kMtgpLanes; l += nt) {
+            const int k = base + l;
+            const uint32_t x1 = s.ring[k & 1023], x2 = s.ring[(k + 1) & 1023];
+            uint32_t y = s.ring[(k + pos) & 1023];
+            uint32_t t = s.ring[(k + pos - 1) & 1023];
+            uint32_t x = (x1 & mask) ^ x2;
+            x ^= x << sh1;
+            y = x ^ (y >> sh2);
+            const uint32_t r = y ^ s.tbl[y & 0x0f];
+            s.ring[(k + kMtgpN) & 1023] = r;
+            t ^= t >> 16;
+            t ^= t >> 8;
+            const uint32_t o = float_out ? ((r >> 9) ^ s.ttb[t & 0x0f]) : (r ^ s.ttb[t & 0x0f]);
+            if (k < n) emit(k, o);
+        }
+        __syncthreads();
+    }
+}
+
+// State after n outputs: x_n .. x_{n+350}.
+__device__ __forceinline__ void mtgp_store(const MtgpSmem& s, uint32_t* __restrict__ gstate, int n)
+{
+    for (int i = threadIdx.x; i < kMtgpN; i += blockDim.x) gstate[i] = s.ring[(n + i) & 1023];
+}
+
+// ---------------------------------------------------------------------------
+// Box-Muller on MTGP floats in [1,2) (boxmuller, pf_generic_soa.cu:481-500):
+// u1 = 2-x, u2 = 2-y in (0,1]; z = sqrt(-2 ln u1) (cos 2 pi u2, sin 2 pi u2).
+// sincospif evaluates the angle as pi*(2 u2) without rounding 2 pi u2 first.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void box_muller(float x, float y, float& z1, float& z2)
+{
+    const float u1 = 2.0f - x, u2 = 2.0f - y;
+    const float r = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    z1 = r * c;
+    z2 = r * s;
+}
+
+// ---------------------------------------------------------------------------
+// Descending bitonic key+index sort of M keys, E consecutive keys per thread
+// (thread t holds positions E*t .. E*t+E-1).  The comparator network is the
+// reference's (bitonic-sort.cu:28-61 with dir = 0): for every (size, stride)
+// the pair (p, p+stride) with p & stride == 0 swaps iff
+// (key[p] > key[p+stride]) == ((p & size) != 0), so equal keys swap.
+// Strides below E are register pairs, strides below 32E are warp shuffles,
+// longer strides go through shared memory (sk/si hold M entries).
+// ---------------------------------------------------------------------------
+template <int M, int E>
+__device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si)
+{
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int size = 2; size <= M; size <<= 1) {
+#pragma unroll
+        for (int stride = size / 2; stride > 0; stride >>= 1) {
+            if (stride < E) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if ((e & stride) == 0) {
+                        const int p = E * tid + e;
+                        const bool ddd = (p & size) != 0;
+                        const float a = k[e], b = k[e + stride];
+                        if ((a > b) == ddd) {
+                            k[e] = b;
+                            k[e + stride] = a;
+                            const int t = ix[e];
+                            ix[e] = ix[e + stride];
+                            ix[e + stride] = t;
+                        }
+                    }
+                }
+            } else if (stride < 32 * E) {
+                const int lm = stride / E;
+                const bool upper = (tid & lm) != 0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float ok = __shfl_xor_sync(kFull, k[e], lm);
+                    const int oi = __shfl_xor_sync(kFull, ix[e], lm);
+                    const int p = E * tid + e;
+                    const bool ddd = (p & size) != 0;
+                    const float lo = upper ? ok : k[e];
+                    const float hi = upper ? k[e] : ok;
+                    if ((lo > hi) == ddd) {
+                        k[e] = ok;
+                        ix[e] = oi;
+                    }
+                }
+            } else {
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    sk[E * tid + e] = k[e];
+                    si[E * tid + e] = ix[e];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int p = E * tid + e;
+                    const int q = p ^ stride;
+                    const float ok = sk[q];
+                    const int oi = si[q];
+                    const bool ddd = (p & size) != 0;
+                    const bool upper = (p & stride) != 0;
+                    const float lo = upper ? ok : k[e];
+                    const float hi = upper ? k[e] : ok;
+                    if ((lo > hi) == ddd) {
+                        k[e] = ok;
+                        ix[e] = oi;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Block reductions / scans.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float block_max(float v, float* red)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    float r = red[0];
+    for (int i = 1; i < nw; ++i) r = fmaxf(r, red[i]);
+    return r;
+}
+
+// Canonical FP64 inclusive scan (the oracle's orc_scan_f64): each thread sums
+// its E weights sequentially, lanes combine with a Kogge-Stone scan, warp
+// totals with a second Kogge-Stone scan; cum[] receives M inclusive sums.
+// Returns the total.  red needs 32 doubles.
+template <int M, int E>
+__device__ __forceinline__ double scan_f64(const float (&w)[E], double* cum, double* red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    constexpr int NW = (M / E + 31) / 32;
+    double tt = (double)w[0];
+#pragma unroll
+    for (int e = 1; e < E; ++e) tt = tt + (double)w[e];
+    double inc = tt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(kFull, inc, d);
+        if (lane >= d) inc = inc + o;
+    }
+    double ex = __shfl_up_sync(kFull, inc, 1);
+    if (lane == 0) ex = 0.0;
+    __syncthreads();
+    if (lane == 31) red[wp] = inc;
+    __syncthreads();
+    if (wp == 0) {
+        double v = lane < NW ? red[lane] : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double o = __shfl_up_sync(kFull, v, d);
+            if (lane >= d) v = v + o;
+        }
+        __syncwarp();
+        if (lane < NW) red[lane] = v;  // inclusive warp prefix
+    }
+    __syncthreads();
+    const double base = (wp == 0 ? 0.0 : red[wp - 1]) + ex;
+    double c = base + (double)w[0];
+    cum[E * tid] = c;
+#pragma unroll
+    for (int e = 1; e < E; ++e) {
+        c = c + (double)w[e];
+        cum[E * tid + e] = c;
+    }
+    __syncthreads();
+    return cum[M - 1];
+}
+
+// Number of cum[] entries <= x (upper bound), clamped to M-1.
+template <int M>
+__device__ __forceinline__ int upper_count(const double* cum, double x)
+{
+    int lo = 0, hi = M;
+#pragma unroll
+    for (int it = 0; it < 11; ++it) {
+        if (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cum[mid] <= x) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    return lo < M ? lo : M - 1;
+}
+
+// FP32 Blelloch exclusive scan of M values in place (prefix_sum,
+// pf_generic_soa.cu:169-216); same tree, pairs shared out over the block.
+template <int M>
+__device__ __forceinline__ float blelloch_scan(float* e)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int offset = 1;
+    for (int d = M / 2; d > 0; d /= 2) {
+        __syncthreads();
+        for (int q = tid; q < d; q += nt) {
+            const int ai = offset * (2 * q + 1) - 1, bi = offset * (2 * q + 2) - 1;
+            e[bi] += e[ai];
+        }
+        offset *= 2;
+    }
+    __syncthreads();
+    const float cum = e[M - 1];
+    __syncthreads();
+    if (tid == 0) e[M - 1] = 0.0f;
+    for (int d = 1; d < M; d *= 2) {
+        offset /= 2;
+        __syncthreads();
+        for (int q = tid; q < d; q += nt) {
+            const int ai = offset * (2 * q + 1) - 1, bi = offset * (2 * q + 2) - 1;
+            const float t = e[ai];
+            e[ai] = e[bi];
+            e[bi] += t;
+        }
+    }
+    __syncthreads();
+    return cum;
+}
+
+// binary_search, pf_generic_soa.cu:221-240: last i with hay[i] <= needle.
+__device__ __forceinline__ int ref_binary_search(const float* hay, float needle, int size)
+{
+    int lo = 0, hi = size - 1;
+    do {
+        const int cur = lo + (hi - lo + 1) / 2;
+        if (hay[cur] > needle) hi = cur - 1;
+        else lo = cur;
+    } while (lo < hi);
+    return lo;
+}
+
+// Block-wide exclusive count of `flag` in ascending rank order where rank =
+// tid + nt*round; returns this thread's exclusive count, *total the sum.
+// red needs 33 ints.  Contains barriers: every thread must call.
+__device__ __forceinline__ int block_excl_count(bool flag, int* red, int* total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, nw = blockDim.x >> 5;
+    const unsigned b = __ballot_sync(kFull, flag);
+    const int in_warp = __popc(b & ((1u << lane) - 1u));
+    __syncthreads();
+    if (lane == 0) red[wp] = __popc(b);
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int i = 0; i < nw; ++i) {
+        const int c = red[i];
+        if (i < wp) before += c;
+        tot += c;
+    }
+    *total = tot;
+    return before + in_warp;
+}
+
+// Vose alias table of M weights (resampling-valias.cl:85-195 + 262-270) in
+// FP32 with the reference's arithmetic: sum_reduce4 order, p = w/sum (or
+// 1/M), prob = p*M, small iff prob <= 1, pairing prob_L = (prob_L + prob_S) - 1.
+// Work lists are filled in ascending slot order where the reference uses
+// atomic_inc / atomic_dec (the oracle does the same).  Shared: prob[M],
+// alias[M], sl[M], scratch[M] floats, red[33].
+template <int M, int E>
+__device__ void vose_build(const float (&w)[E], float* prob, unsigned* alias, unsigned* sl,
+                           float* scratch, int* red)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+#pragma unroll
+    for (int e = 0; e < E; ++e) scratch[E * tid + e] = w[e];
+    __syncthreads();
+    // sum_reduce4
+    int offset = M;
+    while (offset > 2) {
+        offset >>= 2;
+        for (int l = tid; l < offset; l += nt) {
+            const float x = scratch[l + offset] + scratch[l + offset + offset] + scratch[l + offset + offset + offset];
+            scratch[l] = scratch[l] + x;
+        }
+        __syncthreads();
+    }
+    if (offset > 1) {
+        if (tid == 0) scratch[0] = scratch[0] + scratch[1];
+        __syncthreads();
+    }
+    const float sum = scratch[0];
+    // normalise, scale, initial split (small ascending from 0, large descending from M-1)
+    int ns_before = 0;
+    for (int e = 0; e < E; ++e) {
+        const int i = E * tid + e;
+        float p = w[e];
+        if (sum > 0.0f) p = p / sum;
+        else p = 1.0f / (float)M;
+        prob[i] = p * (float)M;
+        alias[i] = (unsigned)i;
+    }
+    // ascending i = E*tid + e: count smalls of lower threads, then within thread
+    int my_small = 0;
+    bool fl[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        fl[e] = prob[E * tid + e] <= 1.0f;
+        my_small += fl[e] ? 1 : 0;
+    }
+    {
+        // exclusive scan of my_small over threads (ascending tid)
+        const int lane = tid & 31, wp = tid >> 5, nw = nt >> 5;
+        int inc = my_small;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(kFull, inc, d);
+            if (lane >= d) inc += o;
+        }
+        __syncthreads();
+        if (lane == 31) red[wp] = inc;
+        __syncthreads();
+        int wbase = 0, tot = 0;
+        for (int i = 0; i < nw; ++i) {
+            if (i < wp) wbase += red[i];
+            tot += red[i];
+        }
+        ns_before = wbase + inc - my_small;
+        int nl_before = E * tid - ns_before;
+        int s_i = ns_before, l_i = nl_before;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int i = E * tid + e;
+            if (fl[e]) sl[s_i++] = (unsigned)i;
+            else sl[M - 1 - (l_i++)] = (unsigned)i;
+        }
+        __syncthreads();
+        if (tid == 0) red[32] = tot;
+        __syncthreads();
+    }
+    unsigned small_end = (unsigned)red[32];
+    unsigned large_rend = small_end - 1u;  // = M-1 - n_large
+    unsigned small_begin = 0;
+    __syncthreads();
+    // pairing rounds; each round retires >= 1 small entry, so <= M rounds
+    for (int round = 0; round < M; ++round) {
+        const unsigned se = small_end;
+        const unsigned a = se - small_begin, b = (unsigned)M - se;
+        const unsigned nactive = a < b ? a : b;
+        if (nactive == 0) break;
+        large_rend += nactive;
+        constexpr int R = (M / 2 + 31) / 32 + 1;  // upper bound on items per thread
+        unsigned lidx[R];
+        float pS[R], pL[R];
+        int nitems = 0;
+        for (unsigned kk = tid, r = 0; kk < nactive && r < (unsigned)R; kk += nt, ++r) {
+            const unsigned sidx = sl[small_begin + kk];
+            lidx[r] = sl[se + kk];
+            pS[r] = prob[sidx];
+            alias[sidx] = lidx[r];
+            pL[r] = prob[lidx[r]];
+            nitems = (int)r + 1;
+        }
+        __syncthreads();
+        unsigned s_base = 0, l_base = 0;
+        const int rounds = (int)((nactive + nt - 1) / nt);
+        for (int r = 0; r < rounds; ++r) {
+            const unsigned kk = (unsigned)tid + (unsigned)r * nt;
+            const bool act = kk < nactive;
+            float nl = 0.0f;
+            bool small = false;
+            if (act && r < nitems) {
+                nl = (pL[r] + pS[r]) - 1.0f;
+                small = nl <= 1.0f;
+            }
+            int tot_s;
+            const int rank_s = block_excl_count(act && small, red, &tot_s);
+            int tot_l;
+            const int rank_l = block_excl_count(act && !small, red, &tot_l);
+            if (act) {
+                const unsigned dst = small ? small_end + s_base + (unsigned)rank_s
+                                           : large_rend - l_base - (unsigned)rank_l;
+                sl[dst] = lidx[r];
+                prob[lidx[r]] = nl;
+            }
+            s_base += (unsigned)tot_s;
+            l_base += (unsigned)tot_l;
+        }
+        small_end += s_base;
+        large_rend -= l_base;
+        small_begin += nactive;
+        __syncthreads();
+    }
+}
+
+// vose_alias_generate_next (resampling-valias.cl:198-202).
+template <int M>
+__device__ __forceinline__ unsigned vose_draw(const float* prob, const unsigned* alias, float ux, float uy)
+{
+    unsigned col = (unsigned)floorf(ux * (float)M);
+    if (col >= (unsigned)M) col = M - 1;
+    return (uy < prob[col]) ? col : alias[col];
+}
+
+// ---------------------------------------------------------------------------
+// Models.  Each provides S (state floats), K (normals per particle), NA
+// (angular state variables, reported as sin/cos for circular means),
+// prepare() (one thread, per-step constants) and step() (one particle:
+// propagate in place, return the FP32 log-likelihood, and sin/cos of the
+// angular variables of the new state).
+// ---------------------------------------------------------------------------
+union ModelParams {
+    pf_unicycle_params uni;
+    pf_dharm_params arm;
+    pf_refarm_params ref;
+};
+
+__device__ __forceinline__ float wrap_pi(float a) { return a - kTwoPi * floorf((a + kPi) * kInvTwoPi); }
+
+struct Unicycle {
+    static constexpr int S = 3, K = 3, NA = 1;
+    __host__ __device__ static constexpr int angle_var(int) { return 2; }
+    struct Consts {
+        float A, B, wd, sq0, sq1, sq2, isr, isb;
+        int L;
+        float lx[8], ly[8], rm[8], cb[8], sb[8];
+    };
+    // Exact-arc velocity model: x' = x + A cos th - B sin th, y' = y + A sin th + B cos th
+    // with A = v sin(w dt)/w, B = v (1 - cos(w dt))/w (straight-line limit as w -> 0).
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    {
+        const pf_unicycle_params& p = mp.uni;
+        const double dt = in.dt > 0.0f ? in.dt : p.dt;
+        const double v = in.control[0], w = in.control[1];
+        const double wd = w * dt;
+        double A, B;
+        if (fabs(wd) < 1e-4) {
+            A = v * dt * (1.0 - wd * wd / 6.0);
+            B = v * dt * (wd / 2.0);
+        } else {
+            A = v * sin(wd) / w;
+            B = v * (1.0 - cos(wd)) / w;
+        }
+        c.A = (float)A;
+        c.B = (float)B;
+        c.wd = (float)wd;
+        c.sq0 = p.sigma_q[0];
+        c.sq1 = p.sigma_q[1];
+        c.sq2 = p.sigma_q[2];
+        c.isr = 1.0f / p.sigma_range;
+        c.isb = 1.0f / p.sigma_bearing;
+        const int L = p.num_landmarks < 1 ? 1 : (p.num_landmarks > 8 ? 8 : p.num_landmarks);
+        c.L = L;
+        for (int j = 0; j < 8; ++j) {
+            c.lx[j] = p.landmarks[j][0];
+            c.ly[j] = p.landmarks[j][1];
+            c.rm[j] = j < L ? in.meas[j] : 0.0f;
+            const double bj = j < L ? (double)in.meas[L + j] : 0.0;
+            c.cb[j] = (float)cos(bj);
+            c.sb[j] = (float)sin(bj);
+        }
+    }
+    __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
+                                                 float* cs)
+    {
+        float st, ct;
+        __sincosf(s[2], &st, &ct);
+        const float nx = s[0] + c.A * ct - c.B * st + c.sq0 * n[0];
+        const float ny = s[1] + c.A * st + c.B * ct + c.sq1 * n[1];
+        const float nt = wrap_pi(s[2] + c.wd + c.sq2 * n[2]);
+        s[0] = nx;
+        s[1] = ny;
+        s[2] = nt;
+        float s2, c2;
+        __sincosf(nt, &s2, &c2);
+        sn[0] = s2;
+        cs[0] = c2;
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (j < c.L) {
+                const float dx = c.lx[j] - nx, dy = c.ly[j] - ny;
+                const float r = sqrtf(dx * dx + dy * dy);
+                const float er = (c.rm[j] - r) * c.isr;
+                const float cp = c2 * c.cb[j] - s2 * c.sb[j];
+                const float sp = s2 * c.cb[j] + c2 * c.sb[j];
+                const float eb = atan2f(sp * dx - cp * dy, cp * dx + sp * dy) * c.isb;
+                acc += er * er + eb * eb;
+            }
+        }
+        return -0.5f * acc;
+    }
+};
+
+struct DhArm {
+    static constexpr int S = 12, K = 6, NA = 6;
+    __host__ __device__ static constexpr int angle_var(int a) { return a; }
+    struct Consts {
+        float dt, sqd, isp, isa;
+        float a[6], d[6], ca[6], sa[6], z[6];
+    };
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    {
+        const pf_dharm_params& p = mp.arm;
+        c.dt = in.dt > 0.0f ? in.dt : p.dt;
+        c.sqd = p.sigma_qd;
+        c.isp = 1.0f / p.sigma_pos;
+        c.isa = 1.0f / p.sigma_ang;
+        for (int i = 0; i < 6; ++i) {
+            c.a[i] = p.a[i];
+            c.d[i] = p.d[i];
+            c.ca[i] = (float)cos((double)p.alpha[i]);
+            c.sa[i] = (float)sin((double)p.alpha[i]);
+            c.z[i] = in.meas[i];
+        }
+    }
+    __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
+                                                 float* cs)
+    {
+        float R00 = 1, R01 = 0, R02 = 0, R10 = 0, R11 = 1, R12 = 0, R20 = 0, R21 = 0, R22 = 1;
+        float p0 = 0, p1 = 0, p2 = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const float q = wrap_pi(s[i] + s[6 + i] * c.dt);
+            s[i] = q;
+            s[6 + i] = s[6 + i] + c.sqd * n[i];
+            float sq, cq;
+            __sincosf(q, &sq, &cq);
+            sn[i] = sq;
+            cs[i] = cq;
+            // A_i = [[c, -s ca, s sa, a c], [s, c ca, -c sa, a s], [0, sa, ca, d]]
+            const float a00 = cq, a01 = -sq * c.ca[i], a02 = sq * c.sa[i];
+            const float a10 = sq, a11 = cq * c.ca[i], a12 = -cq * c.sa[i];
+            const float a21 = c.sa[i], a22 = c.ca[i];
+            const float t0 = c.a[i] * cq, t1 = c.a[i] * sq, t2 = c.d[i];
+            const float n00 = R00 * a00 + R01 * a10, n01 = R00 * a01 + R01 * a11 + R02 * a21,
+                        n02 = R00 * a02 + R01 * a12 + R02 * a22;
+            const float n10 = R10 * a00 + R11 * a10, n11 = R10 * a01 + R11 * a11 + R12 * a21,
+                        n12 = R10 * a02 + R11 * a12 + R12 * a22;
+            const float n20 = R20 * a00 + R21 * a10, n21 = R20 * a01 + R21 * a11 + R22 * a21,
+                        n22 = R20 * a02 + R21 * a12 + R22 * a22;
+            p0 = R00 * t0 + R01 * t1 + R02 * t2 + p0;
+            p1 = R10 * t0 + R11 * t1 + R12 * t2 + p1;
+            p2 = R20 * t0 + R21 * t1 + R22 * t2 + p2;
+            R00 = n00; R01 = n01; R02 = n02;
+            R10 = n10; R11 = n11; R12 = n12;
+            R20 = n20; R21 = n21; R22 = n22;
+        }
+        const float yaw = atan2f(R10, R00);
+        const float pitch = atan2f(-R20, sqrtf(R21 * R21 + R22 * R22));
+        const float roll = atan2f(R21, R22);
+        const float e0 = (c.z[0] - p0) * c.isp, e1 = (c.z[1] - p1) * c.isp, e2 = (c.z[2] - p2) * c.isp;
+        float d3 = c.z[3] - yaw, d4 = c.z[4] - pitch, d5 = c.z[5] - roll;
+        d3 = (d3 - kTwoPi * rintf(d3 * kInvTwoPi)) * c.isa;
+        d4 = (d4 - kTwoPi * rintf(d4 * kInvTwoPi)) * c.isa;
+        d5 = (d5 - kTwoPi * rintf(d5 * kInvTwoPi)) * c.isa;
+        return -0.5f * (e0 * e0 + e1 * e1 + e2 * e2 + d3 * d3 + d4 * d4 + d5 * d5);
+    }
+};
+
+// The reference's camera robot arm (sampling_iw, src/models/robotarm/cuda/
+// pf_model_soa.cuh:114-184): state angles[5], x, y, vX, vY; normals in the
+// same variable order; log weight = -(sum 0.1 e^2) (the reference returns its exp).
+struct RefArm {
+    static constexpr int S = 9, K = 9, NA = 5;
+    __host__ __device__ static constexpr int angle_var(int a) { return a; }
+    struct Consts {
+        float dt;
+        float cdt[5];
+        float z[7];
+    };
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    {
+        c.dt = in.dt > 0.0f ? in.dt : mp.ref.dt;
+        for (int i = 0; i < 5; ++i) c.cdt[i] = in.control[i] * c.dt;
+        for (int i = 0; i < 7; ++i) c.z[i] = in.meas[i];
+    }
+    __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
+                                                 float* cs)
+    {
+        const float arm[5] = {0.0f, 3.0f, 3.0f, 3.0f, 3.0f};
+        const float vX = s[7], vY = s[8];
+        const float x = s[5] + vX * c.dt + n[5] * 0.2f;
+        const float y = s[6] + vY * c.dt + n[6] * 0.2f;
+        s[5] = x;
+        s[6] = y;
+        s[7] = vX + n[7] * 2.0f;
+        s[8] = vY + n[8] * 2.0f;
+        float value = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            const float ang = s[i] + c.cdt[i] + n[i] * 0.2f;
+            s[i] = ang;
+            float sf, cf;
+            __sincosf(ang, &sf, &cf);
+            sn[i] = sf;
+            cs[i] = cf;
+            if (i == 0) {
+                cx = x * cf + y * sf;
+                cy = -x * sf + y * cf;
+                cz = 0.0f;
+            } else {
+                const float nb = cy * cf - cz * sf, nc = cy * sf + cz * cf;
+                cy = nb;
+                cz = nc - arm[i];
+            }
+            const float e = ang - c.z[i];
+            value += e * e * 0.1f;
+        }
+        value += (cx - c.z[5]) * (cx - c.z[5]) * 0.1f;
+        value += (cy - c.z[6]) * (cy - c.z[6]) * 0.1f;
+        return -value;
+    }
+};
+
+template <class Mdl>
+__host__ __device__ constexpr bool is_angle_var(int v)
+{
+    for (int i = 0; i < Mdl::NA; ++i)
+        if (Mdl::angle_var(i) == v) return true;
+    return false;
+}
+
+}  // namespace pfdev

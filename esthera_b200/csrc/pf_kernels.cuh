@@ -1,0 +1,856 @@
+// pf_kernels.cuh -- kernels of the particle-filter step (sm_100a).
+//
+// Fused pipeline (the production path), per step:
+//   k_sample_sort      one CTA per sub-filter: MTGP32 stream -> Box-Muller in
+//                      shared memory -> propagate + log-weight (float2/float4
+//                      SoA loads) -> bitonic sort -> sorted state/keys,
+//                      winner, FP64 estimate partials
+//   k_a2a_merge        (all-to-all exchange only) global top-t of the sorted lists
+//   k_estimate         one CTA per filter: winner + FP64 posterior mean
+//   k_exchange_resample one CTA per sub-filter: neighbours' top-t into the
+//                      weakest slots, weights, resampling, gather, store
+// Phased pipeline (the reference's kernel sequence, pf_generic_soa.cu:842-1234):
+//   k_mtgp_blocks -> k_boxmuller -> k_sample_weight -> k_block_sort ->
+//   k_estimate -> k_exchange_inplace -> k_exchange_resample (no exchange)
+#pragma once
+
+#include "pf_device.cuh"
+
+namespace pfdev {
+
+constexpr int kPartStride = 32;  // doubles of estimate partials per sub-filter
+
+struct FilterDesc {
+    float* state;      // S*T SoA (var-major), propagated / resampled particles
+    float* tmp;        // S*T sorted (pre-exchange) particles
+    float* tkey;       // T sorted keys
+    float* key;        // T unsorted keys (phased pipeline)
+    float* winner;     // N best keys
+    double* part;      // N * kPartStride estimate partials
+    uint32_t* mtgp;    // MTGP32 stream words (351 per stream)
+    float* ru;         // per sub-filter resampling uniforms (fused RNG): decision, then resampler draws
+    const float* rbuf; // reference-layout random buffer: normals then uniforms
+    int32_t* a2a;      // all-to-all: t global slots of the global best
+    int32_t* sel;      // optional T selected slots
+    pf_estimate* est;  // estimate output (indexed by the step counter when one is used)
+    int64_t T;
+    int32_t N, M, t, exchange, resampler, dx, dy;
+    int32_t log_weights, inplace, rng_fused, draws, nbm, ru_stride;
+    uint32_t mask;
+    int32_t stream_base;
+    float freq;
+    int64_t nnorm;     // normals in rbuf before the uniforms (K*T)
+    ModelParams mp;
+};
+
+struct InputRef {
+    const pf_step_input* base;
+    int64_t filter_stride;   // inputs per filter (batched: [filter][step])
+    const int32_t* ctr;      // device step counter (graph replays) or null
+};
+
+template <int E>
+struct VecT;
+template <>
+struct VecT<1> { using T = float; };
+template <>
+struct VecT<2> { using T = float2; };
+template <>
+struct VecT<4> { using T = float4; };
+
+template <int E>
+__device__ __forceinline__ void ldv(const float* __restrict__ p, float (&o)[E])
+{
+    if constexpr (E == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    } else if constexpr (E == 2) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        o[0] = v.x; o[1] = v.y;
+    } else {
+        o[0] = *p;
+    }
+}
+template <int E>
+__device__ __forceinline__ void stv(float* __restrict__ p, const float (&o)[E])
+{
+    if constexpr (E == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+    } else if constexpr (E == 2) {
+        *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+    } else {
+        *p = o[0];
+    }
+}
+
+__device__ __forceinline__ void cta_target(const int2* __restrict__ cta_map, int& f, int& b)
+{
+    if (cta_map) {
+        const int2 c = cta_map[blockIdx.x];
+        f = c.x;
+        b = c.y;
+    } else {
+        f = 0;
+        b = blockIdx.x;
+    }
+}
+
+__device__ __forceinline__ const pf_step_input* input_of(const InputRef& in, int f)
+{
+    return in.base + (int64_t)f * in.filter_stride + (in.ctr ? *in.ctr : 0);
+}
+
+// Shared-memory footprint of k_sample_sort (dynamic part).
+template <class Mdl, int M, bool FR>
+constexpr size_t k1_smem()
+{
+    size_t s = 0;
+    if (FR) s += sizeof(MtgpSmem);
+    size_t nz = FR ? (size_t)(2 * ((Mdl::K * M + 1) / 2)) * 4 : 0;
+    size_t stage = (size_t)Mdl::S * M * 4;
+    s += nz > stage ? nz : stage;
+    s += (size_t)M * 8;  // sort keys + indices
+    return s;
+}
+
+// FP64 block sum of NV values per thread into out[0..NV) (thread 0 writes).
+template <int NV>
+__device__ __forceinline__ void block_sum_f64(double (&a)[NV], double* red, double* out)
+{
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_xor_sync(kFull, a[i], o);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) red[wp * NV + i] = a[i];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = red[threadIdx.x];
+        for (int w = 1; w < nw; ++w) s += red[w * NV + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+// Estimate partials of one sub-filter from particles in any order:
+// [0] key max, [1] sum w, [2+v] sum w x_v (angles: sum w sin), [2+S+a] sum w cos.
+template <class Mdl, int E>
+__device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float lmax,
+                                               const float (&okey)[E], const float (&st)[E][Mdl::S],
+                                               const float (&sn)[E][Mdl::NA], const float (&cs)[E][Mdl::NA],
+                                               double* red)
+{
+    constexpr int S = Mdl::S, NA = Mdl::NA, NV = 1 + S + NA;
+    double acc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const double w = D.log_weights ? (double)__expf(okey[e] - lmax) : (double)okey[e];
+        acc[0] += w;
+        int a = 0;
+#pragma unroll
+        for (int v = 0; v < S; ++v) {
+            if (is_angle_var<Mdl>(v)) {
+                acc[1 + v] += w * (double)sn[e][a];
+                acc[1 + S + a] += w * (double)cs[e][a];
+                ++a;
+            } else {
+                acc[1 + v] += w * (double)st[e][v];
+            }
+        }
+    }
+    double* out = D.part + (int64_t)b * kPartStride;
+    block_sum_f64<NV>(acc, red, out + 1);
+    if (threadIdx.x == 0) out[0] = (double)lmax;
+}
+
+// ---------------------------------------------------------------------------
+// Fused propagate + weight + sort.  FR: generate this sub-filter's MTGP32
+// stream in the kernel; otherwise read reference-layout normals from rbuf.
+// ---------------------------------------------------------------------------
+template <class Mdl, int M, int E, bool FR>
+__global__ void __launch_bounds__(M / E) k_sample_sort(const FilterDesc* __restrict__ descs,
+                                                       const int2* __restrict__ cta_map, InputRef in)
+{
+    constexpr int NT = M / E, S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
+    constexpr int NANG = NA > 0 ? NA : 1;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ typename Mdl::Consts cst;
+    __shared__ double red[(NT / 32) * (1 + S + NANG)];
+    __shared__ float s_lmax;
+    int f, b;
+    cta_target(cta_map, f, b);
+    const FilterDesc& D = descs[f];
+    const int tid = threadIdx.x;
+    const int64_t T = D.T;
+    const int64_t base = (int64_t)b * M + E * tid;
+
+    unsigned char* p = smem;
+    MtgpSmem* ms = nullptr;
+    if constexpr (FR) {
+        ms = reinterpret_cast<MtgpSmem*>(p);
+        p += sizeof(MtgpSmem);
+    }
+    float* nz = reinterpret_cast<float*>(p);     // normals (FR), later the state stage
+    float* stage = nz;
+    {
+        size_t a = FR ? (size_t)(2 * ((K * M + 1) / 2)) * 4 : 0, c = (size_t)S * M * 4;
+        p += a > c ? a : c;
+    }
+    float* sk = reinterpret_cast<float*>(p);
+    int* si = reinterpret_cast<int*>(p + (size_t)M * 4);
+
+    if (tid == 0) Mdl::prepare(cst, *input_of(in, f), D.mp);
+    if constexpr (FR) {
+        uint32_t* gst = D.mtgp + (int64_t)b * kMtgpN;
+        mtgp_load(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, true);
+        const int nbm = D.nbm;
+        float* ru = D.ru + (int64_t)b * D.ru_stride;
+        mtgp_generate(*ms, D.draws, true, [&](int k, uint32_t o) {
+            if (k < nbm) nz[k] = __uint_as_float(o);
+            else ru[k - nbm] = __uint_as_float(o);
+        });
+        mtgp_store(*ms, gst, D.draws);
+        for (int q = tid; q < nbm / 2; q += NT) {
+            float z1, z2;
+            box_muller(nz[2 * q], nz[2 * q + 1], z1, z2);
+            nz[2 * q] = z1;
+            nz[2 * q + 1] = z2;
+        }
+    }
+    __syncthreads();
+
+    float st[E][S];
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+        ldv<E>(D.state + v * T + base, o);
+#pragma unroll
+        for (int e = 0; e < E; ++e) st[e][v] = o[e];
+    }
+    float okey[E], sn[E][NANG], cs[E][NANG];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        float n[K];
+#pragma unroll
+        for (int v = 0; v < K; ++v)
+            n[v] = FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e];
+        const float ll = Mdl::step(cst, st[e], n, sn[e], cs[e]);
+        okey[e] = D.log_weights ? ll : __expf(ll);
+    }
+    if (D.inplace) {
+#pragma unroll
+        for (int v = 0; v < S; ++v) {
+            float o[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) o[e] = st[e][v];
+            stv<E>(D.state + v * T + base, o);
+        }
+    }
+    float k[E];
+    int ix[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        k[e] = okey[e];
+        ix[e] = E * tid + e;
+    }
+    bitonic_sort_desc<M, E>(k, ix, sk, si);
+    stv<E>(D.tkey + base, k);
+    __syncthreads();  // normals consumed, sort buffers free: stage the state
+#pragma unroll
+    for (int v = 0; v < S; ++v)
+#pragma unroll
+        for (int e = 0; e < E; ++e) stage[v * M + E * tid + e] = st[e][v];
+    if (tid == 0) {
+        D.winner[b] = k[0];
+        s_lmax = k[0];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
+        stv<E>(D.tmp + v * T + base, o);
+    }
+    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs, red);
+}
+
+// ---------------------------------------------------------------------------
+// Phased pipeline: propagate + weight only (sampling_importance,
+// pf_generic_soa.cu:245-287): state in place, unsorted keys.
+// ---------------------------------------------------------------------------
+template <class Mdl, int M, int E>
+__global__ void __launch_bounds__(M / E) k_sample_weight(const FilterDesc* __restrict__ descs,
+                                                         const int2* __restrict__ cta_map, InputRef in)
+{
+    constexpr int S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
+    constexpr int NANG = NA > 0 ? NA : 1;
+    __shared__ typename Mdl::Consts cst;
+    int f, b;
+    cta_target(cta_map, f, b);
+    const FilterDesc& D = descs[f];
+    const int tid = threadIdx.x;
+    const int64_t T = D.T;
+    const int64_t base = (int64_t)b * M + E * tid;
+    if (tid == 0) Mdl::prepare(cst, *input_of(in, f), D.mp);
+    __syncthreads();
+    float st[E][S];
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+        ldv<E>(D.state + v * T + base, o);
+#pragma unroll
+        for (int e = 0; e < E; ++e) st[e][v] = o[e];
+    }
+    float key[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        float n[K], sn[NANG], cs[NANG];
+#pragma unroll
+        for (int v = 0; v < K; ++v) n[v] = D.rbuf[v * T + base + e];
+        const float ll = Mdl::step(cst, st[e], n, sn, cs);
+        key[e] = D.log_weights ? ll : __expf(ll);
+    }
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) o[e] = st[e][v];
+        stv<E>(D.state + v * T + base, o);
+    }
+    stv<E>(D.key + base, key);
+}
+
+// Phased pipeline: block_sort (pf_generic_soa.cu:289-323) + estimate partials.
+template <class Mdl, int M, int E>
+__global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restrict__ descs,
+                                                      const int2* __restrict__ cta_map)
+{
+    constexpr int NT = M / E, S = Mdl::S, NA = Mdl::NA;
+    constexpr int NANG = NA > 0 ? NA : 1;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double red[(NT / 32) * (1 + S + NANG)];
+    __shared__ float s_lmax;
+    int f, b;
+    cta_target(cta_map, f, b);
+    const FilterDesc& D = descs[f];
+    const int tid = threadIdx.x;
+    const int64_t T = D.T;
+    const int64_t base = (int64_t)b * M + E * tid;
+    float* stage = reinterpret_cast<float*>(smem);
+    float* sk = stage + (size_t)S * M;
+    int* si = reinterpret_cast<int*>(sk + M);
+    float st[E][S], okey[E], sn[E][NANG], cs[E][NANG];
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+        ldv<E>(D.state + v * T + base, o);
+#pragma unroll
+        for (int e = 0; e < E; ++e) st[e][v] = o[e];
+    }
+    ldv<E>(D.key + base, okey);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) __sincosf(st[e][Mdl::angle_var(a)], &sn[e][a], &cs[e][a]);
+    float k[E];
+    int ix[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        k[e] = okey[e];
+        ix[e] = E * tid + e;
+    }
+    bitonic_sort_desc<M, E>(k, ix, sk, si);
+    stv<E>(D.tkey + base, k);
+#pragma unroll
+    for (int v = 0; v < S; ++v)
+#pragma unroll
+        for (int e = 0; e < E; ++e) stage[v * M + E * tid + e] = st[e][v];
+    if (tid == 0) {
+        D.winner[b] = k[0];
+        s_lmax = k[0];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
+        stv<E>(D.tmp + v * T + base, o);
+    }
+    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs, red);
+}
+
+// ---------------------------------------------------------------------------
+// Exchange routing: the global slot (within the filter) that receiving slot
+// M-1-x of sub-filter b takes, x < t (ring, all-to-all) or x < 4t (torus).
+// ring: exchange_ring (pf_generic_soa.cu:400-413); torus: exchange_2dtorus
+// (pf_generic.cu:352-393) with receiver slots m-1-j-k*t, k = sender's
+// direction L,R,T,B; all-to-all: pf_generic2_all2all.cu:404-419.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t exchange_source(const FilterDesc& D, int b, int x)
+{
+    const int M = D.M, N = D.N, t = D.t;
+    if (D.exchange == PF_EXCHANGE_RING) return (int64_t)((b - 1 + N) % N) * M + x;
+    if (D.exchange == PF_EXCHANGE_ALL2ALL) return D.a2a[x];
+    const int k = x / t, j = x - k * t;
+    const int dx = D.dx, dy = D.dy;
+    const int cx = b % dx, cy = b / dx;
+    int from;
+    if (k == 0) from = cy * dx + (cx + 1) % dx;            // right neighbour sent "left"
+    else if (k == 1) from = cy * dx + (cx - 1 + dx) % dx;  // left neighbour sent "right"
+    else if (k == 2) from = ((cy + 1) % dy) * dx + cx;     // bottom neighbour sent "top"
+    else from = ((cy - 1 + dy) % dy) * dx + cx;            // top neighbour sent "bottom"
+    return (int64_t)from * M + j;
+}
+
+__device__ __forceinline__ int exchange_count(const FilterDesc& D)
+{
+    if (D.exchange == PF_EXCHANGE_NONE || D.t <= 0) return 0;
+    return D.exchange == PF_EXCHANGE_TORUS ? 4 * D.t : D.t;
+}
+
+// Slot sources of every sub-filter (identity where no particle arrives).
+static __global__ void k_exchange_sources(const FilterDesc* __restrict__ d, int32_t* __restrict__ src)
+{
+    const FilterDesc& D = *d;
+    const int b = blockIdx.x;
+    const int nx = exchange_count(D);
+    for (int s = threadIdx.x; s < D.M; s += blockDim.x) {
+        const int x = D.M - 1 - s;
+        src[(int64_t)b * D.M + s] = (int32_t)(x < nx ? exchange_source(D, b, x) : (int64_t)b * D.M + s);
+    }
+}
+
+// Phased pipeline: copy the exchanged particles into the receivers' weakest
+// slots of tmp/tkey (reads slots [0,t), writes [M-4t, M): disjoint by the
+// create-time constraint, so the in-place copy equals the out-of-place one).
+template <int S>
+__global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const int2* __restrict__ cta_map)
+{
+    int f, b;
+    cta_target(cta_map, f, b);
+    const FilterDesc& D = descs[f];
+    const int nx = exchange_count(D);
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        const int64_t g = exchange_source(D, b, x);
+        const int64_t d = (int64_t)b * D.M + D.M - 1 - x;
+        const float kk = D.tkey[g];
+        float v[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = D.tmp[s * D.T + g];
+        D.tkey[d] = kk;
+#pragma unroll
+        for (int s = 0; s < S; ++s) D.tmp[s * D.T + d] = v[s];
+    }
+}
+
+// All-to-all: the t best of all sub-filters' sorted top-t lists, ties to the
+// lower (sub-filter, rank) -- a stable descending sort of the candidates, as
+// thrust::sort_by_key(greater) gives (pf_generic2_all2all.cu:1007).
+static __global__ void k_a2a_merge(const FilterDesc* __restrict__ descs)
+{
+    const FilterDesc& D = descs[blockIdx.x];
+    constexpr int R = 8;  // sub-filters per thread (N <= 8 * blockDim)
+    __shared__ float sk[32];
+    __shared__ int so[32];
+    __shared__ int s_win;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5;
+    int head[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) head[r] = 0;
+    for (int j = 0; j < D.t; ++j) {
+        float bk = -INFINITY;
+        int bo = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int sb = tid + r * nt;
+            if (sb < D.N && head[r] < D.t) {
+                const float kk = D.tkey[(int64_t)sb * D.M + head[r]];
+                const int ord = sb * D.t + head[r];
+                if (kk > bk || (kk == bk && ord < bo)) {
+                    bk = kk;
+                    bo = ord;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ok = __shfl_xor_sync(kFull, bk, o);
+            const int oo = __shfl_xor_sync(kFull, bo, o);
+            if (ok > bk || (ok == bk && oo < bo)) {
+                bk = ok;
+                bo = oo;
+            }
+        }
+        if (lane == 0) {
+            sk[wp] = bk;
+            so[wp] = bo;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float k2 = sk[0];
+            int o2 = so[0];
+            for (int w = 1; w < nt / 32; ++w)
+                if (sk[w] > k2 || (sk[w] == k2 && so[w] < o2)) {
+                    k2 = sk[w];
+                    o2 = so[w];
+                }
+            s_win = o2;
+            const int sbw = o2 / D.t, rank = o2 - sbw * D.t;
+            D.a2a[j] = sbw * D.M + rank;
+        }
+        __syncthreads();
+        const int win = s_win;
+        const int sbw = win / D.t;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (tid + r * nt == sbw) head[r]++;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Global winner (first maximum) + FP64 posterior mean, one CTA per filter.
+// ---------------------------------------------------------------------------
+template <int S>
+__global__ void k_estimate(const FilterDesc* __restrict__ descs, InputRef in, uint32_t angle_mask)
+{
+    const FilterDesc& D = descs[blockIdx.x];
+    if (!D.est) return;
+    __shared__ float wk[32];
+    __shared__ int wb[32];
+    __shared__ double dr[32][S + 2 + S];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5, nw = nt / 32;
+    float bk = -INFINITY;
+    int bb = 0x7fffffff;
+    double gmax = -INFINITY;
+    for (int b = tid; b < D.N; b += nt) {
+        const float kk = D.winner[b];
+        if (kk > bk || (kk == bk && b < bb)) {
+            bk = kk;
+            bb = b;
+        }
+        gmax = fmax(gmax, D.part[(int64_t)b * kPartStride]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ok = __shfl_xor_sync(kFull, bk, o);
+        const int ob = __shfl_xor_sync(kFull, bb, o);
+        if (ok > bk || (ok == bk && ob < bb)) {
+            bk = ok;
+            bb = ob;
+        }
+        gmax = fmax(gmax, __shfl_xor_sync(kFull, gmax, o));
+    }
+    if (lane == 0) {
+        wk[wp] = bk;
+        wb[wp] = bb;
+        dr[wp][0] = gmax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < nw; ++w) {
+            if (wk[w] > wk[0] || (wk[w] == wk[0] && wb[w] < wb[0])) {
+                wk[0] = wk[w];
+                wb[0] = wb[w];
+            }
+            dr[0][0] = fmax(dr[0][0], dr[w][0]);
+        }
+    }
+    __syncthreads();
+    const int best = wb[0];
+    const double gm = D.log_weights ? dr[0][0] : 0.0;
+    __syncthreads();
+    constexpr int NV = 1 + S + S;
+    double acc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+    for (int b = tid; b < D.N; b += nt) {
+        const double* pp = D.part + (int64_t)b * kPartStride;
+        const double sc = D.log_weights ? exp(pp[0] - gm) : 1.0;
+        acc[0] += sc * pp[1];
+        int a = 0;
+#pragma unroll
+        for (int v = 0; v < S; ++v) {
+            acc[1 + v] += sc * pp[2 + v];
+            if ((angle_mask >> v) & 1u) {
+                acc[1 + S + v] += sc * pp[2 + S + a];
+                ++a;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(kFull, acc[i], o);
+    if (lane == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) dr[wp][i] = acc[i];
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < nw; ++w)
+            for (int i = 0; i < NV; ++i) dr[0][i] += dr[w][i];
+        const int64_t idx = in.ctr ? *in.ctr : 0;
+        pf_estimate& E = D.est[idx];
+        const double W = dr[0][0];
+        for (int v = 0; v < PF_MAX_STATE; ++v) E.mean[v] = 0.0;
+        for (int v = 0; v < S; ++v)
+            E.mean[v] = ((angle_mask >> v) & 1u) ? atan2(dr[0][1 + v], dr[0][1 + S + v]) : dr[0][1 + v] / W;
+        E.log_norm = gm + log(W);
+        for (int v = 0; v < PF_MAX_STATE; ++v) E.best[v] = v < S ? D.tmp[v * D.T + (int64_t)best * D.M] : 0.0f;
+        E.best_key = wk[0];
+        E.best_subfilter = best;
+        E.step = (int32_t)idx + 1;
+        E.flags = (isfinite(gm) && isfinite(W) && W > 0.0) ? 0 : 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exchange + resample + gather, one CTA per sub-filter.  `virt`: apply the
+// exchange virtually (read the neighbours' slots straight from tmp).
+// Resampling restates resampling (pf_generic_soa.cu:415-453) for
+// PF_RESAMPLE_REFERENCE, resampling_valias (resampling-valias.cl:214-300)
+// for PF_RESAMPLE_VOSE; PF_RESAMPLE_SYSTEMATIC uses the FP64 scan.
+// ---------------------------------------------------------------------------
+template <int S, int M, int E, int RES>
+constexpr size_t k2_smem()
+{
+    size_t s = (size_t)M * 4 + (size_t)S * M * 4;  // keys + state tile
+    if (RES == PF_RESAMPLE_SYSTEMATIC) s += (size_t)M * 8;
+    else if (RES == PF_RESAMPLE_REFERENCE) s += (size_t)M * 4;
+    else s += (size_t)M * 16;  // prob, alias, work list, scratch
+    return s;
+}
+
+template <int S, int M, int E, int RES>
+__global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* __restrict__ descs,
+                                                             const int2* __restrict__ cta_map,
+                                                             int32_t* step_ctr, int virt)
+{
+    constexpr int NT = M / E;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double dred[33];
+    __shared__ int ired[34];
+    int f, b;
+    cta_target(cta_map, f, b);
+    const FilterDesc& D = descs[f];
+    const int tid = threadIdx.x;
+    if (step_ctr && blockIdx.x == 0 && tid == 0) *step_ctr += 1;
+    const int64_t T = D.T;
+    const int64_t base = (int64_t)b * M + E * tid;
+    const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;
+    const float dec = (D.rng_fused ? U[0] : U[T + b]) - 1.0f;
+    if (dec > D.freq) {
+        if (D.sel) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) D.sel[base + e] = -1;
+        }
+        return;  // the propagated state was written in place by the sampling kernel
+    }
+    float* kb = reinterpret_cast<float*>(smem);
+    float* tile = kb + M;
+    unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
+    {
+        float o[E];
+        ldv<E>(D.tkey + base, o);
+#pragma unroll
+        for (int e = 0; e < E; ++e) kb[E * tid + e] = o[e];
+#pragma unroll
+        for (int v = 0; v < S; ++v) {
+            ldv<E>(D.tmp + v * T + base, o);
+#pragma unroll
+            for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = o[e];
+        }
+    }
+    __syncthreads();
+    if (virt) {
+        const int nx = exchange_count(D);
+        for (int x = tid; x < nx; x += NT) {
+            const int64_t g = exchange_source(D, b, x);
+            const int s = M - 1 - x;
+            kb[s] = D.tkey[g];
+#pragma unroll
+            for (int v = 0; v < S; ++v) tile[v * M + s] = D.tmp[v * T + g];
+        }
+        __syncthreads();
+    }
+    float w[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) w[e] = kb[E * tid + e];
+    if (D.log_weights) {
+        float mx = w[0];
+#pragma unroll
+        for (int e = 1; e < E; ++e) mx = fmaxf(mx, w[e]);
+        mx = block_max(mx, reinterpret_cast<float*>(ired));
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = __expf(w[e] - mx);
+    }
+    int sel[E];
+    if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
+        double* cum = reinterpret_cast<double*>(scratch);
+        const double tot = scan_f64<M, E>(w, cum, dred);
+        const float u0 = (D.rng_fused ? U[1] : U[(int64_t)b * M]) - 1.0f;
+        const double step = tot / (double)M;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const double pos = ((double)u0 + (double)(E * tid + e)) * step;
+            sel[e] = upper_count<M>(cum, pos);
+        }
+    } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
+        float* ex = reinterpret_cast<float*>(scratch);
+#pragma unroll
+        for (int e = 0; e < E; ++e) ex[E * tid + e] = w[e];
+        const float tot = blelloch_scan<M>(ex);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int i = E * tid + e;
+            const float u = D.rng_fused ? U[1 + i] : U[(int64_t)b * M + i];
+            sel[e] = ref_binary_search(ex, (u - 1.0f) * tot, M);
+        }
+    } else {
+        float* prob = reinterpret_cast<float*>(scratch);
+        unsigned* alias = reinterpret_cast<unsigned*>(prob + M);
+        unsigned* sl = alias + M;
+        float* scr = reinterpret_cast<float*>(sl + M);
+        vose_build<M, E>(w, prob, alias, sl, scr, ired);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int64_t i = E * tid + e;
+            const float ux = (D.rng_fused ? U[1 + 2 * i] : U[2 * ((int64_t)b * M + i)]) - 1.0f;
+            const float uy = (D.rng_fused ? U[2 + 2 * i] : U[2 * ((int64_t)b * M + i) + 1]) - 1.0f;
+            sel[e] = (int)vose_draw<M>(prob, alias, ux, uy);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < S; ++v) {
+        float o[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) o[e] = tile[v * M + sel[e]];
+        stv<E>(D.state + v * T + base, o);
+    }
+    if (D.sel) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) D.sel[base + e] = sel[e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RNG in the reference block layout.
+// ---------------------------------------------------------------------------
+// Stream g (parameter set g % 200) writes out[g*size + i] (mtgp32_single_kernel).
+static __global__ void __launch_bounds__(256) k_mtgp_blocks(uint32_t* __restrict__ states, uint32_t* __restrict__ out,
+                                                     int64_t size, uint32_t mask, int float_out, int set_base)
+{
+    __shared__ MtgpSmem ms;
+    const int g = blockIdx.x;
+    uint32_t* gst = states + (int64_t)g * kMtgpN;
+    mtgp_load(ms, gst, (set_base + g) % kMtgpSets, mask, float_out != 0);
+    uint32_t* o = out + (int64_t)g * size;
+    // size may exceed INT_MAX only in absurd configurations; the host bounds it.
+    mtgp_generate(ms, (int)size, float_out != 0, [&](int k, uint32_t w) { o[k] = w; });
+    mtgp_store(ms, gst, (int)size);
+}
+
+// In-place Box-Muller over pairs (2i, 2i+1) with 2i < n.
+static __global__ void k_boxmuller(float* __restrict__ data, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * i < n) {
+        float2 v = reinterpret_cast<float2*>(data)[i];
+        float z1, z2;
+        box_muller(v.x, v.y, z1, z2);
+        reinterpret_cast<float2*>(data)[i] = make_float2(z1, z2);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel-level test entry points (one CTA per sub-filter).
+// ---------------------------------------------------------------------------
+template <int M, int E>
+__global__ void __launch_bounds__(M / E) k_test_sort(float* keys, int32_t* idx)
+{
+    __shared__ float sk[M];
+    __shared__ int si[M];
+    const int64_t base = (int64_t)blockIdx.x * M + E * threadIdx.x;
+    float k[E];
+    int ix[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        k[e] = keys[base + e];
+        ix[e] = E * threadIdx.x + e;
+    }
+    bitonic_sort_desc<M, E>(k, ix, sk, si);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        keys[base + e] = k[e];
+        idx[base + e] = ix[e];
+    }
+}
+
+template <int M, int E, int RES>
+__global__ void __launch_bounds__(M / E) k_test_resample(const float* w_in, const float* u, int32_t* sel_out,
+                                                         float* prob_out, uint32_t* alias_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double dred[33];
+    __shared__ int ired[34];
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const int64_t base = (int64_t)b * M + E * tid;
+    float w[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) w[e] = w_in[base + e];
+    int sel[E];
+    if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
+        double* cum = reinterpret_cast<double*>(smem);
+        const double tot = scan_f64<M, E>(w, cum, dred);
+        const float u0 = u[b];
+        const double step = tot / (double)M;
+#pragma unroll
+        for (int e = 0; e < E; ++e) sel[e] = upper_count<M>(cum, ((double)u0 + (double)(E * tid + e)) * step);
+    } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
+        float* ex = reinterpret_cast<float*>(smem);
+#pragma unroll
+        for (int e = 0; e < E; ++e) ex[E * tid + e] = w[e];
+        const float tot = blelloch_scan<M>(ex);
+#pragma unroll
+        for (int e = 0; e < E; ++e) sel[e] = ref_binary_search(ex, (u[base + e] - 1.0f) * tot, M);
+    } else {
+        float* prob = reinterpret_cast<float*>(smem);
+        unsigned* alias = reinterpret_cast<unsigned*>(prob + M);
+        unsigned* sl = alias + M;
+        float* scr = reinterpret_cast<float*>(sl + M);
+        vose_build<M, E>(w, prob, alias, sl, scr, ired);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int64_t i = base + e;
+            sel[e] = (int)vose_draw<M>(prob, alias, u[2 * i], u[2 * i + 1]);
+            if (prob_out) {
+                prob_out[i] = prob[E * tid + e];
+                alias_out[i] = alias[E * tid + e];
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) sel_out[base + e] = sel[e];
+}
+
+template <class Mdl>
+__global__ void k_test_model(ModelParams mp, const pf_step_input* in, int n, float* state, const float* noise,
+                             float* ll)
+{
+    __shared__ typename Mdl::Consts cst;
+    if (threadIdx.x == 0) Mdl::prepare(cst, *in, mp);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float s[Mdl::S], z[Mdl::K], sn[Mdl::NA > 0 ? Mdl::NA : 1], cs[Mdl::NA > 0 ? Mdl::NA : 1];
+    for (int v = 0; v < Mdl::S; ++v) s[v] = state[(int64_t)v * n + i];
+    for (int v = 0; v < Mdl::K; ++v) z[v] = noise[(int64_t)v * n + i];
+    ll[i] = Mdl::step(cst, s, z, sn, cs);
+    for (int v = 0; v < Mdl::S; ++v) state[(int64_t)v * n + i] = s[v];
+}
+
+}  // namespace pfdev

@@ -1,0 +1,253 @@
+/*
+ * esthera_b200.h -- C ABI of the B200 particle-filter engine.
+ *
+ * The engine replaces the filter step of Esthera's distributed (sub-filter)
+ * particle filter: MTGP32 random numbers -> Box-Muller -> per-particle
+ * propagate + importance weight -> per-sub-filter bitonic sort -> global
+ * winner -> exchange of the best particles between sub-filters -> resampling.
+ * Everything runs as hand-written CUDA for sm_100a; there is no CPU fallback:
+ * every call that needs the GPU returns PF_ERR_CUDA when none is usable.
+ *
+ * Conventions: plain pointers and sizes, no C++ or framework types; every
+ * function returns a pf_status (never exit()); pf_last_error() gives a
+ * thread-local message for the last failure.  A pf_filter is used by one
+ * host thread at a time and owns one CUDA stream.
+ *
+ * Reference interfaces replaced (paths in the Esthera tree):
+ *   driver call  int particle_filter(num_particles, num_blocks, num_transfer,
+ *                resampling_freq, input_file)  src/partfilt/cuda/pf_generic_soa.cu:686,
+ *                src/partfilt/opencl/pf_generic.c:245
+ *   model hooks  sampling_iw / particle_set   src/models/robotarm/cuda/pf_model_soa.cuh:93-184
+ *                read_trace / estimate_error  pf_model_soa.cuh:276-316,
+ *                                             src/models/robotarm/opencl/pf_model_host.h:30-69
+ */
+#ifndef ESTHERA_B200_H
+#define ESTHERA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PF_OK = 0,
+    PF_ERR_INVALID = 1,     /* bad argument / configuration */
+    PF_ERR_CUDA = 2,        /* CUDA runtime failure or no usable GPU */
+    PF_ERR_NOMEM = 3,       /* device or host allocation failed */
+    PF_ERR_UNSUPPORTED = 4, /* valid but not built (e.g. particle count not a power of two) */
+    PF_ERR_IO = 5,          /* trace file missing or malformed */
+    PF_ERR_ADMISSION = 6,   /* serving: request does not fit the memory budget */
+    PF_ERR_TIMEOUT = 7,     /* a bounded wait ran out */
+    PF_ERR_NOT_FOUND = 8,   /* serving: unknown request id */
+    PF_ERR_BUSY = 9         /* serving: no free slot right now */
+} pf_status;
+
+typedef enum {
+    PF_MODEL_UNICYCLE = 0, /* (x, y, theta), range/bearing to landmarks */
+    PF_MODEL_DHARM = 1,    /* 6-joint Denavit-Hartenberg arm, q[6] + qdot[6] */
+    PF_MODEL_REFARM = 2    /* the reference's 5-angle camera arm on a cart */
+} pf_model_id;
+
+typedef enum {
+    PF_EXCHANGE_NONE = 0,
+    PF_EXCHANGE_RING = 1,    /* slot m-1-j <- sub-filter b-1 slot j          (exchange_ring) */
+    PF_EXCHANGE_TORUS = 2,   /* slot m-1-j-k*t <- neighbour k slot j, k = R,L,B,T */
+    PF_EXCHANGE_ALL2ALL = 3  /* slot m-1-j <- j-th best of all sub-filters' top t */
+} pf_exchange;
+
+typedef enum {
+    PF_RESAMPLE_REFERENCE = 0,  /* multinomial, FP32 Blelloch scan + binary search (resampling) */
+    PF_RESAMPLE_SYSTEMATIC = 1, /* systematic, FP64 scan */
+    PF_RESAMPLE_VOSE = 2        /* Vose alias build + draw (resampling_valias) */
+} pf_resampler;
+
+typedef enum {
+    PF_RNG_SUBFILTER = 0, /* one MTGP32 stream per sub-filter, generated inside the step kernel */
+    PF_RNG_REFLAYOUT = 1  /* G streams materialised in the reference's block layout */
+} pf_rng_layout;
+
+typedef enum {
+    PF_PIPELINE_FUSED = 0,  /* sample+weight+sort kernel, exchange+resample kernel */
+    PF_PIPELINE_PHASED = 1  /* one kernel per reference phase */
+} pf_pipeline;
+
+#define PF_MAX_STATE 16
+#define PF_MAX_CONTROL 8
+#define PF_MAX_MEAS 16
+#define PF_MTGP_MASK_PARAMS 0u            /* use each parameter set's own mask (0xfff80000) */
+#define PF_MTGP_MASK_CUDA_REF 0xff800000u /* constant hard-wired in the reference CUDA kernel */
+
+typedef struct {
+    int32_t particles_per_subfilter; /* m: power of two, 32..1024 (reference -m) */
+    int32_t num_subfilters;          /* N (reference -N) */
+    int32_t num_transfer;            /* t (reference -t) */
+    int32_t exchange;                /* pf_exchange */
+    int32_t resampler;               /* pf_resampler */
+    float resampling_freq;           /* sub-filter b resamples iff its uniform u <= freq (reference -r) */
+    uint32_t seed;                   /* stream g / sub-filter b seeded with seed + g + 1 */
+    int32_t rng;                     /* pf_rng_layout */
+    int32_t mtgp_streams;            /* G for PF_RNG_REFLAYOUT (1..200; reference: 96 OpenCL, 120 CUDA) */
+    uint32_t mtgp_mask;              /* PF_MTGP_MASK_PARAMS or PF_MTGP_MASK_CUDA_REF */
+    int32_t log_weights;             /* 1: FP32 max-subtracted log weights; 0: linear FP32 weights */
+    int32_t pipeline;                /* pf_pipeline */
+    int32_t particles_per_thread;    /* 0 = pick; 1, 2 or 4 */
+    int32_t device;                  /* CUDA device ordinal */
+} pf_config;
+
+/* One step's inputs.  control/meas are interpreted by the model:
+ *   unicycle: control {v, omega};        meas {range[L], bearing[L]}
+ *   dharm:    control {};                 meas {px, py, pz, yaw, pitch, roll}
+ *   refarm:   control {joint rates[5]};   meas {angles[5], x, y}
+ * dt <= 0 uses the model's dt. */
+typedef struct {
+    float dt;
+    float control[PF_MAX_CONTROL];
+    float meas[PF_MAX_MEAS];
+    float pad[7];
+} pf_step_input; /* 128 bytes */
+
+typedef struct {
+    double mean[PF_MAX_STATE];  /* weighted posterior mean (circular mean for angles) */
+    double log_norm;            /* log of the global normalisation sum (FP64) */
+    float best[PF_MAX_STATE];   /* the reference's estimate: best particle of the best sub-filter */
+    float best_key;             /* its weight (log or linear, per config) */
+    int32_t best_subfilter;     /* first maximum (thrust::max_element semantics) */
+    int32_t step;               /* steps completed */
+    int32_t flags;              /* nonzero: device-side anomaly (NaN weights ...) */
+} pf_estimate;
+
+typedef struct {
+    float dt;
+    float sigma_q[3];            /* process noise std on x, y, theta */
+    float sigma_range;
+    float sigma_bearing;
+    int32_t num_landmarks;       /* 1..8 */
+    float landmarks[8][2];
+    float init_state[3];
+} pf_unicycle_params;
+
+typedef struct {
+    float dt;
+    float sigma_qd;              /* process noise std on joint velocities */
+    float sigma_pos;             /* end-effector position measurement std */
+    float sigma_ang;             /* yaw/pitch/roll measurement std */
+    float a[6], alpha[6], d[6];  /* standard DH parameters (theta is the joint state) */
+    float init_state[12];        /* q[6], qdot[6] */
+} pf_dharm_params;
+
+typedef struct {
+    float dt;
+    float init_state[9];         /* angles[5], x, y, vX, vY */
+} pf_refarm_params;
+
+typedef struct pf_filter pf_filter;
+
+/* ---- library ---- */
+const char* pf_status_string(pf_status s);
+const char* pf_last_error(void);
+int32_t pf_version(void);
+/* Number of usable CUDA devices (0 when none). */
+int32_t pf_device_count(void);
+/* Model sizes: state floats, normals per particle per step, control and measurement floats. */
+pf_status pf_model_info(pf_model_id model, int32_t* num_state, int32_t* num_noise,
+                        int32_t* num_control, int32_t* num_meas);
+
+/* ---- plain filter (replaces particle_filter()'s step loop body) ---- */
+pf_status pf_config_default(pf_config* cfg);
+pf_status pf_create(const pf_config* cfg, pf_model_id model, const void* params, size_t params_size,
+                    pf_filter** out);
+pf_status pf_destroy(pf_filter* f);
+/* Every particle set to the same state (the reference's init, pf_generic_soa.cu:756-767). */
+pf_status pf_set_initial_state(pf_filter* f, const float* state);
+/* Host SoA arrays, num_state x (m*N) floats. */
+pf_status pf_set_particles(pf_filter* f, const float* soa);
+pf_status pf_get_particles(pf_filter* f, float* soa);
+/* After a step: the sorted (pre-exchange) state, sorted keys, and the slot each
+ * output particle was resampled from (-1: the sub-filter skipped resampling). */
+pf_status pf_get_sorted(pf_filter* f, float* soa, float* keys);
+pf_status pf_get_selection(pf_filter* f, int32_t* sel);
+/* Turn recording of the resampling selections on or off (off by default: it costs 4 bytes per particle-step). */
+pf_status pf_record_selection(pf_filter* f, int32_t enable);
+/* One step with host inputs (copied H2D) and a host estimate (copied D2H); synchronous. */
+pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate* out);
+/* `steps` steps on device-resident inputs: d_inputs[steps] and d_estimates[steps]
+ * (d_estimates may be NULL).  Asynchronous on the filter's stream, captured
+ * into a CUDA graph.  pf_synchronize() waits. */
+pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, int32_t steps,
+                        pf_estimate* d_estimates);
+/* Replays `steps` more steps of the run last set up by pf_run_device (the step
+ * counter continues), e.g. to time steps one at a time. */
+pf_status pf_run_device_continue(pf_filter* f, int32_t steps);
+pf_status pf_synchronize(pf_filter* f);
+/* Per-launch timing: with timing on, every step records a CUDA event before its
+ * first launch and after each launch (graph replays included).
+ * pf_last_step_timing waits for the last step and returns the duration of
+ * each launch in ms; pf_phase_name(i) names launch i ("sample_sort", ...). */
+pf_status pf_set_timing(pf_filter* f, int32_t enable);
+pf_status pf_last_step_timing(pf_filter* f, float* ms, int32_t cap, int32_t* n);
+const char* pf_phase_name(pf_filter* f, int32_t i);
+/* The filter's CUDA stream (a cudaStream_t), for timing with events. */
+void* pf_stream(pf_filter* f);
+/* Resolved configuration: particles per thread used by the kernels, torus dims, bytes held on the device. */
+pf_status pf_get_info(pf_filter* f, int32_t* particles_per_thread, int32_t* torus_dx,
+                      int32_t* torus_dy, int64_t* device_bytes);
+/* Snapshot / restore of particles, sorted keys and MTGP stream words (host buffer of pf_snapshot_size bytes). */
+int64_t pf_snapshot_size(pf_filter* f);
+pf_status pf_snapshot(pf_filter* f, void* host_buf);
+pf_status pf_restore(pf_filter* f, const void* host_buf);
+
+/* ---- kernel-level entry points (device work on host arrays; used by parity tests) ---- */
+/* MTGP32 in the reference block layout: streams g = 0..G-1 with parameter set g,
+ * seed + g + 1; out[g*per_stream + i].  kind 0: uint32, 1: float bits in [1,2).
+ * Replaces mtgp32_uint32_kernel / mtgp32_single_kernel (mtgp32-cuda.cu:180-306). */
+pf_status pfk_mtgp_generate(int32_t G, uint32_t seed, uint32_t mask, int32_t kind,
+                            int64_t per_stream, int32_t calls, uint32_t* out);
+/* In-place Box-Muller over pairs (2i, 2i+1), 2i < n (boxmuller, pf_generic_soa.cu:481-500).
+ * data must hold 2*ceil(n/2) floats. */
+pf_status pfk_boxmuller(float* data, int64_t n);
+/* nsub independent descending bitonic sorts of m keys; idx receives the permutation
+ * (block_sort + bitonic_sort, pf_generic_soa.cu:289-323, bitonic-sort.cu:11-61). */
+pf_status pfk_bitonic_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt);
+/* nsub sub-filters of m weights (linear FP32, slot order) -> sel[nsub*m].
+ * u: REFERENCE: m raw uniforms in [1,2) per sub-filter; SYSTEMATIC: 1 value in [0,1);
+ * VOSE: 2m values in [0,1) (x, y pairs).  ppt: particles per thread (scan grouping). */
+pf_status pfk_resample(int32_t resampler, const float* w, const float* u, int32_t m, int32_t nsub,
+                       int32_t ppt, int32_t* sel);
+/* Vose tables (prob, alias) of nsub sub-filters (vose_alias_init, resampling-valias.cl:111-195). */
+pf_status pfk_vose_build(const float* w, int32_t m, int32_t nsub, int32_t ppt, float* prob,
+                         uint32_t* alias);
+/* Slot sources after exchange for N sub-filters (identity where not replaced). */
+pf_status pfk_exchange_sources(int32_t mode, int32_t N, int32_t m, int32_t t,
+                               const float* sorted_keys, int32_t* src);
+/* One model propagate + log-likelihood for n particles (SoA state in/out, noise SoA K x n). */
+pf_status pfk_model_step(pf_model_id model, const void* params, size_t params_size,
+                         const pf_step_input* in, int32_t n, float* state, const float* noise,
+                         float* loglik);
+
+/* ---- synthetic traces (seeded ground truth + measurements) ---- */
+/* Unicycle: landmarks uniform in [-10,10]^2, truth from (0,0,0), v=1, omega=0.3 sin(0.05 t). */
+pf_status pf_unicycle_default_params(uint32_t seed, int32_t num_landmarks, pf_unicycle_params* p);
+pf_status pf_dharm_default_params(uint32_t seed, pf_dharm_params* p);
+/* steps x pf_step_input and steps x num_state truth floats. */
+pf_status pf_make_trace(pf_model_id model, const void* params, uint32_t seed, int32_t steps,
+                        pf_step_input* inputs, float* truth);
+
+/* ---- reference-compatible driver (reference trace files, C host) ---- */
+/* Parses one line of a reference trace: robot-arm format
+ * "x y angles[5] controls[5] dt actual_x actual_y actual_angles[5]"
+ * (pf_model_soa.cuh:276-301).  Returns PF_OK, or PF_ERR_IO at end of file / bad line. */
+pf_status pf_read_trace_line(void* file, pf_model_id model, pf_step_input* in, float* actual);
+/* The reference's estimate_error for the robot-arm model (pf_model_soa.cuh:303-316). */
+float pf_refarm_estimate_error(const float* est, const float* actual);
+/* Drop-in for the reference driver: runs the robot-arm filter over a trace file with
+ * the reference's defaults (ring exchange, multinomial resampling) and returns the
+ * mean estimate error through *mean_error. */
+pf_status pf_particle_filter(int32_t num_particles, int32_t num_blocks, int32_t num_transfer,
+                             float resampling_freq, const char* input_file, float* mean_error);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
