@@ -115,7 +115,7 @@ def _declare(L):
         "pf_get_selection": (C.c_int, [P, ip]),
         "pf_record_selection": (C.c_int, [P, C.c_int32]),
         "pf_step": (C.c_int, [P, C.POINTER(StepInput), C.POINTER(Estimate)]),
-        "pf_run_device": (C.c_int, [P, P, C.c_int32, P]),
+        "pf_run_device": (C.c_int, [P, P, P, C.c_int32, C.c_int32]),
         "pf_run_device_continue": (C.c_int, [P, C.c_int32]),
         "pf_synchronize": (C.c_int, [P]),
         "pf_stream": (P, [P]),
@@ -314,8 +314,9 @@ class ParticleFilter:
         check(lib().pf_step(self._h, C.byref(s), C.byref(e)))
         return estimate_to_numpy(e)
 
-    def run_device(self, d_inputs_ptr, steps, d_estimates_ptr):
-        check(lib().pf_run_device(self._h, C.c_void_p(d_inputs_ptr), steps, C.c_void_p(d_estimates_ptr)))
+    def run_device(self, d_inputs_ptr, d_estimates_ptr, capacity, steps):
+        """Reset the step counter and run `steps` steps over device arrays of `capacity` entries."""
+        check(lib().pf_run_device(self._h, C.c_void_p(d_inputs_ptr), C.c_void_p(d_estimates_ptr), capacity, steps))
 
     def run_continue(self, steps):
         check(lib().pf_run_device_continue(self._h, steps))

@@ -196,6 +196,7 @@ struct pf_filter {
     cudaGraphExec_t graph = nullptr;
     const pf_step_input* graph_inputs = nullptr;
     pf_estimate* graph_est = nullptr;
+    int32_t graph_cap = 0;
     // per-phase timing: events recorded between the launches of a step
     int timing = 0;
     cudaEvent_t ev[8] = {};
@@ -554,11 +555,16 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
     cudaStream_t st = f->stream;
     const pf_config& c = f->cfg;
     int np = 0;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (f->timing) CU(cudaStreamIsCapturing(st, &cap));
     auto mark = [&](const char* name) -> cudaError_t {
         if (!f->timing) return cudaSuccess;
         if (name) f->phase[np - 1] = name;
         if (np >= 8) return cudaSuccess;
-        return cudaEventRecord(f->ev[np++], st);
+        // inside a capture the record must become an event node of the graph
+        return cudaEventRecordWithFlags(f->ev[np++], st,
+                                        cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                             : cudaEventRecordDefault);
     };
     CU(mark(nullptr));
     if (c.rng == PF_RNG_REFLAYOUT) {
@@ -640,7 +646,7 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     CU(cudaSetDevice(f->cfg.device));
     *f->h_in = *in;
     CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
-    InputRef ir{f->d_in, 0, nullptr};
+    InputRef ir{f->d_in, 0, nullptr, 1};
     pf_status s = enqueue_step(f, f->d_desc, ir, nullptr);
     if (s != PF_OK) return s;
     CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate), cudaMemcpyDeviceToHost, f->stream));
@@ -653,13 +659,12 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     return PF_OK;
 }
 
-extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, int32_t steps,
-                                   pf_estimate* d_estimates)
+extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, pf_estimate* d_estimates,
+                                   int32_t capacity, int32_t steps)
 {
-    if (!f || !d_inputs || !d_estimates || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
+    if (!f || !d_inputs || !d_estimates || capacity < 1 || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
     CU(cudaSetDevice(f->cfg.device));
-    if (steps == 0) return PF_OK;
-    if (!f->graph || f->graph_inputs != d_inputs || f->graph_est != d_estimates) {
+    if (!f->graph || f->graph_inputs != d_inputs || f->graph_est != d_estimates || f->graph_cap != capacity) {
         if (f->graph) {
             cudaGraphExecDestroy(f->graph);
             f->graph = nullptr;
@@ -668,7 +673,7 @@ extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, 
         if (s != PF_OK) return s;
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
-        InputRef ir{d_inputs, 0, f->ctr};
+        InputRef ir{d_inputs, 0, f->ctr, capacity};
         s = enqueue_step(f, f->d_desc + 1, ir, f->ctr);
         cudaError_t e = cudaStreamEndCapture(f->stream, &g);
         if (s != PF_OK) {
@@ -684,6 +689,7 @@ extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, 
         }
         f->graph_inputs = d_inputs;
         f->graph_est = d_estimates;
+        f->graph_cap = capacity;
     }
     CU(cudaMemsetAsync(f->ctr, 0, sizeof(int32_t), f->stream));
     for (int i = 0; i < steps; ++i) CU(cudaGraphLaunch(f->graph, f->stream));

@@ -47,7 +47,13 @@ struct InputRef {
     const pf_step_input* base;
     int64_t filter_stride;   // inputs per filter (batched: [filter][step])
     const int32_t* ctr;      // device step counter (graph replays) or null
+    int32_t cap;             // inputs / estimates per filter: the counter indexes them modulo cap
 };
+
+__device__ __forceinline__ int64_t step_index(const InputRef& in)
+{
+    return in.ctr ? (int64_t)(*in.ctr % (in.cap > 0 ? in.cap : 1)) : 0;
+}
 
 template <int E>
 struct VecT;
@@ -97,7 +103,7 @@ __device__ __forceinline__ void cta_target(const int2* __restrict__ cta_map, int
 
 __device__ __forceinline__ const pf_step_input* input_of(const InputRef& in, int f)
 {
-    return in.base + (int64_t)f * in.filter_stride + (in.ctr ? *in.ctr : 0);
+    return in.base + (int64_t)f * in.filter_stride + step_index(in);
 }
 
 // Shared-memory footprint of k_sample_sort (dynamic part).
@@ -499,6 +505,7 @@ static __global__ void k_a2a_merge(const FilterDesc* __restrict__ descs)
                     k2 = sk[w];
                     o2 = so[w];
                 }
+            if (o2 == 0x7fffffff) o2 = j < D.t ? j : 0;  // only NaN keys left: take sub-filter 0's slot
             s_win = o2;
             const int sbw = o2 / D.t, rank = o2 - sbw * D.t;
             D.a2a[j] = sbw * D.M + rank;
@@ -561,7 +568,7 @@ __global__ void k_estimate(const FilterDesc* __restrict__ descs, InputRef in, ui
         }
     }
     __syncthreads();
-    const int best = wb[0];
+    const int best = (wb[0] >= 0 && wb[0] < D.N) ? wb[0] : 0;  // NaN keys everywhere: report sub-filter 0
     const double gm = D.log_weights ? dr[0][0] : 0.0;
     __syncthreads();
     constexpr int NV = 1 + S + S;
@@ -593,7 +600,7 @@ __global__ void k_estimate(const FilterDesc* __restrict__ descs, InputRef in, ui
     if (tid == 0) {
         for (int w = 1; w < nw; ++w)
             for (int i = 0; i < NV; ++i) dr[0][i] += dr[w][i];
-        const int64_t idx = in.ctr ? *in.ctr : 0;
+        const int64_t idx = step_index(in);
         pf_estimate& E = D.est[idx];
         const double W = dr[0][0];
         for (int v = 0; v < PF_MAX_STATE; ++v) E.mean[v] = 0.0;
@@ -603,7 +610,7 @@ __global__ void k_estimate(const FilterDesc* __restrict__ descs, InputRef in, ui
         for (int v = 0; v < PF_MAX_STATE; ++v) E.best[v] = v < S ? D.tmp[v * D.T + (int64_t)best * D.M] : 0.0f;
         E.best_key = wk[0];
         E.best_subfilter = best;
-        E.step = (int32_t)idx + 1;
+        E.step = in.ctr ? *in.ctr + 1 : 0;
         E.flags = (isfinite(gm) && isfinite(W) && W > 0.0) ? 0 : 1;
     }
 }

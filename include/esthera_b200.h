@@ -172,12 +172,14 @@ pf_status pf_get_selection(pf_filter* f, int32_t* sel);
 pf_status pf_record_selection(pf_filter* f, int32_t enable);
 /* One step with host inputs (copied H2D) and a host estimate (copied D2H); synchronous. */
 pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate* out);
-/* `steps` steps on device-resident inputs: d_inputs[steps] and d_estimates[steps]
- * (d_estimates may be NULL).  Asynchronous on the filter's stream, captured
- * into a CUDA graph.  pf_synchronize() waits. */
-pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, int32_t steps,
-                        pf_estimate* d_estimates);
-/* Replays `steps` more steps of the run last set up by pf_run_device (the step
+/* Device-resident run: d_inputs[capacity] and d_estimates[capacity] in device
+ * memory; resets the step counter and runs `steps` steps (step k reads
+ * d_inputs[k % capacity], writes d_estimates[k % capacity]).  Asynchronous on
+ * the filter's stream: one step is captured into a CUDA graph (once per
+ * argument set) and replayed with a device step counter.  pf_synchronize() waits. */
+pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, pf_estimate* d_estimates,
+                        int32_t capacity, int32_t steps);
+/* Replays `steps` more steps of the run set up by pf_run_device (the step
  * counter continues), e.g. to time steps one at a time. */
 pf_status pf_run_device_continue(pf_filter* f, int32_t steps);
 pf_status pf_synchronize(pf_filter* f);

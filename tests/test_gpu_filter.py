@@ -81,7 +81,7 @@ def test_graph_replay_equals_host_steps(gpu):
     fb = E.ParticleFilter(UNI, p, **cfg)
     d_in = torch.from_numpy(inputs.view(np.uint8).copy()).cuda()
     d_est = torch.zeros(12 * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
-    fb.run_device(d_in.data_ptr(), 12, d_est.data_ptr())
+    fb.run_device(d_in.data_ptr(), d_est.data_ptr(), 12, 12)
     fb.synchronize()
     est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE)
     assert np.array_equal(fa.particles(), fb.particles())
