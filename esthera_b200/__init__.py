@@ -132,6 +132,8 @@ def _declare(L):
         "pfk_resample": (C.c_int, [C.c_int32, fp, fp, C.c_int32, C.c_int32, C.c_int32, ip]),
         "pfk_vose_build": (C.c_int, [fp, C.c_int32, C.c_int32, C.c_int32, fp, up]),
         "pfk_exchange_sources": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, ip]),
+        "pfk_estimate": (C.c_int, [fp, fp, C.c_int32, C.c_int64, C.c_int32, C.c_uint32, C.c_int32,
+                                   C.POINTER(Estimate)]),
         "pfk_model_step": (C.c_int, [C.c_int, P, C.c_size_t, C.POINTER(StepInput), C.c_int32, fp, fp, fp]),
         "pf_unicycle_default_params": (C.c_int, [C.c_uint32, C.c_int32, C.POINTER(UnicycleParams)]),
         "pf_dharm_default_params": (C.c_int, [C.c_uint32, C.POINTER(DhArmParams)]),
@@ -401,6 +403,15 @@ def exchange_sources(mode, N, m, t, sorted_keys=None):
     k = None if sorted_keys is None else _f32(sorted_keys)
     check(lib().pfk_exchange_sources(mode, N, m, t, None if k is None else _fptr(k), _iptr(src)))
     return src
+
+
+def estimate(keys, state, m, angle_mask=0, log_weights=1):
+    """Posterior estimate of SoA particles (pfk_estimate) as an ESTIMATE_DTYPE record."""
+    k = _f32(keys)
+    st = _f32(state)
+    e = Estimate()
+    check(lib().pfk_estimate(_fptr(k), _fptr(st), st.shape[0], len(k), m, angle_mask, log_weights, C.byref(e)))
+    return estimate_to_numpy(e)
 
 
 def model_step(model, params, inp, state, noise):

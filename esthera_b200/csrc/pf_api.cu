@@ -39,6 +39,8 @@ static pf_status fail(pf_status s, const char* fmt, ...)
 
 extern "C" const char* pf_last_error(void) { return g_err.c_str(); }
 
+pf_status pfi_fail(pf_status s, const char* msg) { return fail(s, "%s", msg); }
+
 extern "C" const char* pf_status_string(pf_status s)
 {
     switch (s) {

@@ -228,6 +228,12 @@ pf_status pfk_model_step(pf_model_id model, const void* params, size_t params_si
                          const pf_step_input* in, int32_t n, float* state, const float* noise,
                          float* loglik);
 
+/* Posterior estimate of num_particles particles (keys[T] log or linear weights, state SoA
+ * num_state x T, m per sub-filter): FP64 weighted mean (circular for the variables in
+ * angle_mask), log normalisation sum, first-maximum winner.  Host arrays. */
+pf_status pfk_estimate(const float* keys, const float* state, int32_t num_state, int64_t num_particles,
+                       int32_t m, uint32_t angle_mask, int32_t log_weights, pf_estimate* out);
+
 /* ---- synthetic traces (seeded ground truth + measurements) ---- */
 /* Unicycle: landmarks uniform in [-10,10]^2, truth from (0,0,0), v=1, omega=0.3 sin(0.05 t). */
 pf_status pf_unicycle_default_params(uint32_t seed, int32_t num_landmarks, pf_unicycle_params* p);

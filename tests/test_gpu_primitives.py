@@ -149,3 +149,22 @@ def test_model_step_vs_oracle(gpu, O, model):
             assert np.allclose(gs[v], os_[v], atol=2e-5, rtol=1e-5), v
     # FP32 log-likelihood vs FP64 oracle: relative 1e-4 plus an absolute floor
     assert np.all(np.abs(gl - ol) <= 1e-4 * np.abs(ol) + 5e-3), np.max(np.abs(gl - ol) / (np.abs(ol) + 1))
+
+
+@pytest.mark.parametrize("log_weights", [1, 0])
+def test_estimate_entry_point_vs_fp64(gpu, log_weights):
+    rng = np.random.default_rng(21 + log_weights)
+    m, nsub, S = 256, 37, 3
+    T = m * nsub
+    st = np.stack([rng.normal(0, 2, T), rng.normal(1, 3, T), rng.uniform(-np.pi, np.pi, T)]).astype(np.float32)
+    keys = (rng.normal(-50, 20, T) if log_weights else rng.exponential(1, T)).astype(np.float32)
+    keys[5 * m + 17] = keys.max() + 1  # unique winner
+    e = gpu.estimate(keys, st, m, angle_mask=0b100, log_weights=log_weights)
+    w = np.exp(keys.astype(np.float64) - keys.max()) if log_weights else keys.astype(np.float64)
+    W = w.sum()
+    assert np.allclose(e["mean"][:2], (w[None] * st[:2]).sum(1) / W, rtol=1e-6, atol=1e-6)
+    th = np.arctan2((w * np.sin(st[2])).sum(), (w * np.cos(st[2])).sum())
+    assert abs(np.angle(np.exp(1j * (e["mean"][2] - th)))) < 1e-5
+    ln = (keys.max() + np.log(W)) if log_weights else np.log(W)
+    assert abs(e["log_norm"] - ln) < 1e-5 * abs(ln) + 1e-5
+    assert e["best_subfilter"] == 5 and np.array_equal(e["best"][:3], st[:, 5 * m + 17])
