@@ -134,6 +134,7 @@ def _declare(L):
         "pfk_exchange_sources": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, ip]),
         "pfk_estimate": (C.c_int, [fp, fp, C.c_int32, C.c_int64, C.c_int32, C.c_uint32, C.c_int32,
                                    C.POINTER(Estimate)]),
+        "pfk_estimate_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int64, C.c_int32, C.c_uint32, C.c_int32, P, P]),
         "pfk_model_step": (C.c_int, [C.c_int, P, C.c_size_t, C.POINTER(StepInput), C.c_int32, fp, fp, fp]),
         "pf_unicycle_default_params": (C.c_int, [C.c_uint32, C.c_int32, C.POINTER(UnicycleParams)]),
         "pf_dharm_default_params": (C.c_int, [C.c_uint32, C.POINTER(DhArmParams)]),
@@ -412,6 +413,13 @@ def estimate(keys, state, m, angle_mask=0, log_weights=1):
     e = Estimate()
     check(lib().pfk_estimate(_fptr(k), _fptr(st), st.shape[0], len(k), m, angle_mask, log_weights, C.byref(e)))
     return estimate_to_numpy(e)
+
+
+def estimate_noalloc(d_keys, d_state, num_state, num_particles, m, d_out, angle_mask=0, log_weights=1,
+                     stream=None):
+    """pfk_estimate_noalloc on device pointers (ints); asynchronous on `stream`."""
+    check(lib().pfk_estimate_noalloc(C.c_void_p(d_keys), C.c_void_p(d_state), num_state, num_particles, m,
+                                     angle_mask, log_weights, C.c_void_p(d_out), C.c_void_p(stream)))
 
 
 def model_step(model, params, inp, state, noise):

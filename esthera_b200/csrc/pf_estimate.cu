@@ -6,6 +6,7 @@
 // the reference's winner (first maximum key, thrust::max_element semantics,
 // src/partfilt/cuda/pf_generic_soa.cu:1014-1017).
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "pf_launch.cuh"
@@ -257,6 +258,62 @@ extern "C" pf_status pfk_estimate(const float* keys, const float* state, int32_t
     cudaFree(ds);
     cudaFree(dp);
     cudaFree(de);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return pfi_fail(PF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot call cudaMalloc: code running
+// inside a memory pool or arena that owns every device allocation, embedded
+// hosts whose allocator is locked after start-up, and work that must not
+// allocate between stream captures.  pfk_estimate_noalloc computes exactly
+// what pfk_estimate computes, from device pointers the caller already owns,
+// with its per-sub-filter scratch in the static array below (allocated with
+// the module, held by every GPU that loads the library until exit).
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxSubfilters = 4096;  // 4096 * 35 doubles = 1.15 MB per device
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxSubfilters * kEstStride];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[256];  // device address of g_noalloc_scratch, per device ordinal
+
+extern "C" pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_state, int32_t num_state,
+                                          int64_t num_particles, int32_t m, uint32_t angle_mask,
+                                          int32_t log_weights, pf_estimate* d_out, void* stream)
+{
+    std::string why;
+    if (!d_keys || !d_state || !d_out) return pfi_fail(PF_ERR_INVALID, "null argument");
+    if (!estimate_shape_ok(num_state, num_particles, m, &why)) return pfi_fail(PF_ERR_INVALID, why.c_str());
+    if (num_particles / m > kNoAllocMaxSubfilters)
+        return pfi_fail(PF_ERR_INVALID, "pfk_estimate_noalloc: more than 4096 sub-filters (num_particles / m) "
+                                        "exceed its static scratch; use pfk_estimate");
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 256) {
+        cudaGetLastError();
+        return pfi_fail(PF_ERR_CUDA, "no current CUDA device");
+    }
+    double* scratch = nullptr;
+    {
+        // Once per device, with that device current: the host-side name of the
+        // array is only a stand-in, so ask the runtime for its device address.
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return pfi_fail(PF_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed");
+            }
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    e = launch_estimate(d_keys, d_state, num_state, num_particles, m, angle_mask, log_weights, scratch, d_out,
+                        static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return pfi_fail(PF_ERR_CUDA, cudaGetErrorString(e));

@@ -234,6 +234,22 @@ pf_status pfk_model_step(pf_model_id model, const void* params, size_t params_si
 pf_status pfk_estimate(const float* keys, const float* state, int32_t num_state, int64_t num_particles,
                        int32_t m, uint32_t angle_mask, int32_t log_weights, pf_estimate* out);
 
+/* pfk_estimate for callers that cannot allocate device memory (a pool or arena
+ * owns every allocation, the allocator is locked after start-up, or no
+ * allocation may happen between stream captures).  No counterpart in the
+ * reference.  Inputs and output are device pointers the caller owns; it calls
+ * no cudaMalloc/cudaFree: its per-sub-filter scratch is a static device array
+ * sized for at most 4096 sub-filters (num_particles / m), about 1.15 MB held
+ * by every GPU that loads the library.  Larger inputs return PF_ERR_INVALID.
+ * The first call on a device looks up the array's device address (make that
+ * call before any stream capture).  All calls share the array and every call
+ * overwrites the entries it reads, so nothing needs clearing; calls that
+ * overlap on the GPU (other streams, other threads) race on it.
+ * Asynchronous on `stream` (a cudaStream_t, NULL = default stream). */
+pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_state, int32_t num_state,
+                               int64_t num_particles, int32_t m, uint32_t angle_mask,
+                               int32_t log_weights, pf_estimate* d_out, void* stream);
+
 /* ---- synthetic traces (seeded ground truth + measurements) ---- */
 /* Unicycle: landmarks uniform in [-10,10]^2, truth from (0,0,0), v=1, omega=0.3 sin(0.05 t). */
 pf_status pf_unicycle_default_params(uint32_t seed, int32_t num_landmarks, pf_unicycle_params* p);
