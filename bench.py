@@ -159,6 +159,8 @@ def main():
     ap.add_argument("--resampler", default="systematic", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
+    ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -183,7 +185,9 @@ def main():
     total_steps = args.warmup + args.steps
     inputs, truth = E.make_trace(E.MODEL_UNICYCLE, p, SEED, total_steps + args.e2e_steps)
     f = E.ParticleFilter(E.MODEL_UNICYCLE, p, particles_per_subfilter=M, num_subfilters=NSUB, num_transfer=T_EXCH,
-                         exchange=E.EXCHANGE_TORUS, resampler=resampler, seed=SEED + 1000 * rank, device=local)
+                         exchange=E.EXCHANGE_TORUS, resampler=resampler, seed=SEED + 1000 * rank, device=local,
+                         particles_per_thread=args.ppt if args.pipeline == "split" else 0,
+                         pipeline={"fused": E.PIPELINE_FUSED, "split": E.PIPELINE_SPLIT}[args.pipeline])
     info = f.info()
     stream = torch.cuda.ExternalStream(f.stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -262,6 +266,7 @@ def main():
                                    % args.resampler,
                        "particles": PARTICLES, "subfilters": NSUB, "particles_per_subfilter": M,
                        "particles_per_thread": info["particles_per_thread"], "rng": "MTGP32 per sub-filter",
+                       "pipeline": {0: "fused (one kernel per step)", 1: "phased", 2: "split"}[info["pipeline"]],
                        "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas" if world > 1
                        else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

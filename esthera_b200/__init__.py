@@ -26,7 +26,7 @@ MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM = 0, 1, 2
 EXCHANGE_NONE, EXCHANGE_RING, EXCHANGE_TORUS, EXCHANGE_ALL2ALL = 0, 1, 2, 3
 RESAMPLE_REFERENCE, RESAMPLE_SYSTEMATIC, RESAMPLE_VOSE = 0, 1, 2
 RNG_SUBFILTER, RNG_REFLAYOUT = 0, 1
-PIPELINE_FUSED, PIPELINE_PHASED = 0, 1
+PIPELINE_FUSED, PIPELINE_PHASED, PIPELINE_SPLIT = 0, 1, 2
 MTGP_MASK_PARAMS, MTGP_MASK_CUDA_REF = 0, 0xFF800000
 MAX_STATE, MAX_CONTROL, MAX_MEAS = 16, 8, 16
 
@@ -122,7 +122,7 @@ def _declare(L):
         "pf_set_timing": (C.c_int, [P, C.c_int32]),
         "pf_last_step_timing": (C.c_int, [P, fp, C.c_int32, ip]),
         "pf_phase_name": (C.c_char_p, [P, C.c_int32]),
-        "pf_get_info": (C.c_int, [P, ip, ip, ip, C.POINTER(C.c_int64)]),
+        "pf_get_info": (C.c_int, [P, ip, ip, ip, ip, C.POINTER(C.c_int64)]),
         "pf_snapshot_size": (C.c_int64, [P]),
         "pf_snapshot": (C.c_int, [P, P]),
         "pf_restore": (C.c_int, [P, P]),
@@ -280,9 +280,10 @@ class ParticleFilter:
         self.close()
 
     def info(self):
-        e, dx, dy, b = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
-        check(lib().pf_get_info(self._h, C.byref(e), C.byref(dx), C.byref(dy), C.byref(b)))
-        return {"particles_per_thread": e.value, "torus": (dx.value, dy.value), "device_bytes": b.value}
+        pp, e, dx, dy, b = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib().pf_get_info(self._h, C.byref(pp), C.byref(e), C.byref(dx), C.byref(dy), C.byref(b)))
+        return {"pipeline": pp.value, "particles_per_thread": e.value, "torus": (dx.value, dy.value),
+                "device_bytes": b.value}
 
     def set_initial_state(self, state):
         check(lib().pf_set_initial_state(self._h, _fptr(_f32(state))))

@@ -23,7 +23,10 @@ LIB = PKG / "libesthera_b200.so"
 CLI = PKG / "pf_cli"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+# --fmad=false: no implicit multiply-add contraction, so every kernel that
+# inlines a model or a scan computes bit-identical results (the device code
+# writes its multiply-adds as explicit fmaf where it wants them).
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "--fmad=false",
               "-I" + str(INCLUDE)] + ARCH
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-I" + str(INCLUDE)]
 

@@ -122,20 +122,20 @@ struct ModelOps {
     cudaError_t (*sample_sort)(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
     cudaError_t (*sample_weight)(int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
     cudaError_t (*block_sort)(int, int, int, cudaStream_t, const FilterDesc*, const int2*);
-    cudaError_t (*exchange_resample)(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, int32_t*,
-                                     int);
+    cudaError_t (*exchange_resample)(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef,
+                                     int32_t*, int);
     cudaError_t (*exchange_inplace)(int, int, cudaStream_t, const FilterDesc*, const int2*);
-    cudaError_t (*estimate)(int, cudaStream_t, const FilterDesc*, InputRef);
     cudaError_t (*test_model)(const ModelParams&, const pf_step_input*, int, float*, const float*, float*,
                               cudaStream_t);
+    cudaError_t (*step)(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
 };
 
 template <class Mdl>
 static ModelOps ops_of()
 {
     return {Launch<Mdl>::sample_sort,       Launch<Mdl>::sample_weight,    Launch<Mdl>::block_sort,
-            Launch<Mdl>::exchange_resample, Launch<Mdl>::exchange_inplace, Launch<Mdl>::estimate,
-            Launch<Mdl>::test_model};
+            Launch<Mdl>::exchange_resample, Launch<Mdl>::exchange_inplace, Launch<Mdl>::test_model,
+            Launch<Mdl>::step};
 }
 
 static ModelOps model_ops(int model)
@@ -178,7 +178,9 @@ struct pf_filter {
     ModelParams mp;
     ModelInfo mi;
     ModelOps ops;
-    int M, E, N, t, dx, dy, streams;
+    int M, E, N, t, dx, dy, streams, na, pipe;
+    StepState X{};
+    uint32_t angle_mask;
     int64_t T, rtotal, draws, nbm;
     cudaStream_t stream = nullptr;
     std::vector<void*> allocs;
@@ -186,7 +188,8 @@ struct pf_filter {
           *rbuf = nullptr;
     double* part = nullptr;
     uint32_t* mtgp = nullptr;
-    int32_t *a2a = nullptr, *sel = nullptr, *ctr = nullptr;
+    int32_t *a2a = nullptr, *sel = nullptr, *ctr = nullptr, *est_ctr = nullptr;
+    double* gpart = nullptr;
     pf_estimate* d_est = nullptr;
     pf_step_input* d_in = nullptr;
     FilterDesc* d_desc = nullptr;  // [0]: pf_step, [1]: pf_run_device
@@ -309,10 +312,12 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
         return fail(PF_ERR_INVALID, "mtgp_streams must be in [1, 200]");
     if (c->pipeline == PF_PIPELINE_PHASED && c->rng != PF_RNG_REFLAYOUT)
         return fail(PF_ERR_INVALID, "the phased pipeline uses the reference RNG layout (rng = PF_RNG_REFLAYOUT)");
-    if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED)
+    if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED && c->pipeline != PF_PIPELINE_SPLIT)
         return fail(PF_ERR_INVALID, "unknown pipeline");
-    *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M);
-    if (!me_supported(M, *E))
+    const bool fused = c->pipeline == PF_PIPELINE_FUSED && c->rng == PF_RNG_SUBFILTER && step_supported(M) &&
+                       (c->particles_per_thread == 0 || c->particles_per_thread == M / 32);
+    *E = fused ? M / 32 : (c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M));
+    if (!fused && !me_supported(M, *E))
         return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", *E, M);
     (void)model;
     (void)mi;
@@ -343,7 +348,7 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.dx = f->dx;
     D.dy = f->dy;
     D.log_weights = f->cfg.log_weights ? 1 : 0;
-    D.inplace = (f->cfg.resampling_freq < 1.0f || f->cfg.pipeline == PF_PIPELINE_PHASED) ? 1 : 0;
+    D.inplace = (f->cfg.resampling_freq < 1.0f || f->pipe == PF_PIPELINE_PHASED) ? 1 : 0;
     D.rng_fused = f->cfg.rng == PF_RNG_SUBFILTER ? 1 : 0;
     D.draws = (int32_t)f->draws;
     D.nbm = (int32_t)f->nbm;
@@ -352,6 +357,10 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.stream_base = 0;
     D.freq = f->cfg.resampling_freq;
     D.nnorm = (int64_t)f->mi.K * f->T;
+    D.est_ctr = f->est_ctr;
+    D.gpart = f->gpart;
+    D.angle_mask = f->angle_mask;
+    D.na = f->na;
     D.mp = f->mp;
 }
 
@@ -410,6 +419,12 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     memcpy(&f->mp, params, params_size);
     f->mi = mi;
     f->ops = model_ops(model);
+    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER &&
+               step_supported(cfg->particles_per_subfilter) && E == cfg->particles_per_subfilter / 32)
+                  ? PF_PIPELINE_FUSED
+                  : (cfg->pipeline == PF_PIPELINE_PHASED ? PF_PIPELINE_PHASED : PF_PIPELINE_SPLIT);
+    f->angle_mask = model == PF_MODEL_UNICYCLE ? 0x4u : (model == PF_MODEL_DHARM ? 0x3fu : 0x1fu);
+    f->na = model == PF_MODEL_UNICYCLE ? 1 : (model == PF_MODEL_DHARM ? 6 : 5);
     f->M = cfg->particles_per_subfilter;
     f->E = E;
     f->N = cfg->num_subfilters;
@@ -454,7 +469,22 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     if (cfg->rng == PF_RNG_SUBFILTER) TRY(dalloc(f, &f->ru, (size_t)f->N * (f->draws - f->nbm)));
     else TRY(dalloc(f, &f->rbuf, (size_t)f->rtotal));
     if (cfg->exchange == PF_EXCHANGE_ALL2ALL) TRY(dalloc(f, &f->a2a, (size_t)(f->t > 0 ? f->t : 1)));
+    if (f->pipe == PF_PIPELINE_FUSED) {
+        TRY(dalloc(f, &f->X.tmp2, (size_t)S * f->T));
+        TRY(dalloc(f, &f->X.tkey2, (size_t)f->T));
+        TRY(dalloc(f, &f->X.steps, 1));
+        TRY(dalloc(f, &f->X.need_init, 1));
+        TRY(dalloc(f, &f->X.grp_ctr, (size_t)((f->N + 31) / 32)));
+        if (cudaMemset(f->X.steps, 0, 4) != cudaSuccess ||
+            cudaMemset(f->X.grp_ctr, 0, (size_t)((f->N + 31) / 32) * 4) != cudaSuccess) {
+            cudaGetLastError();
+            release(f);
+            return fail(PF_ERR_CUDA, "cudaMemset failed");
+        }
+    }
     TRY(dalloc(f, &f->ctr, 1));
+    TRY(dalloc(f, &f->est_ctr, 1));
+    TRY(dalloc(f, &f->gpart, (size_t)((f->N + 31) / 32) * kPartStride));
     TRY(dalloc(f, &f->d_est, 1));
     TRY(dalloc(f, &f->d_in, 1));
     TRY(dalloc(f, &f->d_desc, 2));
@@ -465,6 +495,11 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
     }
     TRY(init_streams(f));
+    if (cudaMemset(f->est_ctr, 0, 4) != cudaSuccess || cudaMemset(f->ctr, 0, 4) != cudaSuccess) {
+        cudaGetLastError();
+        release(f);
+        return fail(PF_ERR_CUDA, "cudaMemset failed");
+    }
     TRY(upload_descs(f, nullptr));
     TRY(pf_set_initial_state(f, init_state_of(model, f->mp)));
 #undef TRY
@@ -481,6 +516,26 @@ extern "C" pf_status pf_destroy(pf_filter* f)
     return PF_OK;
 }
 
+// Single-kernel pipeline: the next step starts from `state` instead of resampling.
+static pf_status mark_need_init(pf_filter* f)
+{
+    if (f->pipe != PF_PIPELINE_FUSED) return PF_OK;
+    const int32_t one = 1;
+    CU(cudaMemcpy(f->X.need_init, &one, 4, cudaMemcpyHostToDevice));
+    return PF_OK;
+}
+
+// Single-kernel pipeline: materialise the particles after the last step's
+// resampling into `state` (deferred to the next step otherwise).
+static pf_status materialise(pf_filter* f)
+{
+    if (f->pipe != PF_PIPELINE_FUSED) return PF_OK;
+    InputRef none{nullptr, 0, nullptr, 0};
+    CU(f->ops.step(f->M, f->cfg.resampler, f->N, f->stream, f->d_desc, f->X, none, nullptr, true));
+    CU(cudaStreamSynchronize(f->stream));
+    return PF_OK;
+}
+
 extern "C" pf_status pf_set_initial_state(pf_filter* f, const float* state)
 {
     if (!f || !state) return fail(PF_ERR_INVALID, "null argument");
@@ -490,7 +545,7 @@ extern "C" pf_status pf_set_initial_state(pf_filter* f, const float* state)
         for (int64_t i = 0; i < f->T; ++i) h[(size_t)v * f->T + i] = state[v];
     CU(cudaMemcpy(f->state, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
     f->steps_done = 0;
-    return PF_OK;
+    return mark_need_init(f);
 }
 
 extern "C" pf_status pf_set_particles(pf_filter* f, const float* soa)
@@ -499,7 +554,7 @@ extern "C" pf_status pf_set_particles(pf_filter* f, const float* soa)
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
     CU(cudaMemcpy(f->state, soa, (size_t)f->mi.S * f->T * 4, cudaMemcpyHostToDevice));
-    return PF_OK;
+    return mark_need_init(f);
 }
 
 extern "C" pf_status pf_get_particles(pf_filter* f, float* soa)
@@ -507,6 +562,8 @@ extern "C" pf_status pf_get_particles(pf_filter* f, float* soa)
     if (!f || !soa) return fail(PF_ERR_INVALID, "null argument");
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
+    pf_status s = materialise(f);
+    if (s != PF_OK) return s;
     CU(cudaMemcpy(soa, f->state, (size_t)f->mi.S * f->T * 4, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
@@ -516,8 +573,18 @@ extern "C" pf_status pf_get_sorted(pf_filter* f, float* soa, float* keys)
     if (!f) return fail(PF_ERR_INVALID, "null argument");
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
-    if (soa) CU(cudaMemcpy(soa, f->tmp, (size_t)f->mi.S * f->T * 4, cudaMemcpyDeviceToHost));
-    if (keys) CU(cudaMemcpy(keys, f->tkey, (size_t)f->T * 4, cudaMemcpyDeviceToHost));
+    const float* tmp = f->tmp;
+    const float* tkey = f->tkey;
+    if (f->pipe == PF_PIPELINE_FUSED) {  // the half written by the last step
+        int32_t steps = 0;
+        CU(cudaMemcpy(&steps, f->X.steps, 4, cudaMemcpyDeviceToHost));
+        if (((steps & 1) ^ 1) == 1) {
+            tmp = f->X.tmp2;
+            tkey = f->X.tkey2;
+        }
+    }
+    if (soa) CU(cudaMemcpy(soa, tmp, (size_t)f->mi.S * f->T * 4, cudaMemcpyDeviceToHost));
+    if (keys) CU(cudaMemcpy(keys, tkey, (size_t)f->T * 4, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
 
@@ -544,6 +611,8 @@ extern "C" pf_status pf_get_selection(pf_filter* f, int32_t* sel)
     if (!f->sel) return fail(PF_ERR_INVALID, "selection recording is off (pf_record_selection)");
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
+    pf_status s = materialise(f);
+    if (s != PF_OK) return s;
     CU(cudaMemcpy(sel, f->sel, (size_t)f->T * 4, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
@@ -576,16 +645,21 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
         CU(launch_boxmuller(f->rbuf, (int64_t)f->mi.K * f->T, st));
         CU(mark("boxmuller"));
     }
-    if (c.pipeline == PF_PIPELINE_FUSED) {
+    if (f->pipe == PF_PIPELINE_FUSED) {
+        CU(f->ops.step(M, c.resampler, N, st, desc, f->X, in, ctr_inc, false));
+        CU(mark("step"));
+        if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
+            CU(launch_a2a_merge_step(desc, f->X, st));
+            CU(mark("a2a_merge"));
+        }
+    } else if (f->pipe == PF_PIPELINE_SPLIT) {
         CU(f->ops.sample_sort(M, E, c.rng == PF_RNG_SUBFILTER, N, st, desc, nullptr, in));
         CU(mark("sample_sort"));
         if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
             CU(launch_a2a_merge(1, desc, st));
             CU(mark("a2a_merge"));
         }
-        CU(f->ops.estimate(1, st, desc, in));
-        CU(mark("estimate"));
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, ctr_inc, 1));
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, ctr_inc, 1));
         CU(mark("exchange_resample"));
     } else {
         CU(f->ops.sample_weight(M, E, N, st, desc, nullptr, in));
@@ -596,14 +670,12 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
             CU(launch_a2a_merge(1, desc, st));
             CU(mark("a2a_merge"));
         }
-        CU(f->ops.estimate(1, st, desc, in));
-        CU(mark("estimate"));
         if (c.exchange != PF_EXCHANGE_NONE && f->t > 0) {
             const int nx = c.exchange == PF_EXCHANGE_TORUS ? 4 * f->t : f->t;
             CU(f->ops.exchange_inplace(N, nx < 1024 ? ((nx + 31) / 32) * 32 : 1024, st, desc, nullptr));
             CU(mark("exchange"));
         }
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, ctr_inc, 0));
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, ctr_inc, 0));
         CU(mark("resample"));
     }
     if (f->timing) f->nphase = np - 1;
@@ -648,7 +720,7 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     CU(cudaSetDevice(f->cfg.device));
     *f->h_in = *in;
     CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
-    InputRef ir{f->d_in, 0, nullptr, 1};
+    InputRef ir{f->d_in, 0, nullptr, 0};
     pf_status s = enqueue_step(f, f->d_desc, ir, nullptr);
     if (s != PF_OK) return s;
     CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate), cudaMemcpyDeviceToHost, f->stream));
@@ -720,9 +792,11 @@ extern "C" pf_status pf_synchronize(pf_filter* f)
 
 extern "C" void* pf_stream(pf_filter* f) { return f ? (void*)f->stream : nullptr; }
 
-extern "C" pf_status pf_get_info(pf_filter* f, int32_t* ppt, int32_t* dx, int32_t* dy, int64_t* bytes)
+extern "C" pf_status pf_get_info(pf_filter* f, int32_t* pipe, int32_t* ppt, int32_t* dx, int32_t* dy,
+                                  int64_t* bytes)
 {
     if (!f) return fail(PF_ERR_INVALID, "null argument");
+    if (pipe) *pipe = f->pipe;
     if (ppt) *ppt = f->E;
     if (dx) *dx = f->dx;
     if (dy) *dy = f->dy;
@@ -745,6 +819,8 @@ extern "C" pf_status pf_snapshot(pf_filter* f, void* buf)
     if (!f || !buf) return fail(PF_ERR_INVALID, "null argument");
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
+    pf_status ms = materialise(f);
+    if (ms != PF_OK) return ms;
     char* p = (char*)buf;
     int64_t hdr[4] = {kSnapMagic, f->mi.S, f->T, f->streams};
     memcpy(p, hdr, 32);
@@ -775,7 +851,7 @@ extern "C" pf_status pf_restore(pf_filter* f, const void* buf)
     CU(cudaMemcpy(f->mtgp, p, mb, cudaMemcpyHostToDevice));
     p += mb;
     memcpy(&f->steps_done, p, 4);
-    return PF_OK;
+    return mark_need_init(f);
 }
 
 // ---------------------------------------------------------------------------

@@ -4,6 +4,182 @@
 
 namespace pfdev {
 
+// Slot sources of every sub-filter (identity where no particle arrives).
+__global__ void k_exchange_sources(const FilterDesc* __restrict__ d, int32_t* __restrict__ src)
+{
+    const FilterDesc& D = *d;
+    const int b = blockIdx.x;
+    const int nx = exchange_count(D);
+    for (int s = threadIdx.x; s < D.M; s += blockDim.x) {
+        const int x = D.M - 1 - s;
+        src[(int64_t)b * D.M + s] = (int32_t)(x < nx ? exchange_source(D, b, x) : (int64_t)b * D.M + s);
+    }
+}
+
+// All-to-all: the t best of all sub-filters' sorted top-t lists, ties to the
+// lower (sub-filter, rank) -- a stable descending sort of the candidates, as
+// thrust::sort_by_key(greater) gives (pf_generic2_all2all.cu:1007).
+__global__ void k_a2a_merge(const FilterDesc* __restrict__ descs)
+{
+    const FilterDesc& D = descs[blockIdx.x];
+    constexpr int R = 8;  // sub-filters per thread (N <= 8 * blockDim)
+    __shared__ float sk[32];
+    __shared__ int so[32];
+    __shared__ int s_win;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5;
+    int head[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) head[r] = 0;
+    for (int j = 0; j < D.t; ++j) {
+        float bk = -INFINITY;
+        int bo = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int sb = tid + r * nt;
+            if (sb < D.N && head[r] < D.t) {
+                const float kk = D.tkey[(int64_t)sb * D.M + head[r]];
+                const int ord = sb * D.t + head[r];
+                if (kk > bk || (kk == bk && ord < bo)) {
+                    bk = kk;
+                    bo = ord;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ok = __shfl_xor_sync(kFull, bk, o);
+            const int oo = __shfl_xor_sync(kFull, bo, o);
+            if (ok > bk || (ok == bk && oo < bo)) {
+                bk = ok;
+                bo = oo;
+            }
+        }
+        if (lane == 0) {
+            sk[wp] = bk;
+            so[wp] = bo;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float k2 = sk[0];
+            int o2 = so[0];
+            for (int w = 1; w < nt / 32; ++w)
+                if (sk[w] > k2 || (sk[w] == k2 && so[w] < o2)) {
+                    k2 = sk[w];
+                    o2 = so[w];
+                }
+            if (o2 == 0x7fffffff) o2 = j < D.t ? j : 0;  // only NaN keys left: take sub-filter 0's slot
+            s_win = o2;
+            const int sbw = o2 / D.t, rank = o2 - sbw * D.t;
+            D.a2a[j] = sbw * D.M + rank;
+        }
+        __syncthreads();
+        const int win = s_win;
+        const int sbw = win / D.t;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (tid + r * nt == sbw) head[r]++;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RNG in the reference block layout.
+// ---------------------------------------------------------------------------
+// Stream g (parameter set g % 200) writes out[g*size + i] (mtgp32_single_kernel).
+__global__ void __launch_bounds__(256) k_mtgp_blocks(uint32_t* __restrict__ states, uint32_t* __restrict__ out,
+                                                     int64_t size, uint32_t mask, int float_out, int set_base)
+{
+    __shared__ MtgpSmem ms;
+    const int g = blockIdx.x;
+    uint32_t* gst = states + (int64_t)g * kMtgpN;
+    mtgp_load(ms, gst, (set_base + g) % kMtgpSets, mask, float_out != 0);
+    uint32_t* o = out + (int64_t)g * size;
+    // size may exceed INT_MAX only in absurd configurations; the host bounds it.
+    mtgp_generate(ms, (int)size, float_out != 0, [&](int k, uint32_t w) { o[k] = w; });
+    mtgp_store(ms, gst, (int)size);
+}
+
+// In-place Box-Muller over pairs (2i, 2i+1) with 2i < n.
+__global__ void k_boxmuller(float* __restrict__ data, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * i < n) {
+        float2 v = reinterpret_cast<float2*>(data)[i];
+        float z1, z2;
+        box_muller(v.x, v.y, z1, z2);
+        reinterpret_cast<float2*>(data)[i] = make_float2(z1, z2);
+    }
+}
+
+// All-to-all winners of the half written by the last step (k_a2a_merge on a
+// double-buffered key array).
+__global__ void k_a2a_merge_step(const FilterDesc* __restrict__ descs, StepState X)
+{
+    __shared__ FilterDesc Dl;
+    if (threadIdx.x == 0) {
+        Dl = descs[0];
+        if (((*X.steps) & 1) ^ 1) Dl.tkey = X.tkey2;
+    }
+    __syncthreads();
+    const FilterDesc& D = Dl;
+    constexpr int R = 8;
+    __shared__ float sk[32];
+    __shared__ int so[32];
+    __shared__ int s_win;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5;
+    int head[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) head[r] = 0;
+    for (int j = 0; j < D.t; ++j) {
+        float bk = -INFINITY;
+        int bo = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int sb = tid + r * nt;
+            if (sb < D.N && head[r] < D.t) {
+                const float kk = D.tkey[(int64_t)sb * D.M + head[r]];
+                const int ord = sb * D.t + head[r];
+                if (kk > bk || (kk == bk && ord < bo)) {
+                    bk = kk;
+                    bo = ord;
+                }
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ok = __shfl_xor_sync(kFull, bk, o);
+            const int oo = __shfl_xor_sync(kFull, bo, o);
+            if (ok > bk || (ok == bk && oo < bo)) {
+                bk = ok;
+                bo = oo;
+            }
+        }
+        if (lane == 0) {
+            sk[wp] = bk;
+            so[wp] = bo;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float k2 = sk[0];
+            int o2 = so[0];
+            for (int w = 1; w < nt / 32; ++w)
+                if (sk[w] > k2 || (sk[w] == k2 && so[w] < o2)) {
+                    k2 = sk[w];
+                    o2 = so[w];
+                }
+            if (o2 == 0x7fffffff) o2 = j < D.t ? j : 0;
+            s_win = o2;
+            const int sbw = o2 / D.t, rank = o2 - sbw * D.t;
+            D.a2a[j] = sbw * D.M + rank;
+        }
+        __syncthreads();
+        const int sbw = s_win / D.t;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (tid + r * nt == sbw) head[r]++;
+        __syncthreads();
+    }
+}
+
+
 cudaError_t launch_test_sort(int M, int E, int nsub, float* keys, int32_t* idx, cudaStream_t st)
 {
 #define PF_TS(m, e)                                                  \
@@ -69,6 +245,12 @@ cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStrea
     cudaError_t e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return e;
     k_exchange_sources<<<h.N, 256, 0, st>>>(d, src);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st)
+{
+    k_a2a_merge_step<<<1, 1024, 0, st>>>(d, X);
     return cudaGetLastError();
 }
 

@@ -99,17 +99,50 @@ __device__ __forceinline__ void mtgp_store(const MtgpSmem& s, uint32_t* __restri
 // ---------------------------------------------------------------------------
 // Box-Muller on MTGP floats in [1,2) (boxmuller, pf_generic_soa.cu:481-500):
 // u1 = 2-x, u2 = 2-y in (0,1]; z = sqrt(-2 ln u1) (cos 2 pi u2, sin 2 pi u2).
-// sincospif evaluates the angle as pi*(2 u2) without rounding 2 pi u2 first.
+// The angle is evaluated as 2 pi (u2 - 1/2) in (-pi, pi], where the SFU
+// sine/cosine are accurate to ~4e-7 absolute, and the signs flipped back
+// (cos(a + pi) = -cos a); the radius uses the SFU reciprocal square root.
+// ln u1 keeps the full-precision logf: near u1 = 1 the result is tiny and an
+// approximate logarithm would lose all its relative precision.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void box_muller(float x, float y, float& z1, float& z2)
 {
     const float u1 = 2.0f - x, u2 = 2.0f - y;
-    const float r = sqrtf(-2.0f * logf(u1));
+    const float t = -2.0f * logf(u1);
+    const float r = t > 0.0f ? t * rsqrtf(t) : 0.0f;
     float s, c;
-    sincospif(2.0f * u2, &s, &c);
-    z1 = r * c;
-    z2 = r * s;
+    __sincosf(kTwoPi * (u2 - 0.5f), &s, &c);
+    z1 = -r * c;
+    z2 = -r * s;
 }
+
+// atan2 from an odd polynomial for atan on [0, 1] -- degree 15 in a, i.e. 8
+// coefficients in a^2, fitted for this project by least squares on 4000
+// Chebyshev nodes refined with Lawson iterations towards the minimax fit
+// (max error 1.4e-7 in FP32 Horner) -- plus octant reduction with one fast
+// division.  Max absolute error about 3e-7 rad.
+__device__ __forceinline__ float pf_atan2(float y, float x)
+{
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    const float a = mx > 0.0f ? __fdividef(mn, mx) : 0.0f;
+    const float s = a * a;
+    float p = -4.054567008e-03f;
+    p = fmaf(p, s, 2.186295757e-02f);
+    p = fmaf(p, s, -5.591232720e-02f);
+    p = fmaf(p, s, 9.642197449e-02f);
+    p = fmaf(p, s, -1.390862965e-01f);
+    p = fmaf(p, s, 1.994656569e-01f);
+    p = fmaf(p, s, -3.332986079e-01f);
+    p = fmaf(p, s, 9.999993356e-01f);
+    float r = a * p;
+    if (ay > ax) r = 1.57079632679489662f - r;
+    if (x < 0.0f) r = kPi - r;
+    return copysignf(r, y);
+}
+
+// sqrt(d2) for d2 >= 0 through the SFU reciprocal square root (0 -> 0).
+__device__ __forceinline__ float pf_sqrt(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 
 // ---------------------------------------------------------------------------
 // Descending bitonic key+index sort of M keys, E consecutive keys per thread
@@ -118,12 +151,13 @@ __device__ __forceinline__ void box_muller(float x, float y, float& z1, float& z
 // the pair (p, p+stride) with p & stride == 0 swaps iff
 // (key[p] > key[p+stride]) == ((p & size) != 0), so equal keys swap.
 // Strides below E are register pairs, strides below 32E are warp shuffles,
-// longer strides go through shared memory (sk/si hold M entries).
+// longer strides go through shared memory (sk/si hold M entries).  `tid` is
+// the thread's rank within the sub-filter (the lane when a warp owns one).
 // ---------------------------------------------------------------------------
 template <int M, int E>
-__device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si)
+__device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si,
+                                                  int tid = threadIdx.x)
 {
-    const int tid = threadIdx.x;
 #pragma unroll
     for (int size = 2; size <= M; size <<= 1) {
 #pragma unroll
@@ -484,7 +518,7 @@ union ModelParams {
     pf_refarm_params ref;
 };
 
-__device__ __forceinline__ float wrap_pi(float a) { return a - kTwoPi * floorf((a + kPi) * kInvTwoPi); }
+__device__ __forceinline__ float wrap_pi(float a) { return fmaf(-kTwoPi, floorf((a + kPi) * kInvTwoPi), a); }
 
 struct Unicycle {
     static constexpr int S = 3, K = 3, NA = 1;
@@ -534,9 +568,9 @@ struct Unicycle {
     {
         float st, ct;
         __sincosf(s[2], &st, &ct);
-        const float nx = s[0] + c.A * ct - c.B * st + c.sq0 * n[0];
-        const float ny = s[1] + c.A * st + c.B * ct + c.sq1 * n[1];
-        const float nt = wrap_pi(s[2] + c.wd + c.sq2 * n[2]);
+        const float nx = fmaf(c.sq0, n[0], fmaf(c.A, ct, fmaf(-c.B, st, s[0])));
+        const float ny = fmaf(c.sq1, n[1], fmaf(c.A, st, fmaf(c.B, ct, s[1])));
+        const float nt = wrap_pi(fmaf(c.sq2, n[2], s[2] + c.wd));
         s[0] = nx;
         s[1] = ny;
         s[2] = nt;
@@ -549,12 +583,13 @@ struct Unicycle {
         for (int j = 0; j < 8; ++j) {
             if (j < c.L) {
                 const float dx = c.lx[j] - nx, dy = c.ly[j] - ny;
-                const float r = sqrtf(dx * dx + dy * dy);
+                const float r = pf_sqrt(fmaf(dx, dx, dy * dy));
                 const float er = (c.rm[j] - r) * c.isr;
-                const float cp = c2 * c.cb[j] - s2 * c.sb[j];
-                const float sp = s2 * c.cb[j] + c2 * c.sb[j];
-                const float eb = atan2f(sp * dx - cp * dy, cp * dx + sp * dy) * c.isb;
-                acc += er * er + eb * eb;
+                const float cp = fmaf(c2, c.cb[j], -(s2 * c.sb[j]));
+                const float sp = fmaf(s2, c.cb[j], c2 * c.sb[j]);
+                const float eb = pf_atan2(fmaf(sp, dx, -(cp * dy)), fmaf(cp, dx, sp * dy)) * c.isb;
+                acc = fmaf(er, er, acc);
+                acc = fmaf(eb, eb, acc);
             }
         }
         return -0.5f * acc;
@@ -590,40 +625,46 @@ struct DhArm {
         float p0 = 0, p1 = 0, p2 = 0;
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
-            const float q = wrap_pi(s[i] + s[6 + i] * c.dt);
+            const float q = wrap_pi(fmaf(s[6 + i], c.dt, s[i]));
             s[i] = q;
-            s[6 + i] = s[6 + i] + c.sqd * n[i];
+            s[6 + i] = fmaf(c.sqd, n[i], s[6 + i]);
             float sq, cq;
             __sincosf(q, &sq, &cq);
             sn[i] = sq;
             cs[i] = cq;
             // A_i = [[c, -s ca, s sa, a c], [s, c ca, -c sa, a s], [0, sa, ca, d]]
-            const float a00 = cq, a01 = -sq * c.ca[i], a02 = sq * c.sa[i];
-            const float a10 = sq, a11 = cq * c.ca[i], a12 = -cq * c.sa[i];
+            const float a00 = cq, a01 = -(sq * c.ca[i]), a02 = sq * c.sa[i];
+            const float a10 = sq, a11 = cq * c.ca[i], a12 = -(cq * c.sa[i]);
             const float a21 = c.sa[i], a22 = c.ca[i];
             const float t0 = c.a[i] * cq, t1 = c.a[i] * sq, t2 = c.d[i];
-            const float n00 = R00 * a00 + R01 * a10, n01 = R00 * a01 + R01 * a11 + R02 * a21,
-                        n02 = R00 * a02 + R01 * a12 + R02 * a22;
-            const float n10 = R10 * a00 + R11 * a10, n11 = R10 * a01 + R11 * a11 + R12 * a21,
-                        n12 = R10 * a02 + R11 * a12 + R12 * a22;
-            const float n20 = R20 * a00 + R21 * a10, n21 = R20 * a01 + R21 * a11 + R22 * a21,
-                        n22 = R20 * a02 + R21 * a12 + R22 * a22;
-            p0 = R00 * t0 + R01 * t1 + R02 * t2 + p0;
-            p1 = R10 * t0 + R11 * t1 + R12 * t2 + p1;
-            p2 = R20 * t0 + R21 * t1 + R22 * t2 + p2;
+            const float n00 = fmaf(R01, a10, R00 * a00), n01 = fmaf(R02, a21, fmaf(R01, a11, R00 * a01)),
+                        n02 = fmaf(R02, a22, fmaf(R01, a12, R00 * a02));
+            const float n10 = fmaf(R11, a10, R10 * a00), n11 = fmaf(R12, a21, fmaf(R11, a11, R10 * a01)),
+                        n12 = fmaf(R12, a22, fmaf(R11, a12, R10 * a02));
+            const float n20 = fmaf(R21, a10, R20 * a00), n21 = fmaf(R22, a21, fmaf(R21, a11, R20 * a01)),
+                        n22 = fmaf(R22, a22, fmaf(R21, a12, R20 * a02));
+            p0 = fmaf(R02, t2, fmaf(R01, t1, fmaf(R00, t0, p0)));
+            p1 = fmaf(R12, t2, fmaf(R11, t1, fmaf(R10, t0, p1)));
+            p2 = fmaf(R22, t2, fmaf(R21, t1, fmaf(R20, t0, p2)));
             R00 = n00; R01 = n01; R02 = n02;
             R10 = n10; R11 = n11; R12 = n12;
             R20 = n20; R21 = n21; R22 = n22;
         }
-        const float yaw = atan2f(R10, R00);
-        const float pitch = atan2f(-R20, sqrtf(R21 * R21 + R22 * R22));
-        const float roll = atan2f(R21, R22);
+        const float yaw = pf_atan2(R10, R00);
+        const float pitch = pf_atan2(-R20, pf_sqrt(fmaf(R21, R21, R22 * R22)));
+        const float roll = pf_atan2(R21, R22);
         const float e0 = (c.z[0] - p0) * c.isp, e1 = (c.z[1] - p1) * c.isp, e2 = (c.z[2] - p2) * c.isp;
         float d3 = c.z[3] - yaw, d4 = c.z[4] - pitch, d5 = c.z[5] - roll;
-        d3 = (d3 - kTwoPi * rintf(d3 * kInvTwoPi)) * c.isa;
-        d4 = (d4 - kTwoPi * rintf(d4 * kInvTwoPi)) * c.isa;
-        d5 = (d5 - kTwoPi * rintf(d5 * kInvTwoPi)) * c.isa;
-        return -0.5f * (e0 * e0 + e1 * e1 + e2 * e2 + d3 * d3 + d4 * d4 + d5 * d5);
+        d3 = fmaf(-kTwoPi, rintf(d3 * kInvTwoPi), d3) * c.isa;
+        d4 = fmaf(-kTwoPi, rintf(d4 * kInvTwoPi), d4) * c.isa;
+        d5 = fmaf(-kTwoPi, rintf(d5 * kInvTwoPi), d5) * c.isa;
+        float acc = e0 * e0;
+        acc = fmaf(e1, e1, acc);
+        acc = fmaf(e2, e2, acc);
+        acc = fmaf(d3, d3, acc);
+        acc = fmaf(d4, d4, acc);
+        acc = fmaf(d5, d5, acc);
+        return -0.5f * acc;
     }
 };
 
@@ -649,35 +690,35 @@ struct RefArm {
     {
         const float arm[5] = {0.0f, 3.0f, 3.0f, 3.0f, 3.0f};
         const float vX = s[7], vY = s[8];
-        const float x = s[5] + vX * c.dt + n[5] * 0.2f;
-        const float y = s[6] + vY * c.dt + n[6] * 0.2f;
+        const float x = fmaf(n[5], 0.2f, fmaf(vX, c.dt, s[5]));
+        const float y = fmaf(n[6], 0.2f, fmaf(vY, c.dt, s[6]));
         s[5] = x;
         s[6] = y;
-        s[7] = vX + n[7] * 2.0f;
-        s[8] = vY + n[8] * 2.0f;
+        s[7] = fmaf(n[7], 2.0f, vX);
+        s[8] = fmaf(n[8], 2.0f, vY);
         float value = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
-            const float ang = s[i] + c.cdt[i] + n[i] * 0.2f;
+            const float ang = fmaf(n[i], 0.2f, s[i] + c.cdt[i]);
             s[i] = ang;
             float sf, cf;
             __sincosf(ang, &sf, &cf);
             sn[i] = sf;
             cs[i] = cf;
             if (i == 0) {
-                cx = x * cf + y * sf;
-                cy = -x * sf + y * cf;
+                cx = fmaf(x, cf, y * sf);
+                cy = fmaf(-x, sf, y * cf);
                 cz = 0.0f;
             } else {
-                const float nb = cy * cf - cz * sf, nc = cy * sf + cz * cf;
+                const float nb = fmaf(cy, cf, -(cz * sf)), nc = fmaf(cy, sf, cz * cf);
                 cy = nb;
                 cz = nc - arm[i];
             }
             const float e = ang - c.z[i];
-            value += e * e * 0.1f;
+            value = fmaf(e * e, 0.1f, value);
         }
-        value += (cx - c.z[5]) * (cx - c.z[5]) * 0.1f;
-        value += (cy - c.z[6]) * (cy - c.z[6]) * 0.1f;
+        value = fmaf((cx - c.z[5]) * (cx - c.z[5]), 0.1f, value);
+        value = fmaf((cy - c.z[6]) * (cy - c.z[6]), 0.1f, value);
         return -value;
     }
 };

@@ -1,0 +1,6 @@
+// Kernel instantiations: the single-kernel step, systematic for the 6-joint Denavit-Hartenberg arm.
+#define PF_PART_STEPSYS
+#include "pf_launch_impl.cuh"
+namespace pfdev {
+template cudaError_t Launch<DhArm>::step_sys(int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+}  // namespace pfdev

@@ -1,0 +1,6 @@
+// Kernel instantiations: the single-kernel step, systematic for the unicycle (range/bearing) model.
+#define PF_PART_STEPSYS
+#include "pf_launch_impl.cuh"
+namespace pfdev {
+template cudaError_t Launch<Unicycle>::step_sys(int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+}  // namespace pfdev

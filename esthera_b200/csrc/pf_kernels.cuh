@@ -40,6 +40,10 @@ struct FilterDesc {
     int32_t stream_base;
     float freq;
     int64_t nnorm;     // normals in rbuf before the uniforms (K*T)
+    int32_t* est_ctr;  // ticket counter of the two-level estimate (0 between steps)
+    double* gpart;     // ceil(N/32) * kPartStride group partials
+    uint32_t angle_mask;
+    int32_t na;        // angular state variables (circular means)
     ModelParams mp;
 };
 
@@ -64,28 +68,36 @@ struct VecT<2> { using T = float2; };
 template <>
 struct VecT<4> { using T = float4; };
 
+// E consecutive floats per thread: float4 chunks when E is a multiple of 4.
 template <int E>
 __device__ __forceinline__ void ldv(const float* __restrict__ p, float (&o)[E])
 {
-    if constexpr (E == 4) {
-        const float4 v = *reinterpret_cast<const float4*>(p);
-        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    if constexpr (E % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < E; q += 4) {
+            const float4 v = *reinterpret_cast<const float4*>(p + q);
+            o[q] = v.x; o[q + 1] = v.y; o[q + 2] = v.z; o[q + 3] = v.w;
+        }
     } else if constexpr (E == 2) {
         const float2 v = *reinterpret_cast<const float2*>(p);
         o[0] = v.x; o[1] = v.y;
     } else {
-        o[0] = *p;
+#pragma unroll
+        for (int q = 0; q < E; ++q) o[q] = p[q];
     }
 }
 template <int E>
 __device__ __forceinline__ void stv(float* __restrict__ p, const float (&o)[E])
 {
-    if constexpr (E == 4) {
-        *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+    if constexpr (E % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < E; q += 4)
+            *reinterpret_cast<float4*>(p + q) = make_float4(o[q], o[q + 1], o[q + 2], o[q + 3]);
     } else if constexpr (E == 2) {
         *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
     } else {
-        *p = o[0];
+#pragma unroll
+        for (int q = 0; q < E; ++q) p[q] = o[q];
     }
 }
 
@@ -420,18 +432,6 @@ __device__ __forceinline__ int exchange_count(const FilterDesc& D)
     return D.exchange == PF_EXCHANGE_TORUS ? 4 * D.t : D.t;
 }
 
-// Slot sources of every sub-filter (identity where no particle arrives).
-static __global__ void k_exchange_sources(const FilterDesc* __restrict__ d, int32_t* __restrict__ src)
-{
-    const FilterDesc& D = *d;
-    const int b = blockIdx.x;
-    const int nx = exchange_count(D);
-    for (int s = threadIdx.x; s < D.M; s += blockDim.x) {
-        const int x = D.M - 1 - s;
-        src[(int64_t)b * D.M + s] = (int32_t)(x < nx ? exchange_source(D, b, x) : (int64_t)b * D.M + s);
-    }
-}
-
 // Phased pipeline: copy the exchanged particles into the receivers' weakest
 // slots of tmp/tkey (reads slots [0,t), writes [M-4t, M): disjoint by the
 // create-time constraint, so the in-place copy equals the out-of-place one).
@@ -455,163 +455,124 @@ __global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const i
     }
 }
 
-// All-to-all: the t best of all sub-filters' sorted top-t lists, ties to the
-// lower (sub-filter, rank) -- a stable descending sort of the candidates, as
-// thrust::sort_by_key(greater) gives (pf_generic2_all2all.cu:1007).
-static __global__ void k_a2a_merge(const FilterDesc* __restrict__ descs)
-{
-    const FilterDesc& D = descs[blockIdx.x];
-    constexpr int R = 8;  // sub-filters per thread (N <= 8 * blockDim)
-    __shared__ float sk[32];
-    __shared__ int so[32];
-    __shared__ int s_win;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5;
-    int head[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) head[r] = 0;
-    for (int j = 0; j < D.t; ++j) {
-        float bk = -INFINITY;
-        int bo = 0x7fffffff;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int sb = tid + r * nt;
-            if (sb < D.N && head[r] < D.t) {
-                const float kk = D.tkey[(int64_t)sb * D.M + head[r]];
-                const int ord = sb * D.t + head[r];
-                if (kk > bk || (kk == bk && ord < bo)) {
-                    bk = kk;
-                    bo = ord;
-                }
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ok = __shfl_xor_sync(kFull, bk, o);
-            const int oo = __shfl_xor_sync(kFull, bo, o);
-            if (ok > bk || (ok == bk && oo < bo)) {
-                bk = ok;
-                bo = oo;
-            }
-        }
-        if (lane == 0) {
-            sk[wp] = bk;
-            so[wp] = bo;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            float k2 = sk[0];
-            int o2 = so[0];
-            for (int w = 1; w < nt / 32; ++w)
-                if (sk[w] > k2 || (sk[w] == k2 && so[w] < o2)) {
-                    k2 = sk[w];
-                    o2 = so[w];
-                }
-            if (o2 == 0x7fffffff) o2 = j < D.t ? j : 0;  // only NaN keys left: take sub-filter 0's slot
-            s_win = o2;
-            const int sbw = o2 / D.t, rank = o2 - sbw * D.t;
-            D.a2a[j] = sbw * D.M + rank;
-        }
-        __syncthreads();
-        const int win = s_win;
-        const int sbw = win / D.t;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (tid + r * nt == sbw) head[r]++;
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------------------
-// Global winner (first maximum) + FP64 posterior mean, one CTA per filter.
+// Global winner (first maximum, thrust::max_element semantics,
+// pf_generic_soa.cu:1014-1017) + FP64 posterior mean, reduced in two fixed-order
+// levels inside the resampling kernel: warp 0 of the CTA of sub-filter 32g
+// combines sub-filters 32g..32g+31 (all partials are final when that kernel
+// starts); the last group to finish (atomic ticket) combines the groups in
+// index order and writes the estimate.  Deterministic for a given N.
 // ---------------------------------------------------------------------------
 template <int S>
-__global__ void k_estimate(const FilterDesc* __restrict__ descs, InputRef in, uint32_t angle_mask)
+__device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, const InputRef& in, int32_t* step_ctr)
 {
-    const FilterDesc& D = descs[blockIdx.x];
-    if (!D.est) return;
-    __shared__ float wk[32];
-    __shared__ int wb[32];
-    __shared__ double dr[32][S + 2 + S];
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wp = tid >> 5, nw = nt / 32;
-    float bk = -INFINITY;
-    int bb = 0x7fffffff;
-    double gmax = -INFINITY;
-    for (int b = tid; b < D.N; b += nt) {
-        const float kk = D.winner[b];
-        if (kk > bk || (kk == bk && b < bb)) {
-            bk = kk;
-            bb = b;
-        }
-        gmax = fmax(gmax, D.part[(int64_t)b * kPartStride]);
-    }
+    if ((b & 31) != 0 || threadIdx.x >= 32) return;
+    constexpr int NVMAX = 2 + 2 * S;
+    const int lane = threadIdx.x;
+    const int g = b >> 5, ng = (D.N + 31) >> 5;
+    const int NV = 2 + S + D.na;
+    const int sb = b + lane;
+    const bool valid = sb < D.N;
+    const double* pp = D.part + (int64_t)(valid ? sb : b) * kPartStride;
+    double gl = valid ? pp[0] : -INFINITY;
+    float wk = valid ? D.winner[sb] : -INFINITY;
+    int wi = valid ? sb : 0x7fffffff;
+#pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        const float ok = __shfl_xor_sync(kFull, bk, o);
-        const int ob = __shfl_xor_sync(kFull, bb, o);
-        if (ok > bk || (ok == bk && ob < bb)) {
-            bk = ok;
-            bb = ob;
+        gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
+        const float ok = __shfl_xor_sync(kFull, wk, o);
+        const int oi = __shfl_xor_sync(kFull, wi, o);
+        if (ok > wk || (ok == wk && oi < wi)) {
+            wk = ok;
+            wi = oi;
         }
-        gmax = fmax(gmax, __shfl_xor_sync(kFull, gmax, o));
+    }
+    const double sc = valid ? (D.log_weights ? exp(pp[0] - gl) : 1.0) : 0.0;
+    double* go = D.gpart + (int64_t)g * kPartStride;
+#pragma unroll
+    for (int j = 1; j < NVMAX; ++j) {
+        if (j < NV) {
+            double v = valid ? sc * pp[j] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+            if (lane == 0) go[j] = v;
+        }
     }
     if (lane == 0) {
-        wk[wp] = bk;
-        wb[wp] = bb;
-        dr[wp][0] = gmax;
+        go[0] = D.log_weights ? gl : 0.0;
+        go[NV] = (double)wk;
+        go[NV + 1] = (double)wi;
     }
-    __syncthreads();
-    if (tid == 0) {
-        for (int w = 1; w < nw; ++w) {
-            if (wk[w] > wk[0] || (wk[w] == wk[0] && wb[w] < wb[0])) {
-                wk[0] = wk[w];
-                wb[0] = wb[w];
-            }
-            dr[0][0] = fmax(dr[0][0], dr[w][0]);
-        }
-    }
-    __syncthreads();
-    const int best = (wb[0] >= 0 && wb[0] < D.N) ? wb[0] : 0;  // NaN keys everywhere: report sub-filter 0
-    const double gm = D.log_weights ? dr[0][0] : 0.0;
-    __syncthreads();
-    constexpr int NV = 1 + S + S;
-    double acc[NV];
-#pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = 0.0;
-    for (int b = tid; b < D.N; b += nt) {
-        const double* pp = D.part + (int64_t)b * kPartStride;
-        const double sc = D.log_weights ? exp(pp[0] - gm) : 1.0;
-        acc[0] += sc * pp[1];
-        int a = 0;
-#pragma unroll
-        for (int v = 0; v < S; ++v) {
-            acc[1 + v] += sc * pp[2 + v];
-            if ((angle_mask >> v) & 1u) {
-                acc[1 + S + v] += sc * pp[2 + S + a];
-                ++a;
-            }
+    __syncwarp();
+    __threadfence();
+    int last = 0;
+    if (lane == 0) last = atomicAdd(D.est_ctr, 1) == ng - 1;
+    last = __shfl_sync(kFull, last, 0);
+    if (!last) return;
+    __threadfence();
+    double gm = -INFINITY;
+    float bk = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int q = lane; q < ng; q += 32) {
+        const double* gq = D.gpart + (int64_t)q * kPartStride;
+        gm = fmax(gm, __ldcg(gq));
+        const float k = (float)__ldcg(gq + NV);
+        const int i = (int)__ldcg(gq + NV + 1);
+        if (k > bk || (k == bk && i < bi)) {
+            bk = k;
+            bi = i;
         }
     }
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
+    for (int o = 16; o > 0; o >>= 1) {
+        gm = fmax(gm, __shfl_xor_sync(kFull, gm, o));
+        const float ok = __shfl_xor_sync(kFull, bk, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        if (ok > bk || (ok == bk && oi < bi)) {
+            bk = ok;
+            bi = oi;
+        }
+    }
+    double acc[NVMAX];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(kFull, acc[i], o);
-    if (lane == 0)
+    for (int j = 0; j < NVMAX; ++j) acc[j] = 0.0;
+    for (int q = lane; q < ng; q += 32) {
+        const double* gq = D.gpart + (int64_t)q * kPartStride;
+        const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
 #pragma unroll
-        for (int i = 0; i < NV; ++i) dr[wp][i] = acc[i];
-    __syncthreads();
-    if (tid == 0) {
-        for (int w = 1; w < nw; ++w)
-            for (int i = 0; i < NV; ++i) dr[0][i] += dr[w][i];
+        for (int j = 1; j < NVMAX; ++j)
+            if (j < NV) acc[j] += sq * __ldcg(gq + j);
+    }
+#pragma unroll
+    for (int j = 1; j < NVMAX; ++j)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(kFull, acc[j], o);
+    if (lane == 0) {
+        const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
+        const double lg = D.log_weights ? gm : 0.0;
         const int64_t idx = step_index(in);
         pf_estimate& E = D.est[idx];
-        const double W = dr[0][0];
+        const double W = acc[1];
+        int a = 0;
         for (int v = 0; v < PF_MAX_STATE; ++v) E.mean[v] = 0.0;
-        for (int v = 0; v < S; ++v)
-            E.mean[v] = ((angle_mask >> v) & 1u) ? atan2(dr[0][1 + v], dr[0][1 + S + v]) : dr[0][1 + v] / W;
-        E.log_norm = gm + log(W);
+#pragma unroll
+        for (int v = 0; v < S; ++v) {
+            if ((D.angle_mask >> v) & 1u) {
+                E.mean[v] = atan2(acc[2 + v], acc[2 + S + a]);
+                ++a;
+            } else {
+                E.mean[v] = acc[2 + v] / W;
+            }
+        }
+        E.log_norm = lg + log(W);
         for (int v = 0; v < PF_MAX_STATE; ++v) E.best[v] = v < S ? D.tmp[v * D.T + (int64_t)best * D.M] : 0.0f;
-        E.best_key = wk[0];
+        E.best_key = bk;
         E.best_subfilter = best;
         E.step = in.ctr ? *in.ctr + 1 : 0;
-        E.flags = (isfinite(gm) && isfinite(W) && W > 0.0) ? 0 : 1;
+        E.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
+        *D.est_ctr = 0;
+        __threadfence();
+        if (step_ctr) *step_ctr += 1;
     }
 }
 
@@ -634,7 +595,7 @@ constexpr size_t k2_smem()
 
 template <int S, int M, int E, int RES>
 __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* __restrict__ descs,
-                                                             const int2* __restrict__ cta_map,
+                                                             const int2* __restrict__ cta_map, InputRef in,
                                                              int32_t* step_ctr, int virt)
 {
     constexpr int NT = M / E;
@@ -645,7 +606,7 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     cta_target(cta_map, f, b);
     const FilterDesc& D = descs[f];
     const int tid = threadIdx.x;
-    if (step_ctr && blockIdx.x == 0 && tid == 0) *step_ctr += 1;
+    estimate_groups<S>(D, b, in, step_ctr);
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
     const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;
@@ -741,35 +702,6 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     if (D.sel) {
 #pragma unroll
         for (int e = 0; e < E; ++e) D.sel[base + e] = sel[e];
-    }
-}
-
-// ---------------------------------------------------------------------------
-// RNG in the reference block layout.
-// ---------------------------------------------------------------------------
-// Stream g (parameter set g % 200) writes out[g*size + i] (mtgp32_single_kernel).
-static __global__ void __launch_bounds__(256) k_mtgp_blocks(uint32_t* __restrict__ states, uint32_t* __restrict__ out,
-                                                     int64_t size, uint32_t mask, int float_out, int set_base)
-{
-    __shared__ MtgpSmem ms;
-    const int g = blockIdx.x;
-    uint32_t* gst = states + (int64_t)g * kMtgpN;
-    mtgp_load(ms, gst, (set_base + g) % kMtgpSets, mask, float_out != 0);
-    uint32_t* o = out + (int64_t)g * size;
-    // size may exceed INT_MAX only in absurd configurations; the host bounds it.
-    mtgp_generate(ms, (int)size, float_out != 0, [&](int k, uint32_t w) { o[k] = w; });
-    mtgp_store(ms, gst, (int)size);
-}
-
-// In-place Box-Muller over pairs (2i, 2i+1) with 2i < n.
-static __global__ void k_boxmuller(float* __restrict__ data, int64_t n)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (2 * i < n) {
-        float2 v = reinterpret_cast<float2*>(data)[i];
-        float z1, z2;
-        box_muller(v.x, v.y, z1, z2);
-        reinterpret_cast<float2*>(data)[i] = make_float2(z1, z2);
     }
 }
 

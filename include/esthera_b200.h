@@ -69,8 +69,10 @@ typedef enum {
 } pf_rng_layout;
 
 typedef enum {
-    PF_PIPELINE_FUSED = 0,  /* sample+weight+sort kernel, exchange+resample kernel */
-    PF_PIPELINE_PHASED = 1  /* one kernel per reference phase */
+    PF_PIPELINE_FUSED = 0,  /* one kernel per step, one warp per sub-filter (m = 128, 256, 512 with
+                               PF_RNG_SUBFILTER; other configurations run PF_PIPELINE_SPLIT) */
+    PF_PIPELINE_PHASED = 1, /* one kernel per reference phase */
+    PF_PIPELINE_SPLIT = 2   /* sample+weight+sort kernel, then exchange+resample+estimate kernel */
 } pf_pipeline;
 
 #define PF_MAX_STATE 16
@@ -192,8 +194,8 @@ pf_status pf_last_step_timing(pf_filter* f, float* ms, int32_t cap, int32_t* n);
 const char* pf_phase_name(pf_filter* f, int32_t i);
 /* The filter's CUDA stream (a cudaStream_t), for timing with events. */
 void* pf_stream(pf_filter* f);
-/* Resolved configuration: particles per thread used by the kernels, torus dims, bytes held on the device. */
-pf_status pf_get_info(pf_filter* f, int32_t* particles_per_thread, int32_t* torus_dx,
+/* Resolved configuration: pipeline actually used, particles per thread, torus dims, device bytes. */
+pf_status pf_get_info(pf_filter* f, int32_t* pipeline, int32_t* particles_per_thread, int32_t* torus_dx,
                       int32_t* torus_dy, int64_t* device_bytes);
 /* Snapshot / restore of particles, sorted keys and MTGP stream words (host buffer of pf_snapshot_size bytes). */
 int64_t pf_snapshot_size(pf_filter* f);

@@ -25,17 +25,43 @@ def run(E, model, params, inputs, steps=None, **cfg):
 
 @pytest.mark.parametrize("res", [0, 1, 2])
 @pytest.mark.parametrize("exch,t", [(0, 0), (1, 3), (2, 2), (3, 4)])
-def test_phased_equals_fused(gpu, res, exch, t):
+def test_phased_equals_split(gpu, res, exch, t):
+    """One kernel per reference phase vs the two-kernel split pipeline (reference RNG layout)."""
     E = gpu
     p, inputs, _ = uni_setup()
     common = dict(particles_per_subfilter=256, num_subfilters=16, num_transfer=t, exchange=exch, resampler=res,
                   rng=E.RNG_REFLAYOUT, mtgp_streams=96)
     fa, ea = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_PHASED, **common)
-    fb, eb = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_FUSED, **common)
+    fb, eb = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_SPLIT, **common)
+    assert fa.info()["pipeline"] == E.PIPELINE_PHASED and fb.info()["pipeline"] == E.PIPELINE_SPLIT
     assert np.array_equal(fa.particles(), fb.particles())
     for x, y in zip(ea, eb):
         assert x["best_subfilter"] == y["best_subfilter"] and x["best_key"] == y["best_key"]
         assert np.allclose(x["mean"], y["mean"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("m", [128, 256, 512])
+@pytest.mark.parametrize("res", [0, 1, 2])
+@pytest.mark.parametrize("exch,t", [(0, 0), (1, 3), (2, 2), (3, 4)])
+def test_fused_equals_split(gpu, m, res, exch, t):
+    """The single-kernel step (one warp per sub-filter, resampling deferred to the
+    next launch) against the split pipeline with the same particles per thread."""
+    E = gpu
+    p, inputs, _ = uni_setup()
+    common = dict(particles_per_subfilter=m, num_subfilters=16, num_transfer=t, exchange=exch, resampler=res,
+                  particles_per_thread=m // 32)
+    fa, ea = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_SPLIT, **common)
+    fb, eb = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_FUSED, **common)
+    assert fb.info()["pipeline"] == E.PIPELINE_FUSED and fa.info()["pipeline"] == E.PIPELINE_SPLIT
+    sa, ka = fa.sorted()
+    sb, kb = fb.sorted()
+    assert np.array_equal(ka, kb) and np.array_equal(sa, sb)
+    assert np.array_equal(fa.particles(), fb.particles())
+    for x, y in zip(ea, eb):
+        assert x["best_subfilter"] == y["best_subfilter"] and x["best_key"] == y["best_key"]
+        assert np.array_equal(x["best"], y["best"])
+        assert np.allclose(x["mean"], y["mean"], rtol=1e-12, atol=1e-12)
+        assert abs(x["log_norm"] - y["log_norm"]) <= 1e-12 * abs(x["log_norm"])
 
 
 @pytest.mark.parametrize("rng_mode", [0, 1])
@@ -105,22 +131,24 @@ def test_snapshot_restore(gpu):
     assert all(np.array_equal(x["mean"], y["mean"]) for x, y in zip(a, b))
 
 
-def test_skipped_subfilters_keep_propagated_state(gpu, O):
+@pytest.mark.parametrize("m", [64, 128])
+def test_skipped_subfilters_keep_propagated_state(gpu, O, m):
     E = gpu
-    p, inputs, _ = uni_setup(steps=2)
-    f = E.ParticleFilter(UNI, p, particles_per_subfilter=64, num_subfilters=64, num_transfer=1, exchange=1,
+    p, inputs, _ = uni_setup(steps=3)
+    f = E.ParticleFilter(UNI, p, particles_per_subfilter=m, num_subfilters=64, num_transfer=1, exchange=1,
                          resampling_freq=0.5)
     f.record_selection(True)
-    f.step(inputs[0])
-    sel = f.selection().reshape(64, 64)
-    skipped = np.all(sel == -1, axis=1)
-    assert 10 < skipped.sum() < 54  # about half of the sub-filters skip at freq 0.5
-    assert np.all((sel[~skipped] >= 0) & (sel[~skipped] < 64))
-    st = f.particles().reshape(3, 64, 64)
-    srt, _ = f.sorted()
-    srt = srt.reshape(3, 64, 64)
-    for b in np.flatnonzero(skipped):  # unsorted propagated particles = a permutation of the sorted ones
-        assert np.array_equal(np.sort(st[0, b]), np.sort(srt[0, b]))
+    for k in range(2):
+        f.step(inputs[k])
+        sel = f.selection().reshape(64, m)
+        skipped = np.all(sel == -1, axis=1)
+        assert 10 < skipped.sum() < 54  # about half of the sub-filters skip at freq 0.5
+        assert np.all((sel[~skipped] >= 0) & (sel[~skipped] < m))
+        st = f.particles().reshape(3, 64, m)
+        srt, _ = f.sorted()
+        srt = srt.reshape(3, 64, m)
+        for b in np.flatnonzero(skipped):  # unsorted propagated particles = a permutation of the sorted ones
+            assert np.array_equal(np.sort(st[0, b]), np.sort(srt[0, b]))
 
 
 def rmse_xy(ests, truth):
