@@ -36,7 +36,8 @@ class PFConfig(C.Structure):
                 ("num_transfer", C.c_int32), ("exchange", C.c_int32), ("resampler", C.c_int32),
                 ("resampling_freq", C.c_float), ("seed", C.c_uint32), ("rng", C.c_int32),
                 ("mtgp_streams", C.c_int32), ("mtgp_mask", C.c_uint32), ("log_weights", C.c_int32),
-                ("pipeline", C.c_int32), ("particles_per_thread", C.c_int32), ("device", C.c_int32)]
+                ("pipeline", C.c_int32), ("particles_per_thread", C.c_int32), ("device", C.c_int32),
+                ("stream_offset", C.c_int32), ("exchange_period", C.c_int32)]
 
 
 class StepInput(C.Structure):
@@ -126,6 +127,17 @@ def _declare(L):
         "pf_snapshot_size": (C.c_int64, [P]),
         "pf_snapshot": (C.c_int, [P, P]),
         "pf_restore": (C.c_int, [P, P]),
+        "pf_batch_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, C.POINTER(P)]),
+        "pf_batch_destroy": (C.c_int, [P]),
+        "pf_batch_set_initial_states": (C.c_int, [P, fp]),
+        "pf_batch_get_particles": (C.c_int, [P, C.c_int32, fp]),
+        "pf_batch_step": (C.c_int, [P, P, P]),
+        "pf_batch_submit": (C.c_int, [P, P, P, C.c_int32, C.c_int32]),
+        "pf_batch_poll": (C.c_int, [P, ip]),
+        "pf_batch_synchronize": (C.c_int, [P]),
+        "pf_batch_stream": (P, [P]),
+        "pf_batch_info": (C.c_int, [P, ip, C.POINTER(C.c_int64), ip, ip, C.POINTER(C.c_int64)]),
+        "pf_batch_filter_info": (C.c_int, [P, C.c_int32, ip, ip, C.POINTER(C.c_int64)]),
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
         "pfk_boxmuller": (C.c_int, [fp, C.c_int64]),
         "pfk_bitonic_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32]),
@@ -350,6 +362,84 @@ class ParticleFilter:
     def restore(self, buf):
         b = np.ascontiguousarray(buf, np.uint8)
         check(lib().pf_restore(self._h, b.ctypes.data_as(C.c_void_p)))
+
+
+class FilterBatch:
+    """Many independent filters of uneven particle counts stepped together
+    (pf_batch_*).  params: a sequence of per-filter model parameter structs."""
+
+    def __init__(self, model, params, num_particles, config=None, **cfg):
+        self.model = model
+        self.config = config if config is not None else default_config(**cfg)
+        self.num_state, self.num_noise, _, _ = model_info(model)
+        self.counts = np.ascontiguousarray(num_particles, np.int32)
+        self.F = len(self.counts)
+        if len(params) != self.F:
+            raise ValueError("one parameter struct per filter")
+        ptype = type(params[0])
+        arr = (ptype * self.F)(*params)
+        h = C.c_void_p()
+        check(lib().pf_batch_create(C.byref(self.config), model, self.F, _iptr(self.counts), C.cast(arr, C.c_void_p),
+                                    C.sizeof(ptype), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        nf, tp, ns, e, b = C.c_int32(), C.c_int64(), C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib().pf_batch_info(self._h, C.byref(nf), C.byref(tp), C.byref(ns), C.byref(e), C.byref(b)))
+        return {"num_filters": nf.value, "total_particles": tp.value, "total_subfilters": ns.value,
+                "particles_per_thread": e.value, "device_bytes": b.value}
+
+    def filter_info(self, f):
+        n, so, po = C.c_int32(), C.c_int32(), C.c_int64()
+        check(lib().pf_batch_filter_info(self._h, f, C.byref(n), C.byref(so), C.byref(po)))
+        return {"num_subfilters": n.value, "stream_offset": so.value, "particle_offset": po.value}
+
+    def set_initial_states(self, states):
+        a = _f32(states).reshape(self.F, self.num_state)
+        check(lib().pf_batch_set_initial_states(self._h, _fptr(a)))
+
+    def particles(self, f):
+        a = np.zeros((self.num_state, int(self.counts[f])), np.float32)
+        check(lib().pf_batch_get_particles(self._h, f, _fptr(a)))
+        return a
+
+    def step(self, inputs):
+        """One step of every filter; inputs: STEP_INPUT_DTYPE array [F]; returns ESTIMATE_DTYPE [F]."""
+        a = np.ascontiguousarray(inputs, STEP_INPUT_DTYPE)
+        out = np.zeros(self.F, ESTIMATE_DTYPE)
+        check(lib().pf_batch_step(self._h, a.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def submit(self, d_inputs_ptr, d_estimates_ptr, capacity, steps):
+        check(lib().pf_batch_submit(self._h, C.c_void_p(d_inputs_ptr), C.c_void_p(d_estimates_ptr), capacity, steps))
+
+    def poll(self):
+        d = C.c_int32()
+        check(lib().pf_batch_poll(self._h, C.byref(d)))
+        return bool(d.value)
+
+    def synchronize(self):
+        check(lib().pf_batch_synchronize(self._h))
+
+    def stream(self):
+        return lib().pf_batch_stream(self._h)
 
 
 def particle_filter(num_particles, num_blocks, num_transfer, resampling_freq, input_file):

@@ -9,16 +9,17 @@
 #include <unordered_set>
 #include <vector>
 
-#include "pf_launch.cuh"
+#include "pf_host.cuh"
 
 using namespace pfdev;
+using namespace pfhost;
 
 // ---------------------------------------------------------------------------
 // errors
 // ---------------------------------------------------------------------------
 static thread_local std::string g_err;
 
-static pf_status fail(pf_status s, const char* fmt, ...)
+pf_status pfhost::fail(pf_status s, const char* fmt, ...)
 {
     char buf[512];
     va_list ap;
@@ -28,14 +29,6 @@ static pf_status fail(pf_status s, const char* fmt, ...)
     g_err = buf;
     return s;
 }
-
-#define CU(call)                                                                                    \
-    do {                                                                                            \
-        cudaError_t e_ = (call);                                                                    \
-        if (e_ != cudaSuccess)                                                                      \
-            return fail(e_ == cudaErrorMemoryAllocation ? PF_ERR_NOMEM : PF_ERR_CUDA, "%s: %s (%s:%d)", \
-                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
-    } while (0)
 
 extern "C" const char* pf_last_error(void) { return g_err.c_str(); }
 
@@ -70,7 +63,7 @@ extern "C" int32_t pf_device_count(void)
     return n;
 }
 
-static pf_status require_gpu(int device)
+pf_status pfhost::require_gpu(int device)
 {
     const int n = pf_device_count();
     if (n <= 0) return fail(PF_ERR_CUDA, "no CUDA device available (this engine has no CPU path)");
@@ -82,12 +75,8 @@ static pf_status require_gpu(int device)
 // ---------------------------------------------------------------------------
 // model table
 // ---------------------------------------------------------------------------
-struct ModelInfo {
-    int S, K, C, Z;
-    size_t psize;
-};
 
-static bool model_info(int model, ModelInfo* mi)
+bool pfhost::model_info(int model, ModelInfo* mi)
 {
     switch (model) {
     case PF_MODEL_UNICYCLE: *mi = {Unicycle::S, Unicycle::K, 2, 16, sizeof(pf_unicycle_params)}; return true;
@@ -108,7 +97,7 @@ extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, in
     return PF_OK;
 }
 
-static const float* init_state_of(int model, const ModelParams& mp)
+const float* pfhost::init_state_of(int model, const ModelParams& mp)
 {
     switch (model) {
     case PF_MODEL_UNICYCLE: return mp.uni.init_state;
@@ -117,18 +106,13 @@ static const float* init_state_of(int model, const ModelParams& mp)
     }
 }
 
-// Launch dispatch over the model template.
-struct ModelOps {
-    cudaError_t (*sample_sort)(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
-    cudaError_t (*sample_weight)(int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
-    cudaError_t (*block_sort)(int, int, int, cudaStream_t, const FilterDesc*, const int2*);
-    cudaError_t (*exchange_resample)(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef,
-                                     int32_t*, int);
-    cudaError_t (*exchange_inplace)(int, int, cudaStream_t, const FilterDesc*, const int2*);
-    cudaError_t (*test_model)(const ModelParams&, const pf_step_input*, int, float*, const float*, float*,
-                              cudaStream_t);
-    cudaError_t (*step)(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
-};
+
+uint32_t pfhost::angle_mask_of(int model)
+{
+    return model == PF_MODEL_UNICYCLE ? 0x4u : (model == PF_MODEL_DHARM ? 0x3fu : 0x1fu);
+}
+
+int pfhost::angle_count_of(int model) { return model == PF_MODEL_UNICYCLE ? 1 : (model == PF_MODEL_DHARM ? 6 : 5); }
 
 template <class Mdl>
 static ModelOps ops_of()
@@ -138,7 +122,7 @@ static ModelOps ops_of()
             Launch<Mdl>::step};
 }
 
-static ModelOps model_ops(int model)
+ModelOps pfhost::model_ops(int model)
 {
     if (model == PF_MODEL_UNICYCLE) return ops_of<Unicycle>();
     if (model == PF_MODEL_DHARM) return ops_of<DhArm>();
@@ -154,7 +138,7 @@ static const uint32_t kHostParams[200 * 52] = {
 #include "mtgp32_params_11213.inc"
 };
 
-static void mtgp_init_state_host(uint32_t* st, int set, uint32_t seed)
+void pfhost::mtgp_init_state_host(uint32_t* st, int set, uint32_t seed)
 {
     const uint32_t* tbl = kHostParams + set * 52 + 4;
     const uint32_t hidden = tbl[4] ^ (tbl[8] << 16);
@@ -260,6 +244,8 @@ extern "C" pf_status pf_config_default(pf_config* c)
     c->pipeline = PF_PIPELINE_FUSED;
     c->particles_per_thread = 0;
     c->device = 0;
+    c->stream_offset = 0;
+    c->exchange_period = 1;
     return PF_OK;
 }
 
@@ -270,15 +256,13 @@ static int default_ppt(int M)
     return 2;
 }
 
-static void torus_dims(int N, int* dx, int* dy)
+void pfhost::torus_dims(int N, int* dx, int* dy)
 {
     int x = 1;
     while ((int64_t)(2 * x) * (2 * x) <= N) x *= 2;
     *dx = x;
     *dy = N / x;
 }
-
-static void torus_dims(int N, int* dx, int* dy);
 
 static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, int* E)
 {
@@ -308,6 +292,10 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
     if (!(c->resampling_freq >= 0.0f && c->resampling_freq <= 1.0f))
         return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
     if (c->rng != PF_RNG_SUBFILTER && c->rng != PF_RNG_REFLAYOUT) return fail(PF_ERR_INVALID, "unknown rng layout");
+    if (c->stream_offset < 0) return fail(PF_ERR_INVALID, "stream_offset must be >= 0");
+    if (c->exchange_period < 0) return fail(PF_ERR_INVALID, "exchange_period must be >= 0");
+    if (c->exchange_period > 1 && c->pipeline == PF_PIPELINE_PHASED)
+        return fail(PF_ERR_UNSUPPORTED, "the phased pipeline exchanges every step (exchange_period <= 1)");
     if (c->rng == PF_RNG_REFLAYOUT && (c->mtgp_streams < 1 || c->mtgp_streams > 200))
         return fail(PF_ERR_INVALID, "mtgp_streams must be in [1, 200]");
     if (c->pipeline == PF_PIPELINE_PHASED && c->rng != PF_RNG_REFLAYOUT)
@@ -315,6 +303,7 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
     if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED && c->pipeline != PF_PIPELINE_SPLIT)
         return fail(PF_ERR_INVALID, "unknown pipeline");
     const bool fused = c->pipeline == PF_PIPELINE_FUSED && c->rng == PF_RNG_SUBFILTER && step_supported(M) &&
+                       c->exchange_period <= 1 &&
                        (c->particles_per_thread == 0 || c->particles_per_thread == M / 32);
     *E = fused ? M / 32 : (c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M));
     if (!fused && !me_supported(M, *E))
@@ -354,7 +343,8 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.nbm = (int32_t)f->nbm;
     D.ru_stride = (int32_t)(f->draws - f->nbm);
     D.mask = f->cfg.mtgp_mask;
-    D.stream_base = 0;
+    D.stream_base = f->cfg.stream_offset;
+    D.exch_period = f->cfg.exchange_period;
     D.freq = f->cfg.resampling_freq;
     D.nnorm = (int64_t)f->mi.K * f->T;
     D.est_ctr = f->est_ctr;
@@ -375,7 +365,7 @@ static pf_status upload_descs(pf_filter* f, pf_estimate* run_est)
     return PF_OK;
 }
 
-static int64_t resample_draws(int res, int M)
+int64_t pfhost::resample_draws(int res, int M)
 {
     return res == PF_RESAMPLE_REFERENCE ? M : (res == PF_RESAMPLE_VOSE ? 2 * (int64_t)M : 1);
 }
@@ -383,8 +373,10 @@ static int64_t resample_draws(int res, int M)
 static pf_status init_streams(pf_filter* f)
 {
     std::vector<uint32_t> st((size_t)f->streams * kMtgpN);
+    const int off = f->cfg.rng == PF_RNG_SUBFILTER ? f->cfg.stream_offset : 0;
     for (int g = 0; g < f->streams; ++g)
-        mtgp_init_state_host(st.data() + (size_t)g * kMtgpN, g % kMtgpSets, f->cfg.seed + (uint32_t)g + 1u);
+        mtgp_init_state_host(st.data() + (size_t)g * kMtgpN, (off + g) % kMtgpSets,
+                             f->cfg.seed + (uint32_t)(off + g) + 1u);
     CU(cudaMemcpy(f->mtgp, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
     return PF_OK;
 }
@@ -419,12 +411,12 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     memcpy(&f->mp, params, params_size);
     f->mi = mi;
     f->ops = model_ops(model);
-    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER &&
+    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER && cfg->exchange_period <= 1 &&
                step_supported(cfg->particles_per_subfilter) && E == cfg->particles_per_subfilter / 32)
                   ? PF_PIPELINE_FUSED
                   : (cfg->pipeline == PF_PIPELINE_PHASED ? PF_PIPELINE_PHASED : PF_PIPELINE_SPLIT);
-    f->angle_mask = model == PF_MODEL_UNICYCLE ? 0x4u : (model == PF_MODEL_DHARM ? 0x3fu : 0x1fu);
-    f->na = model == PF_MODEL_UNICYCLE ? 1 : (model == PF_MODEL_DHARM ? 6 : 5);
+    f->angle_mask = angle_mask_of(model);
+    f->na = angle_count_of(model);
     f->M = cfg->particles_per_subfilter;
     f->E = E;
     f->N = cfg->num_subfilters;
@@ -720,7 +712,7 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     CU(cudaSetDevice(f->cfg.device));
     *f->h_in = *in;
     CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
-    InputRef ir{f->d_in, 0, nullptr, 0};
+    InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
     pf_status s = enqueue_step(f, f->d_desc, ir, nullptr);
     if (s != PF_OK) return s;
     CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate), cudaMemcpyDeviceToHost, f->stream));

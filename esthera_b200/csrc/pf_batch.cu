@@ -1,0 +1,504 @@
+// pf_batch.cu -- batched filters (include/esthera_b200.h, pf_batch_*): many
+// independent filters of uneven particle counts stepped by one sequence of
+// launches.  All filters share the model, the sub-filter size m, the
+// resampler and the exchange settings; each has its own particle count (a
+// multiple of m), model parameters, MTGP32 streams, inputs and estimates.
+//
+// One CTA per sub-filter of every filter: a CTA -> (filter, sub-filter) map
+// drives the split pipeline's two kernels (k_sample_sort, k_exchange_resample)
+// over the whole batch, the exchange stays inside each filter, and a run of
+// many steps is captured once into a CUDA graph and replayed by one launch.
+// Sub-filter b of filter f draws from stream stream_offset + first(f) + b,
+// first(f) = the number of sub-filters of filters 0..f-1, so filter f alone
+// (pf_create with that stream offset) reproduces its batched results exactly.
+#include <cstring>
+#include <vector>
+
+#include "pf_host.cuh"
+
+using namespace pfdev;
+using namespace pfhost;
+
+namespace {
+
+// Fills every particle of filter f with init[f * S + v].
+__global__ void k_batch_fill(const FilterDesc* __restrict__ descs, const int2* __restrict__ map,
+                             const float* __restrict__ init, int S)
+{
+    int f, b;
+    cta_target(map, f, b);
+    const FilterDesc& D = descs[f];
+    for (int v = 0; v < S; ++v) {
+        const float x = init[(int64_t)f * S + v];
+        float* dst = D.state + v * D.T + (int64_t)b * D.M;
+        for (int i = threadIdx.x; i < D.M; i += blockDim.x) dst[i] = x;
+    }
+}
+
+// Advances the run's step counter once every filter's step is enqueued before it.
+__global__ void k_counter_inc(int32_t* ctr)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *ctr += 1;
+}
+
+constexpr int kMaxGraphSteps = 256;
+
+}  // namespace
+
+struct pf_batch {
+    pf_config cfg;
+    int model = 0;
+    ModelInfo mi{};
+    ModelOps ops{};
+    int F = 0, M = 0, E = 0, S = 0, t = 0;
+    int64_t P = 0;   // particles in all filters
+    int NS = 0;      // sub-filters in all filters
+    std::vector<int32_t> nsub, sub_off, grp_off;  // grp_off: first estimate group (32 sub-filters) of a filter
+    std::vector<int64_t> part_off;
+    std::vector<ModelParams> mp;
+    int64_t nbm = 0, draws = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    int64_t dev_bytes = 0;
+    float *state = nullptr, *tmp = nullptr, *tkey = nullptr, *winner = nullptr, *ru = nullptr;
+    double *part = nullptr, *gpart = nullptr;
+    uint32_t* mtgp = nullptr;
+    int32_t *est_ctr = nullptr, *ctr = nullptr;
+    int2* map = nullptr;
+    FilterDesc* d_desc = nullptr;  // [0, F): pf_batch_step, [F, 2F): pf_batch_submit
+    pf_step_input* d_in = nullptr;
+    pf_estimate* d_est = nullptr;
+    pf_step_input* h_in = nullptr;
+    pf_estimate* h_est = nullptr;
+    int32_t steps_done = 0;
+    cudaGraphExec_t graph_n = nullptr, graph_1 = nullptr;
+    int graph_steps = 0;
+    const pf_step_input* graph_inputs = nullptr;
+    pf_estimate* graph_est = nullptr;
+    int32_t graph_cap = 0;
+};
+
+template <class T>
+static pf_status balloc(pf_batch* B, T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return PF_OK;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PF_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    }
+    B->allocs.push_back(q);
+    B->dev_bytes += (int64_t)(count * sizeof(T));
+    *p = static_cast<T*>(q);
+    return PF_OK;
+}
+
+static void drop_graphs(pf_batch* B)
+{
+    if (B->graph_n) cudaGraphExecDestroy(B->graph_n);
+    if (B->graph_1) cudaGraphExecDestroy(B->graph_1);
+    B->graph_n = B->graph_1 = nullptr;
+    B->graph_steps = 0;
+}
+
+static void release(pf_batch* B)
+{
+    if (!B) return;
+    drop_graphs(B);
+    for (void* p : B->allocs) cudaFree(p);
+    if (B->h_in) cudaFreeHost(B->h_in);
+    if (B->h_est) cudaFreeHost(B->h_est);
+    if (B->stream) cudaStreamDestroy(B->stream);
+    delete B;
+}
+
+static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate* est)
+{
+    memset(&D, 0, sizeof(D));
+    const int64_t p0 = B->part_off[f];
+    const int64_t s0 = B->sub_off[f];
+    const int N = B->nsub[f];
+    D.T = (int64_t)B->M * N;
+    D.state = B->state + (int64_t)B->S * p0;
+    D.tmp = B->tmp + (int64_t)B->S * p0;
+    D.tkey = B->tkey + p0;
+    D.winner = B->winner + s0;
+    D.part = B->part + s0 * kPartStride;
+    D.mtgp = B->mtgp + s0 * kMtgpN;
+    D.ru = B->ru + s0 * (B->draws - B->nbm);
+    D.est = est;
+    D.N = N;
+    D.M = B->M;
+    D.t = B->t;
+    D.exchange = B->cfg.exchange;
+    D.resampler = B->cfg.resampler;
+    torus_dims(N, &D.dx, &D.dy);
+    D.log_weights = B->cfg.log_weights ? 1 : 0;
+    D.inplace = B->cfg.resampling_freq < 1.0f ? 1 : 0;
+    D.rng_fused = 1;
+    D.draws = (int32_t)B->draws;
+    D.nbm = (int32_t)B->nbm;
+    D.ru_stride = (int32_t)(B->draws - B->nbm);
+    D.mask = B->cfg.mtgp_mask;
+    D.stream_base = B->cfg.stream_offset + (int32_t)s0;
+    D.exch_period = B->cfg.exchange_period;
+    D.freq = B->cfg.resampling_freq;
+    D.nnorm = (int64_t)B->mi.K * D.T;
+    D.est_ctr = B->est_ctr + f;
+    D.gpart = B->gpart + (int64_t)B->grp_off[f] * kPartStride;
+    D.angle_mask = angle_mask_of(B->model);
+    D.na = angle_count_of(B->model);
+    D.mp = B->mp[f];
+}
+
+static pf_status upload_batch_descs(pf_batch* B, pf_estimate* run_est, int32_t cap)
+{
+    std::vector<FilterDesc> d(2 * (size_t)B->F);
+    for (int f = 0; f < B->F; ++f) {
+        fill_batch_desc(B, f, d[f], B->d_est + f);
+        fill_batch_desc(B, f, d[B->F + f], run_est ? run_est + (int64_t)f * cap : nullptr);
+    }
+    CU(cudaMemcpyAsync(B->d_desc, d.data(), d.size() * sizeof(FilterDesc), cudaMemcpyHostToDevice, B->stream));
+    CU(cudaStreamSynchronize(B->stream));
+    return PF_OK;
+}
+
+static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRef in, int32_t* ctr_inc)
+{
+    const int M = B->M, E = B->E;
+    CU(B->ops.sample_sort(M, E, true, B->NS, B->stream, desc, B->map, in));
+    CU(B->ops.exchange_resample(M, E, B->cfg.resampler, B->NS, B->stream, desc, B->map, in, nullptr, 1));
+    if (ctr_inc) {
+        k_counter_inc<<<1, 32, 0, B->stream>>>(ctr_inc);
+        CU(cudaGetLastError());
+    }
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, int32_t num_filters,
+                                     const int32_t* num_particles, const void* params, size_t params_size,
+                                     pf_batch** out)
+{
+    if (!cfg || !num_particles || !params || !out) return fail(PF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    if (params_size != mi.psize)
+        return fail(PF_ERR_INVALID, "model params size %zu, expected %zu", params_size, mi.psize);
+    if (num_filters < 1) return fail(PF_ERR_INVALID, "num_filters must be >= 1");
+    const int M = cfg->particles_per_subfilter;
+    if (M < 32 || M > 1024 || (M & (M - 1)))
+        return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
+    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : 2;
+    if (!me_supported(M, E)) return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E, M);
+    if (cfg->rng != PF_RNG_SUBFILTER) return fail(PF_ERR_UNSUPPORTED, "batched filters use per-sub-filter streams");
+    if (cfg->pipeline == PF_PIPELINE_PHASED)
+        return fail(PF_ERR_UNSUPPORTED, "batched filters run the split pipeline, not the phased one");
+    if (cfg->exchange != PF_EXCHANGE_NONE && cfg->exchange != PF_EXCHANGE_RING && cfg->exchange != PF_EXCHANGE_TORUS)
+        return fail(PF_ERR_UNSUPPORTED, "batched filters exchange by ring or torus (or not at all)");
+    if (cfg->num_transfer < 0) return fail(PF_ERR_INVALID, "num_transfer must be >= 0");
+    if (cfg->exchange == PF_EXCHANGE_RING && 2 * cfg->num_transfer > M)
+        return fail(PF_ERR_INVALID, "exchange needs 2*t <= m (t=%d, m=%d)", cfg->num_transfer, M);
+    if (cfg->exchange == PF_EXCHANGE_TORUS && 5 * cfg->num_transfer > M)
+        return fail(PF_ERR_INVALID, "torus exchange needs 5*t <= m (t=%d, m=%d)", cfg->num_transfer, M);
+    if (cfg->resampler < PF_RESAMPLE_REFERENCE || cfg->resampler > PF_RESAMPLE_VOSE)
+        return fail(PF_ERR_INVALID, "unknown resampler %d", cfg->resampler);
+    if (!(cfg->resampling_freq >= 0.0f && cfg->resampling_freq <= 1.0f))
+        return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
+    if (cfg->stream_offset < 0 || cfg->exchange_period < 0)
+        return fail(PF_ERR_INVALID, "stream_offset and exchange_period must be >= 0");
+    int64_t P = 0, NS = 0;
+    for (int f = 0; f < num_filters; ++f) {
+        const int32_t n = num_particles[f];
+        if (n < M || n % M) return fail(PF_ERR_INVALID, "filter %d: %d particles is not a multiple of m=%d", f, n, M);
+        const int N = n / M;
+        if (cfg->exchange == PF_EXCHANGE_TORUS) {
+            int dx, dy;
+            torus_dims(N, &dx, &dy);
+            if (dx * dy != N)
+                return fail(PF_ERR_INVALID, "filter %d: torus exchange needs N = dx*dy (N=%d)", f, N);
+        }
+        P += n;
+        NS += N;
+    }
+    if (NS > INT32_MAX / 2 || P > ((int64_t)1 << 34)) return fail(PF_ERR_INVALID, "batch too large");
+    pf_status s = require_gpu(cfg->device);
+    if (s != PF_OK) return s;
+
+    pf_batch* B = new pf_batch();
+    B->cfg = *cfg;
+    B->model = model;
+    B->mi = mi;
+    B->ops = model_ops(model);
+    B->F = num_filters;
+    B->M = M;
+    B->E = E;
+    B->S = mi.S;
+    B->t = cfg->exchange == PF_EXCHANGE_NONE ? 0 : cfg->num_transfer;
+    B->P = P;
+    B->NS = (int)NS;
+    B->nsub.resize(num_filters);
+    B->sub_off.resize(num_filters);
+    B->part_off.resize(num_filters);
+    B->grp_off.resize(num_filters);
+    B->mp.resize(num_filters);
+    int64_t po = 0;
+    int so = 0, go = 0;
+    for (int f = 0; f < num_filters; ++f) {
+        B->nsub[f] = num_particles[f] / M;
+        B->sub_off[f] = so;
+        B->part_off[f] = po;
+        B->grp_off[f] = go;
+        so += B->nsub[f];
+        go += (B->nsub[f] + 31) / 32;
+        po += num_particles[f];
+        memset(&B->mp[f], 0, sizeof(ModelParams));
+        memcpy(&B->mp[f], static_cast<const char*>(params) + (size_t)f * params_size, params_size);
+        if (model == PF_MODEL_UNICYCLE) {
+            const pf_unicycle_params& p = B->mp[f].uni;
+            if (p.num_landmarks < 1 || p.num_landmarks > 8 || !(p.sigma_range > 0) || !(p.sigma_bearing > 0)) {
+                release(B);
+                return fail(PF_ERR_INVALID, "filter %d: 1..8 landmarks and positive sigmas", f);
+            }
+        }
+    }
+    B->nbm = 2 * (((int64_t)mi.K * M + 1) / 2);
+    B->draws = B->nbm + 1 + resample_draws(cfg->resampler, M);
+    cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        release(B);
+        return fail(PF_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+#define TRY(x)              \
+    do {                    \
+        pf_status s_ = (x); \
+        if (s_ != PF_OK) {  \
+            release(B);     \
+            return s_;      \
+        }                   \
+    } while (0)
+    TRY(balloc(B, &B->state, (size_t)B->S * P));
+    TRY(balloc(B, &B->tmp, (size_t)B->S * P));
+    TRY(balloc(B, &B->tkey, (size_t)P));
+    TRY(balloc(B, &B->winner, (size_t)NS));
+    TRY(balloc(B, &B->part, (size_t)NS * kPartStride));
+    TRY(balloc(B, &B->mtgp, (size_t)NS * kMtgpN));
+    TRY(balloc(B, &B->ru, (size_t)NS * (B->draws - B->nbm)));
+    TRY(balloc(B, &B->gpart, (size_t)go * kPartStride));
+    TRY(balloc(B, &B->est_ctr, (size_t)num_filters));
+    TRY(balloc(B, &B->ctr, 1));
+    TRY(balloc(B, &B->map, (size_t)NS));
+    TRY(balloc(B, &B->d_desc, 2 * (size_t)num_filters));
+    TRY(balloc(B, &B->d_in, (size_t)num_filters));
+    TRY(balloc(B, &B->d_est, (size_t)num_filters));
+    if (cudaMallocHost(&B->h_in, sizeof(pf_step_input) * num_filters) != cudaSuccess ||
+        cudaMallocHost(&B->h_est, sizeof(pf_estimate) * num_filters) != cudaSuccess) {
+        cudaGetLastError();
+        release(B);
+        return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
+    }
+    {
+        std::vector<int2> map((size_t)NS);
+        for (int f = 0; f < num_filters; ++f)
+            for (int b = 0; b < B->nsub[f]; ++b) map[(size_t)B->sub_off[f] + b] = make_int2(f, b);
+        std::vector<uint32_t> st((size_t)kMtgpN * 4096);
+        for (int64_t g0 = 0; g0 < NS; g0 += 4096) {
+            const int n = (int)std::min<int64_t>(4096, NS - g0);
+            for (int i = 0; i < n; ++i) {
+                const int g = cfg->stream_offset + (int)(g0 + i);
+                mtgp_init_state_host(st.data() + (size_t)i * kMtgpN, g % kMtgpSets, cfg->seed + (uint32_t)g + 1u);
+            }
+            if (cudaMemcpy(B->mtgp + g0 * kMtgpN, st.data(), (size_t)n * kMtgpN * 4, cudaMemcpyHostToDevice) !=
+                    cudaSuccess ||
+                (g0 == 0 &&
+                 cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)) {
+                cudaGetLastError();
+                release(B);
+                return fail(PF_ERR_CUDA, "initial upload failed");
+            }
+        }
+    }
+    if (cudaMemset(B->est_ctr, 0, 4 * (size_t)num_filters) != cudaSuccess || cudaMemset(B->ctr, 0, 4) != cudaSuccess) {
+        cudaGetLastError();
+        release(B);
+        return fail(PF_ERR_CUDA, "cudaMemset failed");
+    }
+    TRY(upload_batch_descs(B, nullptr, 0));
+    {
+        std::vector<float> init((size_t)num_filters * B->S);
+        for (int f = 0; f < num_filters; ++f)
+            memcpy(init.data() + (size_t)f * B->S, init_state_of(model, B->mp[f]), sizeof(float) * B->S);
+        TRY(pf_batch_set_initial_states(B, init.data()));
+    }
+#undef TRY
+    *out = B;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_destroy(pf_batch* B)
+{
+    if (!B) return PF_OK;
+    cudaSetDevice(B->cfg.device);
+    cudaStreamSynchronize(B->stream);
+    release(B);
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_set_initial_states(pf_batch* B, const float* states)
+{
+    if (!B || !states) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(B->cfg.device));
+    CU(cudaStreamSynchronize(B->stream));
+    float* d = nullptr;
+    CU(cudaMalloc(&d, sizeof(float) * B->S * B->F));
+    cudaError_t e = cudaMemcpy(d, states, sizeof(float) * B->S * B->F, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_batch_fill<<<B->NS, 256, 0, B->stream>>>(B->d_desc, B->map, d, B->S);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "set initial states: %s", cudaGetErrorString(e));
+    B->steps_done = 0;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_get_particles(pf_batch* B, int32_t filter, float* soa)
+{
+    if (!B || !soa) return fail(PF_ERR_INVALID, "null argument");
+    if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
+    CU(cudaSetDevice(B->cfg.device));
+    CU(cudaStreamSynchronize(B->stream));
+    const int64_t T = (int64_t)B->M * B->nsub[filter];
+    for (int v = 0; v < B->S; ++v)
+        CU(cudaMemcpy(soa + v * T, B->state + (int64_t)B->S * B->part_off[filter] + v * T, (size_t)T * 4,
+                      cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_step(pf_batch* B, const pf_step_input* inputs, pf_estimate* out)
+{
+    if (!B || !inputs) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(B->cfg.device));
+    memcpy(B->h_in, inputs, sizeof(pf_step_input) * B->F);
+    CU(cudaMemcpyAsync(B->d_in, B->h_in, sizeof(pf_step_input) * B->F, cudaMemcpyHostToDevice, B->stream));
+    InputRef ir{B->d_in, 1, nullptr, 0, B->steps_done};
+    pf_status s = enqueue_batch_step(B, B->d_desc, ir, nullptr);
+    if (s != PF_OK) return s;
+    if (out) CU(cudaMemcpyAsync(B->h_est, B->d_est, sizeof(pf_estimate) * B->F, cudaMemcpyDeviceToHost, B->stream));
+    CU(cudaStreamSynchronize(B->stream));
+    B->steps_done++;
+    if (out) {
+        memcpy(out, B->h_est, sizeof(pf_estimate) * B->F);
+        for (int f = 0; f < B->F; ++f) out[f].step = B->steps_done;
+    }
+    return PF_OK;
+}
+
+static pf_status capture(pf_batch* B, int steps, InputRef ir, cudaGraphExec_t* exec)
+{
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    pf_status s = PF_OK;
+    for (int i = 0; i < steps && s == PF_OK; ++i) s = enqueue_batch_step(B, B->d_desc + B->F, ir, B->ctr);
+    cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    if (s != PF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *exec = nullptr;
+        return fail(PF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_submit(pf_batch* B, const pf_step_input* d_inputs, pf_estimate* d_estimates,
+                                     int32_t capacity, int32_t steps)
+{
+    if (!B || !d_inputs || !d_estimates || capacity < 1 || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
+    CU(cudaSetDevice(B->cfg.device));
+    if (B->graph_inputs != d_inputs || B->graph_est != d_estimates || B->graph_cap != capacity) {
+        CU(cudaStreamSynchronize(B->stream));
+        drop_graphs(B);
+        pf_status s = upload_batch_descs(B, d_estimates, capacity);
+        if (s != PF_OK) return s;
+        B->graph_inputs = d_inputs;
+        B->graph_est = d_estimates;
+        B->graph_cap = capacity;
+    }
+    InputRef ir{d_inputs, capacity, B->ctr, capacity, 0};
+    if (!B->graph_n && steps > 0) {
+        B->graph_steps = steps < kMaxGraphSteps ? steps : kMaxGraphSteps;
+        pf_status s = capture(B, B->graph_steps, ir, &B->graph_n);
+        if (s != PF_OK) return s;
+    }
+    if (!B->graph_1 && steps % (B->graph_steps > 0 ? B->graph_steps : 1) != 0) {
+        pf_status s = capture(B, 1, ir, &B->graph_1);
+        if (s != PF_OK) return s;
+    }
+    CU(cudaMemsetAsync(B->ctr, 0, sizeof(int32_t), B->stream));
+    int left = steps;
+    while (left >= B->graph_steps && B->graph_steps > 0) {
+        CU(cudaGraphLaunch(B->graph_n, B->stream));
+        left -= B->graph_steps;
+    }
+    for (; left > 0; --left) CU(cudaGraphLaunch(B->graph_1, B->stream));
+    B->steps_done += steps;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_poll(pf_batch* B, int32_t* done)
+{
+    if (!B || !done) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(B->cfg.device));
+    const cudaError_t e = cudaStreamQuery(B->stream);
+    if (e == cudaSuccess) {
+        *done = 1;
+        return PF_OK;
+    }
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        *done = 0;
+        return PF_OK;
+    }
+    return fail(PF_ERR_CUDA, "pf_batch_poll: %s", cudaGetErrorString(e));
+}
+
+extern "C" pf_status pf_batch_synchronize(pf_batch* B)
+{
+    if (!B) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(B->cfg.device));
+    CU(cudaStreamSynchronize(B->stream));
+    return PF_OK;
+}
+
+extern "C" void* pf_batch_stream(pf_batch* B) { return B ? (void*)B->stream : nullptr; }
+
+extern "C" pf_status pf_batch_info(pf_batch* B, int32_t* num_filters, int64_t* total_particles,
+                                   int32_t* total_subfilters, int32_t* ppt, int64_t* bytes)
+{
+    if (!B) return fail(PF_ERR_INVALID, "null argument");
+    if (num_filters) *num_filters = B->F;
+    if (total_particles) *total_particles = B->P;
+    if (total_subfilters) *total_subfilters = B->NS;
+    if (ppt) *ppt = B->E;
+    if (bytes) *bytes = B->dev_bytes;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_filter_info(pf_batch* B, int32_t filter, int32_t* num_subfilters,
+                                          int32_t* stream_offset, int64_t* particle_offset)
+{
+    if (!B) return fail(PF_ERR_INVALID, "null argument");
+    if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
+    if (num_subfilters) *num_subfilters = B->nsub[filter];
+    if (stream_offset) *stream_offset = B->cfg.stream_offset + B->sub_off[filter];
+    if (particle_offset) *particle_offset = B->part_off[filter];
+    return PF_OK;
+}

@@ -44,6 +44,7 @@ struct FilterDesc {
     double* gpart;     // ceil(N/32) * kPartStride group partials
     uint32_t angle_mask;
     int32_t na;        // angular state variables (circular means)
+    int32_t exch_period;  // exchange on steps with step % period == 0 (<= 1: every step)
     ModelParams mp;
 };
 
@@ -52,21 +53,17 @@ struct InputRef {
     int64_t filter_stride;   // inputs per filter (batched: [filter][step])
     const int32_t* ctr;      // device step counter (graph replays) or null
     int32_t cap;             // inputs / estimates per filter: the counter indexes them modulo cap
+    int32_t step;            // step number of this step when there is no device counter
 };
+
+// Step number within the run: the device counter, else the host-given number.
+__device__ __forceinline__ int32_t run_step(const InputRef& in) { return in.ctr ? *in.ctr : in.step; }
 
 __device__ __forceinline__ int64_t step_index(const InputRef& in)
 {
     return in.ctr ? (int64_t)(*in.ctr % (in.cap > 0 ? in.cap : 1)) : 0;
 }
 
-template <int E>
-struct VecT;
-template <>
-struct VecT<1> { using T = float; };
-template <>
-struct VecT<2> { using T = float2; };
-template <>
-struct VecT<4> { using T = float4; };
 
 // E consecutive floats per thread: float4 chunks when E is a multiple of 4.
 template <int E>
@@ -635,7 +632,8 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     }
     __syncthreads();
     if (virt) {
-        const int nx = exchange_count(D);
+        int nx = exchange_count(D);
+        if (D.exch_period > 1 && (run_step(in) % D.exch_period) != 0) nx = 0;
         for (int x = tid; x < nx; x += NT) {
             const int64_t g = exchange_source(D, b, x);
             const int s = M - 1 - x;

@@ -94,8 +94,14 @@ typedef struct {
     uint32_t mtgp_mask;              /* PF_MTGP_MASK_PARAMS or PF_MTGP_MASK_CUDA_REF */
     int32_t log_weights;             /* 1: FP32 max-subtracted log weights; 0: linear FP32 weights */
     int32_t pipeline;                /* pf_pipeline */
-    int32_t particles_per_thread;    /* 0 = pick; 1, 2 or 4 */
+    int32_t particles_per_thread;    /* 0 = pick; 1, 2, 4 (8, 16 for m = 256, 512) */
     int32_t device;                  /* CUDA device ordinal */
+    int32_t stream_offset;           /* PF_RNG_SUBFILTER: sub-filter b uses stream offset + b (parameter
+                                        set (offset + b) mod 200, seed + offset + b + 1); 0 by default */
+    int32_t exchange_period;         /* exchange on run steps s with s mod period == 0 (<= 1: every step;
+                                        s counts pf_step calls since the initial state was set, or the
+                                        steps of the current pf_run_device run); single-kernel and
+                                        split pipelines only */
 } pf_config;
 
 /* One step's inputs.  control/meas are interpreted by the model:
@@ -201,6 +207,41 @@ pf_status pf_get_info(pf_filter* f, int32_t* pipeline, int32_t* particles_per_th
 int64_t pf_snapshot_size(pf_filter* f);
 pf_status pf_snapshot(pf_filter* f, void* host_buf);
 pf_status pf_restore(pf_filter* f, const void* host_buf);
+
+/* ---- batched filters: many independent filters of uneven sizes stepped together ----
+ * The reference runs one filter per process (particle_filter, pf_generic_soa.cu:686);
+ * these calls have no counterpart there.  Every filter shares cfg's model, m,
+ * resampler and exchange settings (exchange stays inside each filter: none,
+ * ring, or torus when every filter's N = dx*dy; all-to-all is not offered) and
+ * runs the split pipeline with per-sub-filter streams.  Filter f has
+ * num_particles[f] particles (a positive multiple of m) and params + f
+ * (params_size bytes each); its sub-filter b uses stream cfg.stream_offset +
+ * first(f) + b, first(f) = sub-filters of filters 0..f-1 (pf_batch_filter_info),
+ * so a pf_filter created with that stream_offset reproduces filter f exactly. */
+typedef struct pf_batch pf_batch;
+pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, int32_t num_filters,
+                          const int32_t* num_particles, const void* params, size_t params_size, pf_batch** out);
+pf_status pf_batch_destroy(pf_batch* b);
+/* states: num_filters x S floats (host); every particle of filter f starts at states[f*S..]. */
+pf_status pf_batch_set_initial_states(pf_batch* b, const float* states);
+/* Filter f's particles (host, SoA, S x num_particles[f]). */
+pf_status pf_batch_get_particles(pf_batch* b, int32_t filter, float* soa);
+/* One step of every filter from host inputs[num_filters]; estimates to out[num_filters] (may be NULL). */
+pf_status pf_batch_step(pf_batch* b, const pf_step_input* inputs, pf_estimate* out);
+/* Enqueues `steps` steps on the batch's stream and returns: step k of filter f
+ * reads d_inputs[f*capacity + k % capacity] and writes d_estimates[f*capacity +
+ * k % capacity] (device arrays).  The steps are captured once into a CUDA graph
+ * of up to 256 steps and replayed; pf_batch_poll reports completion without
+ * blocking, pf_batch_synchronize waits. */
+pf_status pf_batch_submit(pf_batch* b, const pf_step_input* d_inputs, pf_estimate* d_estimates,
+                          int32_t capacity, int32_t steps);
+pf_status pf_batch_poll(pf_batch* b, int32_t* done);
+pf_status pf_batch_synchronize(pf_batch* b);
+void* pf_batch_stream(pf_batch* b);
+pf_status pf_batch_info(pf_batch* b, int32_t* num_filters, int64_t* total_particles, int32_t* total_subfilters,
+                        int32_t* particles_per_thread, int64_t* device_bytes);
+pf_status pf_batch_filter_info(pf_batch* b, int32_t filter, int32_t* num_subfilters, int32_t* stream_offset,
+                               int64_t* particle_offset);
 
 /* ---- kernel-level entry points (device work on host arrays; used by parity tests) ---- */
 /* MTGP32 in the reference block layout: streams g = 0..G-1 with parameter set g,

@@ -1,0 +1,142 @@
+"""Batched filters of uneven particle counts (pf_batch_*) on the GPU through the
+C ABI: every filter of a batch reproduces, bit for bit, the same filter run
+alone (pf_create with the filter's stream offset) -- host-stepped and
+graph-replayed, with exchange every step or every few steps, ring or torus."""
+import numpy as np
+import pytest
+
+UNI = 0
+
+
+def batch_setup(E, counts, steps, seed0=4):
+    params = [E.unicycle_params(seed0 + i) for i in range(len(counts))]
+    traces = [E.make_trace(UNI, p, seed0 + i, steps) for i, p in enumerate(params)]
+    inputs = np.stack([t[0] for t in traces])          # [F, steps]
+    truth = np.stack([t[1] for t in traces])           # [F, steps, S]
+    return params, inputs, truth
+
+
+def single(E, p, cfg, stream_offset, n, m):
+    return E.ParticleFilter(UNI, p, pipeline=E.PIPELINE_SPLIT, particles_per_subfilter=m, num_subfilters=n // m,
+                            stream_offset=stream_offset, **cfg)
+
+
+def same_estimate(x, y):
+    return (np.array_equal(x["mean"], y["mean"]) and x["log_norm"] == y["log_norm"] and
+            np.array_equal(x["best"], y["best"]) and x["best_key"] == y["best_key"] and
+            x["best_subfilter"] == y["best_subfilter"] and x["step"] == y["step"])
+
+
+CASES = [
+    # m, ppt, exchange, t, period, resampler, counts
+    (256, 2, 1, 2, 1, 1, [256, 512, 1024, 256, 768, 2304]),
+    (128, 4, 1, 3, 2, 0, [128, 640, 384, 1024]),
+    (256, 4, 2, 2, 1, 2, [1024, 2048, 512, 4096]),   # torus: N = 4, 8, 2, 16
+    (256, 2, 2, 1, 4, 1, [1536, 256, 4096]),          # N = 6 (2x3), 1, 16
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,ppt,exch,t,period,res,counts", CASES)
+def test_batch_equals_single_filters(gpu, m, ppt, exch, t, period, res, counts):
+    E = gpu
+    steps = 7
+    params, inputs, _ = batch_setup(E, counts, steps)
+    cfg = dict(num_transfer=t, exchange=exch, resampler=res, exchange_period=period, particles_per_thread=ppt)
+    B = E.FilterBatch(UNI, params, counts, particles_per_subfilter=m, **cfg)
+    info = B.info()
+    assert info["num_filters"] == len(counts) and info["total_particles"] == sum(counts)
+    best = [B.step(inputs[:, k]) for k in range(steps)]
+    for f, n in enumerate(counts):
+        fi = B.filter_info(f)
+        assert fi["num_subfilters"] == n // m
+        s = single(E, params[f], cfg, fi["stream_offset"], n, m)
+        for k in range(steps):
+            e = s.step(inputs[f, k])
+            assert same_estimate(best[k][f], e), (f, k)
+        assert np.array_equal(B.particles(f), s.particles()), f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("period", [1, 2])
+def test_batch_graph_equals_host_steps(gpu, period):
+    """pf_batch_submit (graph of many steps, device counter) == pf_batch_step."""
+    import torch
+    E = gpu
+    counts = [256, 1280, 512, 3072, 256]
+    steps = 9
+    params, inputs, _ = batch_setup(E, counts, steps)
+    cfg = dict(particles_per_subfilter=256, num_transfer=2, exchange=1, exchange_period=period)
+    A = E.FilterBatch(UNI, params, counts, **cfg)
+    ea = [A.step(inputs[:, k]) for k in range(steps)]
+    B = E.FilterBatch(UNI, params, counts, **cfg)
+    cap = steps
+    d_in = torch.from_numpy(np.ascontiguousarray(inputs).view(np.uint8).reshape(-1).copy()).cuda()
+    d_est = torch.zeros(len(counts) * cap * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    # two submissions: 5 steps (one 5-step graph) then 4 more would restart the
+    # counter, so run all 9 at once and also check the poll/synchronize calls
+    B.submit(d_in.data_ptr(), d_est.data_ptr(), cap, steps)
+    B.synchronize()
+    assert B.poll()
+    est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE).reshape(len(counts), cap)
+    for f in range(len(counts)):
+        assert np.array_equal(A.particles(f), B.particles(f)), f
+        for k in range(steps):
+            x, y = est[f, k], ea[k][f]
+            assert np.array_equal(x["mean"], y["mean"]) and x["best_key"] == y["best_key"], (f, k)
+            assert x["step"] == k + 1
+
+
+@pytest.mark.gpu
+def test_batch_submit_split_into_graphs(gpu):
+    """A run longer than one captured graph (300 steps: a 256-step graph plus
+    single-step replays) matches host stepping at the end."""
+    import torch
+    E = gpu
+    counts = [256, 512]
+    steps = 300
+    params, inputs, _ = batch_setup(E, counts, steps)
+    cfg = dict(particles_per_subfilter=128, num_transfer=1, exchange=1, exchange_period=4)
+    A = E.FilterBatch(UNI, params, counts, **cfg)
+    for k in range(steps):
+        ea = A.step(inputs[:, k])
+    B = E.FilterBatch(UNI, params, counts, **cfg)
+    d_in = torch.from_numpy(np.ascontiguousarray(inputs).view(np.uint8).reshape(-1).copy()).cuda()
+    d_est = torch.zeros(len(counts) * steps * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    B.submit(d_in.data_ptr(), d_est.data_ptr(), steps, steps)
+    B.synchronize()
+    est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE).reshape(len(counts), steps)
+    for f in range(len(counts)):
+        assert np.array_equal(A.particles(f), B.particles(f))
+        assert np.array_equal(est[f, -1]["mean"], ea[f]["mean"])
+
+
+@pytest.mark.gpu
+def test_batch_tracks(gpu):
+    """Every filter of a mixed-size batch tracks its own seeded trajectory."""
+    E = gpu
+    counts = [256, 512, 2048, 8192]
+    steps = 60
+    params, inputs, truth = batch_setup(E, counts, steps, seed0=40)
+    B = E.FilterBatch(UNI, params, counts, particles_per_subfilter=256, num_transfer=2, exchange=1)
+    est = np.stack([B.step(inputs[:, k])["mean"][:, :2] for k in range(steps)], 1)  # [F, steps, 2]
+    err = np.sqrt(((est[:, 10:] - truth[:, 10:, :2]) ** 2).sum(-1).mean(-1))
+    assert np.all(err < 0.5), err
+
+
+def test_batch_rejects_bad_shapes(E):
+    import esthera_b200 as EB
+    p = [EB.UnicycleParams() for _ in range(2)]
+    for x in p:
+        x.num_landmarks = 4
+        x.sigma_range = 0.2
+        x.sigma_bearing = 0.05
+    with pytest.raises(EB.PFError) as ei:
+        EB.FilterBatch(UNI, p, [256, 300], particles_per_subfilter=256)
+    assert ei.value.status == EB.PF_ERR_INVALID
+    with pytest.raises(EB.PFError) as ei:
+        EB.FilterBatch(UNI, p, [256, 512], particles_per_subfilter=256, exchange=3)
+    assert ei.value.status == EB.PF_ERR_UNSUPPORTED
+    with pytest.raises(EB.PFError) as ei:
+        EB.FilterBatch(UNI, p, [256, 7 * 256], particles_per_subfilter=256, exchange=2)
+    assert ei.value.status == EB.PF_ERR_INVALID
