@@ -150,6 +150,116 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def run_batched(E, torch, args, local):
+    """Batched uneven filters: 4096 unicycle filters, counts log-uniform over
+    [256, 65536] rounded to 256, 200 steps, one graph-captured launch per run;
+    m / particles per thread / exchange period picked by pf_batch_autotune on a
+    256-filter slice; compared with looping the plain single-filter path
+    (pf_step per filter and step) over a sample of the same filters."""
+    from esthera_b200 import workloads as W
+    steps = args.batch_steps
+    counts, params, inputs, truth = W.batched_unicycle(args.batch_filters, steps)
+    F = len(counts)
+    P = int(counts.sum())
+    base = dict(num_transfer=2, exchange=E.EXCHANGE_RING, resampler=E.RESAMPLE_SYSTEMATIC, seed=SEED, device=local)
+    # autotune on an evenly spaced slice of the filters, 16 steps
+    sl = np.arange(0, F, max(1, F // 256))[:256]
+    t0 = time.time()
+    best, table = E.batch_autotune(E.MODEL_UNICYCLE, [params[i] for i in sl], counts[sl], inputs[sl, :16],
+                                   truth[sl, :16], m_list=(128, 256, 512, 1024), ppt_list=(1, 2, 4, 8),
+                                   period_list=(1, 2, 4), burn_in=4, rmse_tol=0.02, **base)
+    tune_s = time.time() - t0
+    cfg = dict(base, particles_per_subfilter=best.particles_per_subfilter,
+               particles_per_thread=best.particles_per_thread, exchange_period=best.exchange_period)
+    B = E.FilterBatch(E.MODEL_UNICYCLE, params, counts, **cfg)
+    info = B.info()
+    d_in = torch.from_numpy(np.ascontiguousarray(inputs).view(np.uint8).reshape(-1).copy()).cuda()
+    d_est = torch.zeros(F * steps * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(B.stream(), device=torch.device("cuda", local))
+    init = np.stack([np.array(p.init_state[:3], np.float32) for p in params])
+    # warm-up run (captures the graph), then the timed run from the initial states
+    B.submit(d_in.data_ptr(), d_est.data_ptr(), steps, steps)
+    B.synchronize()
+    est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE).reshape(F, steps)  # from fresh streams
+    B.set_initial_states(init)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    B.submit(d_in.data_ptr(), d_est.data_ptr(), steps, steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    run_ms = ev0.elapsed_time(ev1)
+    err = est["mean"][:, :, :2] - truth[:, :, :2]
+    rmse_f = np.sqrt(np.mean(np.sum(err[:, 20:] ** 2, axis=-1), axis=1))
+    value = P * steps / (run_ms * 1e-3)
+    # end to end through pf_batch_step: host inputs in, host estimates out, per step
+    B.set_initial_states(init)
+    lat = []
+    e2e_steps = min(steps, args.batch_e2e_steps)
+    for k in range(e2e_steps):
+        ev0.record(stream)
+        B.step(inputs[:, k])
+        ev1.record(stream)
+        ev1.synchronize()
+        lat.append(ev0.elapsed_time(ev1))
+    B.close()
+    # plain path: one filter at a time through pf_step (same m, ppt, period and
+    # streams, so the results are identical to the batched ones)
+    sample = np.arange(0, F, max(1, F // args.plain_sample))[:args.plain_sample]
+    plain_s, plain_ps, same = 0.0, 0, True
+    warm = E.ParticleFilter(E.MODEL_UNICYCLE, params[0], particles_per_subfilter=cfg["particles_per_subfilter"],
+                            num_subfilters=1, pipeline=E.PIPELINE_SPLIT,
+                            **{k: v for k, v in cfg.items() if k != "particles_per_subfilter"})
+    warm.step(inputs[0, 0])  # loads the kernels once; every sampled filter below starts fresh
+    warm.close()
+    for i in sample:
+        n = int(counts[i])
+        f = E.ParticleFilter(E.MODEL_UNICYCLE, params[i], particles_per_subfilter=cfg["particles_per_subfilter"],
+                             num_subfilters=n // cfg["particles_per_subfilter"], pipeline=E.PIPELINE_SPLIT,
+                             stream_offset=int(np.sum(counts[:i] // cfg["particles_per_subfilter"])),
+                             **{k: v for k, v in cfg.items() if k != "particles_per_subfilter"})
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(steps):
+            e = f.step(inputs[i, k])
+        plain_s += time.perf_counter() - t0
+        plain_ps += n * steps
+        same = same and bool(np.array_equal(e["mean"], est[i, steps - 1]["mean"]))
+        f.close()
+    plain = plain_ps / plain_s
+    lat = np.array(lat)
+    return {
+        "metric": "particle-steps/s (batched uneven filters)", "value": value, "unit": "particle-steps/s",
+        "steps": steps, "ms_per_step": run_ms / steps, "higher_is_better": True,
+        "config": {"workload": "%d unicycle filters, particle counts log-uniform [256, 65536] rounded to 256 "
+                               "(total %d), landmarks from seed 4+i, ring exchange t=2, systematic resampling, "
+                               "%d steps in one graph launch" % (F, P, steps),
+                   "filters": F, "particles": P, "subfilters": info["total_subfilters"],
+                   "particles_per_subfilter": cfg["particles_per_subfilter"],
+                   "particles_per_thread": cfg["particles_per_thread"], "exchange_period": cfg["exchange_period"],
+                   "l2": "working set %.1f GB > L2" % (info["device_bytes"] / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": ALG_BYTES * P * steps / (run_ms * 1e-3) / 1e9, "unit": "GB/s"},
+        "e2e": {"value": P * e2e_steps / (lat.sum() * 1e-3), "unit": "particle-steps/s",
+                "h2d_bytes_per_step": F * 128, "d2h_bytes_per_step": F * int(E.ESTIMATE_DTYPE.itemsize)},
+        "latency_ms": {"what": "one step of all filters through pf_batch_step (host in/out)",
+                       "p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "p999": float(np.percentile(lat, 99.9))},
+        "plain_loop": {"value": plain, "unit": "particle-steps/s",
+                       "sample": "%d filters x %d steps through pf_step, same configuration" % (len(sample), steps),
+                       "identical_results": same, "speedup": value / plain},
+        "rmse_xy": {"mean": float(rmse_f.mean()), "p99": float(np.percentile(rmse_f, 99))},
+        "autotune": {"seconds": tune_s, "slice": "%d filters x 16 steps" % len(sl),
+                     "candidates": [{"m": r["particles_per_subfilter"], "ppt": r["particles_per_thread"],
+                                     "period": r["exchange_period"], "ms_per_step": r["ms_per_step"],
+                                     "rmse": r["rmse"], "accepted": r["accepted"]}
+                                    for r in table if r["status"] == 0],
+                     "not_runnable": len([r for r in table if r["status"] != 0]),
+                     "not_runnable_why": "m not dividing every count (512, 1024) or particles per thread "
+                                         "not built for m"},
+        "gpu_launches": 3 * steps,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +271,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--batch-filters", type=int, default=4096)
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--batch-e2e-steps", type=int, default=50)
+    ap.add_argument("--plain-sample", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -180,6 +295,15 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     import esthera_b200 as E
+    if args.workload == "batched":
+        if rank == 0 or world == 1:
+            line = run_batched(E, torch, args, local)
+            line.update({"n_gpus": 1, "warmup": 1, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+                         "data": "synthetic (seeded traces, seeds 4+i)"})
+            peak, kind = peaks()
+            line["roofline"].update({"peak": peak, "frac": line["roofline"]["achieved"] / peak, "peak_kind": kind})
+            print(json.dumps(line), flush=True)
+        return 0
     resampler = CONFIGS[args.resampler]
     p = E.unicycle_params(SEED)
     total_steps = args.warmup + args.steps

@@ -138,6 +138,10 @@ def _declare(L):
         "pf_batch_stream": (P, [P]),
         "pf_batch_info": (C.c_int, [P, ip, C.POINTER(C.c_int64), ip, ip, C.POINTER(C.c_int64)]),
         "pf_batch_filter_info": (C.c_int, [P, C.c_int32, ip, ip, C.POINTER(C.c_int64)]),
+        "pf_batch_get_sorted": (C.c_int, [P, C.c_int32, fp, fp]),
+        "pf_batch_autotune": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, P, fp, C.c_int32,
+                                        C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32, C.c_float,
+                                        C.POINTER(TuneEntry), C.c_int32, ip, C.POINTER(PFConfig)]),
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
         "pfk_boxmuller": (C.c_int, [fp, C.c_int64]),
         "pfk_bitonic_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32]),
@@ -427,6 +431,13 @@ class FilterBatch:
         check(lib().pf_batch_step(self._h, a.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def sorted(self, f):
+        n = int(self.counts[f])
+        s = np.zeros((self.num_state, n), np.float32)
+        k = np.zeros(n, np.float32)
+        check(lib().pf_batch_get_sorted(self._h, f, _fptr(s), _fptr(k)))
+        return s, k
+
     def submit(self, d_inputs_ptr, d_estimates_ptr, capacity, steps):
         check(lib().pf_batch_submit(self._h, C.c_void_p(d_inputs_ptr), C.c_void_p(d_estimates_ptr), capacity, steps))
 
@@ -440,6 +451,37 @@ class FilterBatch:
 
     def stream(self):
         return lib().pf_batch_stream(self._h)
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("particles_per_subfilter", C.c_int32), ("particles_per_thread", C.c_int32),
+                ("exchange_period", C.c_int32), ("status", C.c_int32), ("ms_per_step", C.c_float),
+                ("accepted", C.c_int32), ("particle_steps_per_s", C.c_double), ("rmse", C.c_double)]
+
+
+def batch_autotune(model, params, counts, inputs, truth=None, m_list=(128, 256, 512, 1024), ppt_list=(1, 2, 4),
+                   period_list=(1, 2, 4), burn_in=0, rmse_tol=0.01, **cfg):
+    """pf_batch_autotune over host inputs [F][steps] (and truth [F][steps][S]):
+    returns (best pf_config, [candidate dicts])."""
+    base = default_config(**cfg)
+    counts = np.ascontiguousarray(counts, np.int32)
+    F = len(counts)
+    ptype = type(params[0])
+    arr = (ptype * F)(*params)
+    inp = np.ascontiguousarray(inputs, STEP_INPUT_DTYPE)
+    steps = inp.shape[1]
+    tr = None if truth is None else _f32(truth)
+    ml, pl, ql = (np.ascontiguousarray(x, np.int32) for x in (m_list, ppt_list, period_list))
+    cap = len(ml) * len(pl) * len(ql)
+    table = (TuneEntry * cap)()
+    n = C.c_int32()
+    best = PFConfig()
+    check(lib().pf_batch_autotune(C.byref(base), model, F, _iptr(counts), C.cast(arr, C.c_void_p), C.sizeof(ptype),
+                                  inp.ctypes.data_as(C.c_void_p), None if tr is None else _fptr(tr), steps, burn_in,
+                                  _iptr(ml), len(ml), _iptr(pl), len(pl), _iptr(ql), len(ql), rmse_tol, table, cap,
+                                  C.byref(n), C.byref(best)))
+    rows = [{k: getattr(table[i], k) for k, _ in TuneEntry._fields_} for i in range(n.value)]
+    return best, rows
 
 
 def particle_filter(num_particles, num_blocks, num_transfer, resampling_freq, input_file):

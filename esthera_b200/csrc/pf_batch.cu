@@ -11,6 +11,8 @@
 // Sub-filter b of filter f draws from stream stream_offset + first(f) + b,
 // first(f) = the number of sub-filters of filters 0..f-1, so filter f alone
 // (pf_create with that stream offset) reproduces its batched results exactly.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -500,5 +502,169 @@ extern "C" pf_status pf_batch_filter_info(pf_batch* B, int32_t filter, int32_t* 
     if (num_subfilters) *num_subfilters = B->nsub[filter];
     if (stream_offset) *stream_offset = B->cfg.stream_offset + B->sub_off[filter];
     if (particle_offset) *particle_offset = B->part_off[filter];
+    return PF_OK;
+}
+
+extern "C" pf_status pf_batch_get_sorted(pf_batch* B, int32_t filter, float* soa, float* keys)
+{
+    if (!B || !soa || !keys) return fail(PF_ERR_INVALID, "null argument");
+    if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
+    CU(cudaSetDevice(B->cfg.device));
+    CU(cudaStreamSynchronize(B->stream));
+    const int64_t T = (int64_t)B->M * B->nsub[filter];
+    const int64_t p0 = B->part_off[filter];
+    for (int v = 0; v < B->S; ++v)
+        CU(cudaMemcpy(soa + v * T, B->tmp + (int64_t)B->S * p0 + v * T, (size_t)T * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(keys, B->tkey + p0, (size_t)T * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: times every (m, particles per thread, exchange period) candidate
+// on the caller's inputs and picks the fastest whose tracking error stays
+// within a tolerance of the every-step-exchange candidates.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DevMem {
+    void* p = nullptr;
+    ~DevMem()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+// Root mean square over filters, steps >= burn_in and state variables of
+// (estimate mean - truth), angular variables wrapped to (-pi, pi].
+double tracking_rmse(const std::vector<pf_estimate>& est, const float* truth, int F, int steps, int burn_in, int S,
+                     uint32_t amask)
+{
+    double acc = 0.0;
+    int64_t n = 0;
+    for (int f = 0; f < F; ++f)
+        for (int k = burn_in; k < steps; ++k) {
+            const pf_estimate& e = est[(size_t)f * steps + k];
+            const float* x = truth + ((size_t)f * steps + k) * S;
+            for (int v = 0; v < S; ++v) {
+                double d = e.mean[v] - (double)x[v];
+                if ((amask >> v) & 1u) d = std::remainder(d, 2.0 * M_PI);
+                acc += d * d;
+                ++n;
+            }
+        }
+    return n ? std::sqrt(acc / (double)n) : NAN;
+}
+
+}  // namespace
+
+extern "C" pf_status pf_batch_autotune(const pf_config* base, pf_model_id model, int32_t num_filters,
+                                       const int32_t* num_particles, const void* params, size_t params_size,
+                                       const pf_step_input* inputs, const float* truth, int32_t steps,
+                                       int32_t burn_in, const int32_t* m_list, int32_t n_m, const int32_t* ppt_list,
+                                       int32_t n_ppt, const int32_t* period_list, int32_t n_period, float rmse_tol,
+                                       pf_tune_entry* table, int32_t table_cap, int32_t* n_table, pf_config* best)
+{
+    if (!base || !num_particles || !params || !inputs || !m_list || !ppt_list || !period_list || !table ||
+        !n_table || !best)
+        return fail(PF_ERR_INVALID, "null argument");
+    if (num_filters < 1 || steps < 1 || burn_in < 0 || burn_in >= steps || n_m < 1 || n_ppt < 1 || n_period < 1)
+        return fail(PF_ERR_INVALID, "bad tuning shape");
+    if ((int64_t)n_m * n_ppt * n_period > table_cap) return fail(PF_ERR_INVALID, "table too small for the candidates");
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    pf_status s = require_gpu(base->device);
+    if (s != PF_OK) return s;
+    const size_t nio = (size_t)num_filters * steps;
+    DevMem din, dest;
+    CU(cudaMalloc(&din.p, nio * sizeof(pf_step_input)));
+    CU(cudaMalloc(&dest.p, nio * sizeof(pf_estimate)));
+    CU(cudaMemcpy(din.p, inputs, nio * sizeof(pf_step_input), cudaMemcpyHostToDevice));
+    EventPair ev;
+    CU(cudaEventCreate(&ev.a));
+    CU(cudaEventCreate(&ev.b));
+    std::vector<pf_estimate> est(nio);
+    std::vector<float> init((size_t)num_filters * mi.S);
+    for (int f = 0; f < num_filters; ++f) {
+        ModelParams mp;
+        memset(&mp, 0, sizeof(mp));
+        memcpy(&mp, static_cast<const char*>(params) + (size_t)f * params_size,
+               std::min(params_size, sizeof(ModelParams)));
+        memcpy(init.data() + (size_t)f * mi.S, init_state_of(model, mp), sizeof(float) * mi.S);
+    }
+    int n = 0;
+    for (int im = 0; im < n_m; ++im)
+        for (int ip = 0; ip < n_ppt; ++ip)
+            for (int iq = 0; iq < n_period; ++iq) {
+                pf_tune_entry& t = table[n++];
+                memset(&t, 0, sizeof(t));
+                t.particles_per_subfilter = m_list[im];
+                t.particles_per_thread = ppt_list[ip];
+                t.exchange_period = period_list[iq];
+                t.rmse = NAN;
+                pf_config c = *base;
+                c.particles_per_subfilter = m_list[im];
+                c.particles_per_thread = ppt_list[ip];
+                c.exchange_period = period_list[iq];
+                pf_batch* B = nullptr;
+                t.status = pf_batch_create(&c, model, num_filters, num_particles, params, params_size, &B);
+                if (t.status != PF_OK) continue;
+                // first run captures the graph; the timed run replays it from the initial states
+                pf_status r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
+                if (r == PF_OK) r = pf_batch_synchronize(B);
+                if (r == PF_OK) r = pf_batch_set_initial_states(B, init.data());
+                cudaError_t e = cudaSuccess;
+                if (r == PF_OK) e = cudaEventRecord(ev.a, B->stream);
+                if (r == PF_OK && e == cudaSuccess)
+                    r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
+                if (r == PF_OK && e == cudaSuccess) e = cudaEventRecord(ev.b, B->stream);
+                if (r == PF_OK && e == cudaSuccess) e = cudaEventSynchronize(ev.b);
+                float ms = 0.0f;
+                if (r == PF_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev.a, ev.b);
+                if (r == PF_OK && e == cudaSuccess)
+                    e = cudaMemcpy(est.data(), dest.p, nio * sizeof(pf_estimate), cudaMemcpyDeviceToHost);
+                pf_batch_destroy(B);
+                if (r != PF_OK || e != cudaSuccess) {
+                    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+                    t.status = r;
+                    continue;
+                }
+                t.ms_per_step = ms / (float)steps;
+                int64_t P = 0;
+                for (int f = 0; f < num_filters; ++f) P += num_particles[f];
+                t.particle_steps_per_s = (double)P * steps / (ms * 1e-3);
+                if (truth) t.rmse = tracking_rmse(est, truth, num_filters, steps, burn_in, mi.S, angle_mask_of(model));
+            }
+    *n_table = n;
+    // reference error: mean over the runnable every-step-exchange candidates
+    double ref = 0.0;
+    int nref = 0;
+    for (int i = 0; i < n; ++i)
+        if (table[i].status == PF_OK && table[i].exchange_period <= 1 && std::isfinite(table[i].rmse)) {
+            ref += table[i].rmse;
+            ++nref;
+        }
+    ref = nref ? ref / nref : NAN;
+    int pick = -1;
+    for (int i = 0; i < n; ++i) {
+        pf_tune_entry& t = table[i];
+        if (t.status != PF_OK) continue;
+        t.accepted = truth ? (nref > 0 && std::isfinite(t.rmse) && t.rmse <= ref * (1.0 + rmse_tol))
+                           : (t.exchange_period <= 1);
+        if (t.accepted && (pick < 0 || t.particle_steps_per_s > table[pick].particle_steps_per_s)) pick = i;
+    }
+    if (pick < 0) return fail(PF_ERR_UNSUPPORTED, "autotune: no candidate could run (last: %s)", pf_last_error());
+    *best = *base;
+    best->particles_per_subfilter = table[pick].particles_per_subfilter;
+    best->particles_per_thread = table[pick].particles_per_thread;
+    best->exchange_period = table[pick].exchange_period;
     return PF_OK;
 }

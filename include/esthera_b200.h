@@ -242,6 +242,36 @@ pf_status pf_batch_info(pf_batch* b, int32_t* num_filters, int64_t* total_partic
                         int32_t* particles_per_thread, int64_t* device_bytes);
 pf_status pf_batch_filter_info(pf_batch* b, int32_t filter, int32_t* num_subfilters, int32_t* stream_offset,
                                int64_t* particle_offset);
+/* Filter f's sorted (pre-exchange) particles and keys of the last step (host, SoA). */
+pf_status pf_batch_get_sorted(pf_batch* b, int32_t filter, float* soa, float* keys);
+
+/* Autotuner for batched filters (project-written; no reference counterpart).
+ * Every candidate (m from m_list x particles per thread from ppt_list x exchange
+ * period from period_list) runs `steps` steps of the whole batch on `inputs`
+ * (host, [F][steps]) twice -- the first run captures the CUDA graph, the second
+ * is timed with CUDA events -- and, when `truth` ([F][steps][S], host) is given,
+ * its tracking RMSE over steps >= burn_in is computed (angles wrapped).  A
+ * candidate is accepted when its RMSE is within (1 + rmse_tol) of the mean
+ * RMSE of the period-1 candidates (without truth: period-1 candidates only);
+ * *best = base with the fastest accepted candidate's m, ppt and period.
+ * Candidates that cannot run (m not dividing every count, ppt not built for m)
+ * keep their pf_status in the table. */
+typedef struct {
+    int32_t particles_per_subfilter;
+    int32_t particles_per_thread;
+    int32_t exchange_period;
+    int32_t status;
+    float ms_per_step;
+    int32_t accepted;
+    double particle_steps_per_s;
+    double rmse;
+} pf_tune_entry;
+pf_status pf_batch_autotune(const pf_config* base, pf_model_id model, int32_t num_filters,
+                            const int32_t* num_particles, const void* params, size_t params_size,
+                            const pf_step_input* inputs, const float* truth, int32_t steps, int32_t burn_in,
+                            const int32_t* m_list, int32_t n_m, const int32_t* ppt_list, int32_t n_ppt,
+                            const int32_t* period_list, int32_t n_period, float rmse_tol,
+                            pf_tune_entry* table, int32_t table_cap, int32_t* n_table, pf_config* best);
 
 /* ---- kernel-level entry points (device work on host arrays; used by parity tests) ---- */
 /* MTGP32 in the reference block layout: streams g = 0..G-1 with parameter set g,

@@ -140,3 +140,43 @@ def test_batch_rejects_bad_shapes(E):
     with pytest.raises(EB.PFError) as ei:
         EB.FilterBatch(UNI, p, [256, 7 * 256], particles_per_subfilter=256, exchange=2)
     assert ei.value.status == EB.PF_ERR_INVALID
+
+
+@pytest.mark.gpu
+def test_batch_autotune(gpu):
+    """The autotuner runs every buildable candidate, reports the others with
+    their status, and picks the fastest accepted one."""
+    E = gpu
+    counts = [256, 768, 1536, 512]
+    steps = 12
+    params, inputs, truth = batch_setup(E, counts, steps)
+    best, rows = E.batch_autotune(UNI, params, counts, inputs, truth, m_list=(128, 256, 512), ppt_list=(2, 4),
+                                  period_list=(1, 2), burn_in=2, rmse_tol=0.5, num_transfer=1, exchange=1)
+    assert len(rows) == 3 * 2 * 2
+    for r in rows:
+        if r["particles_per_subfilter"] == 512:      # 768 is not a multiple of 512
+            assert r["status"] == E.PF_ERR_INVALID and not r["accepted"]
+        else:
+            assert r["status"] == E.PF_OK and r["ms_per_step"] > 0 and np.isfinite(r["rmse"])
+    ok = [r for r in rows if r["accepted"]]
+    pick = max(ok, key=lambda r: r["particle_steps_per_s"])
+    assert (best.particles_per_subfilter, best.particles_per_thread, best.exchange_period) == (
+        pick["particles_per_subfilter"], pick["particles_per_thread"], pick["exchange_period"])
+
+
+@pytest.mark.gpu
+def test_batch_normalisation_vs_fp64(gpu):
+    """Each filter's log normalisation (FP64 accumulation of FP32 weights)
+    against an FP64 log-sum-exp of the same sorted keys on the host."""
+    E = gpu
+    counts = [256, 4096, 1280, 65536]
+    params, inputs, _ = batch_setup(E, counts, 3)
+    B = E.FilterBatch(UNI, params, counts, particles_per_subfilter=256, num_transfer=2, exchange=1)
+    for k in range(3):
+        est = B.step(inputs[:, k])
+    for f in range(len(counts)):
+        _, keys = B.sorted(f)
+        kk = keys.astype(np.float64)
+        mx = kk.max()
+        ln = mx + np.log(np.sum(np.exp(kk - mx)))
+        assert abs(est[f]["log_norm"] - ln) <= 1e-6 * max(1.0, abs(ln)), (f, est[f]["log_norm"], ln)
