@@ -142,6 +142,18 @@ def _declare(L):
         "pf_batch_autotune": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, P, fp, C.c_int32,
                                         C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32, C.c_float,
                                         C.POINTER(TuneEntry), C.c_int32, ip, C.POINTER(PFConfig)]),
+        "pf_server_create": (C.c_int, [C.POINTER(PFConfig), C.c_int64, C.c_int32, C.POINTER(P)]),
+        "pf_server_destroy": (C.c_int, [P]),
+        "pf_server_footprint": (C.c_int64, [P, C.c_int, C.c_int32]),
+        "pf_server_open": (C.c_int, [P, C.c_int, P, C.c_size_t, C.c_int32, C.c_uint32, ip]),
+        "pf_server_close": (C.c_int, [P, C.c_int32]),
+        "pf_server_update": (C.c_int, [P, C.c_int32, P, C.c_uint64]),
+        "pf_server_launch": (C.c_int, [P, ip]),
+        "pf_server_poll": (C.c_int, [P, C.c_int32, P, C.c_int32, ip]),
+        "pf_server_stats_get": (C.c_int, [P, C.POINTER(ServerStats)]),
+        "pf_server_get_particles": (C.c_int, [P, C.c_int32, fp, fp, fp]),
+        "pf_load_default": (C.c_int, [C.POINTER(LoadConfig)]),
+        "pf_serve_load": (C.c_int, [C.POINTER(PFConfig), C.POINTER(LoadConfig), C.POINTER(LoadReport)]),
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
         "pfk_boxmuller": (C.c_int, [fp, C.c_int64]),
         "pfk_bitonic_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32]),
@@ -451,6 +463,121 @@ class FilterBatch:
 
     def stream(self):
         return lib().pf_batch_stream(self._h)
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("open_filters", C.c_int32), ("in_flight", C.c_int32), ("resident_particles", C.c_int64),
+                ("queued_updates", C.c_int64), ("bytes_in_use", C.c_int64), ("budget", C.c_int64),
+                ("launches", C.c_int64), ("updates", C.c_int64), ("particle_steps", C.c_int64)]
+
+
+SERVER_RESULT_DTYPE = np.dtype([("filter", np.int32), ("step", np.int32), ("tag", np.uint64),
+                                ("particles", np.int64), ("estimate", ESTIMATE_DTYPE)])
+
+
+class Server:
+    """Resident filters with continuously batched updates (pf_server_*)."""
+
+    def __init__(self, hbm_budget, max_filters, config=None, **cfg):
+        self.config = config if config is not None else default_config(**cfg)
+        self.max_filters = max_filters
+        h = C.c_void_p()
+        check(lib().pf_server_create(C.byref(self.config), int(hbm_budget), max_filters, C.byref(h)))
+        self._h = h
+        self._out = np.zeros(max_filters, SERVER_RESULT_DTYPE)
+        self.models = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def footprint(self, model, num_particles):
+        return lib().pf_server_footprint(self._h, model, num_particles)
+
+    def open(self, model, params, num_particles, seed):
+        i = C.c_int32()
+        check(lib().pf_server_open(self._h, model, C.byref(params), C.sizeof(params), num_particles, seed,
+                                   C.byref(i)))
+        self.models[i.value] = model
+        return i.value
+
+    def close_filter(self, fid):
+        check(lib().pf_server_close(self._h, fid))
+        self.models.pop(fid, None)
+
+    def update(self, fid, inp, tag=0):
+        a = np.ascontiguousarray(inp, STEP_INPUT_DTYPE)
+        check(lib().pf_server_update(self._h, fid, a.ctypes.data_as(C.c_void_p), tag))
+
+    def launch(self):
+        n = C.c_int32()
+        check(lib().pf_server_launch(self._h, C.byref(n)))
+        return n.value
+
+    def poll(self, wait=True):
+        n = C.c_int32()
+        check(lib().pf_server_poll(self._h, 1 if wait else 0, self._out.ctypes.data_as(C.c_void_p),
+                                   self.max_filters, C.byref(n)))
+        return self._out[:n.value].copy()
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().pf_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def particles(self, fid, n):
+        S = model_info(self.models[fid])[0]
+        a = np.zeros((S, n), np.float32)
+        srt = np.zeros((S, n), np.float32)
+        k = np.zeros(n, np.float32)
+        check(lib().pf_server_get_particles(self._h, fid, _fptr(a), _fptr(srt), _fptr(k)))
+        return a, srt, k
+
+
+class LoadConfig(C.Structure):
+    _fields_ = [("rate", C.c_double), ("duration_s", C.c_double), ("frac_unicycle", C.c_double),
+                ("min_particles", C.c_int32), ("max_particles", C.c_int32), ("min_updates", C.c_int32),
+                ("max_updates", C.c_int32), ("min_gap_ms", C.c_double), ("max_gap_ms", C.c_double),
+                ("seed", C.c_uint32), ("max_filters", C.c_int32), ("hbm_budget", C.c_int64),
+                ("norm_check_every", C.c_int32), ("pad0", C.c_int32), ("drain_limit_s", C.c_double)]
+
+
+class LoadReport(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("requests", "admitted", "admission_waits", "completed_requests", "updates",
+                                         "launches", "max_resident_particles", "max_bytes_in_use")] + \
+               [("max_open_filters", C.c_int32), ("incomplete", C.c_int32)] + \
+               [(k, C.c_double) for k in ("wall_s", "particle_steps", "particle_steps_per_s",
+                                          "demanded_particle_steps_per_s", "mean_batch", "lat_p50_ms", "lat_p99_ms",
+                                          "lat_p999_ms", "lat_max_ms")] + \
+               [("norm_checked", C.c_int64), ("norm_err_max", C.c_double), ("norm_err_mean", C.c_double)]
+
+
+def serve_load(filter_config=None, load=None, **load_kw):
+    """Run the served tracking load (pf_serve_load); returns the report as a dict."""
+    cfg = filter_config if filter_config is not None else default_config(
+        particles_per_subfilter=256, particles_per_thread=4, num_transfer=2, exchange=EXCHANGE_RING)
+    lc = LoadConfig()
+    check(lib().pf_load_default(C.byref(lc)))
+    for k, v in dict(load or {}, **load_kw).items():
+        if not hasattr(lc, k):
+            raise AttributeError("pf_load_config has no field %r" % k)
+        setattr(lc, k, v)
+    rep = LoadReport()
+    check(lib().pf_serve_load(C.byref(cfg), C.byref(lc), C.byref(rep)))
+    return {k: getattr(rep, k) for k, _ in LoadReport._fields_}
 
 
 class TuneEntry(C.Structure):

@@ -305,21 +305,12 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         std::vector<int2> map((size_t)NS);
         for (int f = 0; f < num_filters; ++f)
             for (int b = 0; b < B->nsub[f]; ++b) map[(size_t)B->sub_off[f] + b] = make_int2(f, b);
-        std::vector<uint32_t> st((size_t)kMtgpN * 4096);
-        for (int64_t g0 = 0; g0 < NS; g0 += 4096) {
-            const int n = (int)std::min<int64_t>(4096, NS - g0);
-            for (int i = 0; i < n; ++i) {
-                const int g = cfg->stream_offset + (int)(g0 + i);
-                mtgp_init_state_host(st.data() + (size_t)i * kMtgpN, g % kMtgpSets, cfg->seed + (uint32_t)g + 1u);
-            }
-            if (cudaMemcpy(B->mtgp + g0 * kMtgpN, st.data(), (size_t)n * kMtgpN * 4, cudaMemcpyHostToDevice) !=
-                    cudaSuccess ||
-                (g0 == 0 &&
-                 cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess)) {
-                cudaGetLastError();
-                release(B);
-                return fail(PF_ERR_CUDA, "initial upload failed");
-            }
+        if (cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            launch_mtgp_init(B->mtgp, (int)NS, cfg->stream_offset, cfg->seed, B->stream) != cudaSuccess ||
+            cudaStreamSynchronize(B->stream) != cudaSuccess) {
+            cudaGetLastError();
+            release(B);
+            return fail(PF_ERR_CUDA, "initial upload failed");
         }
     }
     if (cudaMemset(B->est_ctr, 0, 4 * (size_t)num_filters) != cudaSuccess || cudaMemset(B->ctr, 0, 4) != cudaSuccess) {

@@ -225,6 +225,40 @@ cudaError_t launch_mtgp_blocks(int G, uint32_t* states, uint32_t* out, int64_t s
     return cudaGetLastError();
 }
 
+// MTGP32 stream initialisation (mtgp32_init_state, mtgp32-fast.c:119-137), one
+// thread per stream: stream i gets parameter set (g0 + i) mod 200 and seed
+// seed + g0 + i + 1 -- the words the host-side initialisation writes.
+__global__ void k_mtgp_init(uint32_t* __restrict__ states, int n, int g0, uint32_t seed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int g = g0 + i;
+    const uint32_t* tbl = g_mtgp_params + (g % kMtgpSets) * 52 + 4;
+    const uint32_t hidden = tbl[4] ^ (tbl[8] << 16);
+    uint32_t t = hidden;
+    t += t >> 16;
+    t += t >> 8;
+    const uint32_t b = t & 0xffu;
+    const uint32_t fill = b | (b << 8) | (b << 16) | (b << 24);
+    uint32_t* st = states + (int64_t)i * kMtgpN;
+    uint32_t prev = seed + (uint32_t)g + 1u;
+    st[0] = prev;
+    // word 0 is the seed; word k >= 1 is (k == 1 ? hidden : fill) xor'ed with
+    // 1812433253 * (w ^ (w >> 30)) + k of its predecessor w
+    for (int k = 1; k < kMtgpN; ++k) {
+        const uint32_t w = (k == 1 ? hidden : fill) ^ (1812433253u * (prev ^ (prev >> 30)) + (uint32_t)k);
+        st[k] = w;
+        prev = w;
+    }
+}
+
+cudaError_t launch_mtgp_init(uint32_t* states, int n, int g0, uint32_t seed, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    k_mtgp_init<<<(n + 127) / 128, 128, 0, st>>>(states, n, g0, seed);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_boxmuller(float* data, int64_t n, cudaStream_t st)
 {
     const int64_t pairs = (n + 1) / 2;

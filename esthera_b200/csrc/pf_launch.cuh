@@ -71,6 +71,8 @@ cudaError_t launch_test_resample(int res, int M, int E, int nsub, const float* w
 cudaError_t launch_mtgp_blocks(int G, uint32_t* states, uint32_t* out, int64_t size, uint32_t mask, int float_out,
                                int set_base, cudaStream_t st);
 cudaError_t launch_boxmuller(float* data, int64_t n, cudaStream_t st);
+// Initial words of MTGP32 streams g0 .. g0+n-1 (parameter set g mod 200, seed + g + 1).
+cudaError_t launch_mtgp_init(uint32_t* states, int n, int g0, uint32_t seed, cudaStream_t st);
 cudaError_t launch_a2a_merge(int nfilters, const FilterDesc* d, cudaStream_t st);
 cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStream_t st);
 cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st);

@@ -273,6 +273,86 @@ pf_status pf_batch_autotune(const pf_config* base, pf_model_id model, int32_t nu
                             const int32_t* period_list, int32_t n_period, float rmse_tol,
                             pf_tune_entry* table, int32_t table_cap, int32_t* n_table, pf_config* best);
 
+/* ---- serving: many resident filters, updates batched as they arrive ----
+ * No counterpart in the reference (one filter per process there).  Filters
+ * of any compiled-in model share the server's pf_config template (m,
+ * particles per thread, ring/no exchange, resampler, resampling_freq,
+ * log_weights, mtgp_mask); each has its own particle count (a multiple of m),
+ * parameters and seed (sub-filter b: parameter set b mod 200, seed + b + 1, as
+ * a pf_filter with that seed).  Device memory per filter comes from a
+ * stream-ordered pool; pf_server_open fails with PF_ERR_ADMISSION when the
+ * filter's block (pf_server_footprint) does not fit the HBM budget or no slot
+ * is free.  pf_server_update queues an update; pf_server_launch runs the
+ * oldest queued update of every filter without one in flight as one batch
+ * (no-op while a batch is in flight); pf_server_poll returns the finished
+ * batch's results (wait = 0: without blocking).  A handle is used by one
+ * host thread at a time. */
+typedef struct pf_server pf_server;
+typedef struct {
+    int32_t filter;       /* id from pf_server_open */
+    int32_t step;         /* updates completed by this filter */
+    uint64_t tag;         /* the caller's tag of the update */
+    int64_t particles;
+    pf_estimate estimate;
+} pf_server_result;
+typedef struct {
+    int32_t open_filters;
+    int32_t in_flight;
+    int64_t resident_particles;
+    int64_t queued_updates;
+    int64_t bytes_in_use;
+    int64_t budget;
+    int64_t launches;
+    int64_t updates;
+    int64_t particle_steps;
+} pf_server_stats;
+pf_status pf_server_create(const pf_config* filter_cfg, int64_t hbm_budget, int32_t max_filters, pf_server** out);
+pf_status pf_server_destroy(pf_server* s);
+int64_t pf_server_footprint(const pf_server* s, pf_model_id model, int32_t num_particles);
+pf_status pf_server_open(pf_server* s, pf_model_id model, const void* params, size_t params_size,
+                         int32_t num_particles, uint32_t seed, int32_t* id);
+pf_status pf_server_close(pf_server* s, int32_t id);
+pf_status pf_server_update(pf_server* s, int32_t id, const pf_step_input* in, uint64_t tag);
+pf_status pf_server_launch(pf_server* s, int32_t* n_launched);
+pf_status pf_server_poll(pf_server* s, int32_t wait, pf_server_result* out, int32_t cap, int32_t* n);
+pf_status pf_server_stats_get(pf_server* s, pf_server_stats* st);
+/* Current particles, sorted copy and sorted keys of filter id (host; any may be NULL). */
+pf_status pf_server_get_particles(pf_server* s, int32_t id, float* soa, float* sorted_soa, float* keys);
+
+/* ---- the served tracking load (request loop over pf_server_*, host C) ----
+ * Poisson arrivals at `rate` per second for `duration_s`; each request is a
+ * unicycle (probability frac_unicycle) or DH-arm filter with a log-uniform
+ * particle count in [min_particles, max_particles] (rounded to m), a uniform
+ * number of updates in [min_updates, max_updates] spaced uniformly in
+ * [min_gap_ms, max_gap_ms].  Everything is generated from `seed`.  The loop
+ * runs in real time on the calling thread and fills the report; it stops
+ * drain_limit_s after the last arrival if work is left (report.incomplete). */
+typedef struct {
+    double rate;
+    double duration_s;
+    double frac_unicycle;
+    int32_t min_particles, max_particles;
+    int32_t min_updates, max_updates;
+    double min_gap_ms, max_gap_ms;
+    uint32_t seed;
+    int32_t max_filters;
+    int64_t hbm_budget;
+    int32_t norm_check_every;  /* every k-th request: FP64 check of its last normalisation (0: off) */
+    int32_t pad0;
+    double drain_limit_s;
+} pf_load_config;
+typedef struct {
+    int64_t requests, admitted, admission_waits, completed_requests, updates, launches;
+    int64_t max_resident_particles, max_bytes_in_use;
+    int32_t max_open_filters, incomplete;
+    double wall_s, particle_steps, particle_steps_per_s, demanded_particle_steps_per_s, mean_batch;
+    double lat_p50_ms, lat_p99_ms, lat_p999_ms, lat_max_ms;
+    int64_t norm_checked;
+    double norm_err_max, norm_err_mean;  /* |log_norm - FP64 log-sum-exp| / max(1, |.|) */
+} pf_load_report;
+pf_status pf_load_default(pf_load_config* c);
+pf_status pf_serve_load(const pf_config* filter_cfg, const pf_load_config* load, pf_load_report* report);
+
 /* ---- kernel-level entry points (device work on host arrays; used by parity tests) ---- */
 /* MTGP32 in the reference block layout: streams g = 0..G-1 with parameter set g,
  * seed + g + 1; out[g*per_stream + i].  kind 0: uint32, 1: float bits in [1,2).
