@@ -1,24 +1,31 @@
 #!/usr/bin/env python3
 """Particle-filter step throughput on B200 (particle-steps/s).
 
-Workload (N=1): the large unicycle filter -- 2^20 particles as 2048
-sub-filters of 512 on a 32 x 64 torus, top-2 exchange with each neighbour,
-systematic resampling every step, FP32 state and log-weights, FP64
-normalisation and cumulative sums, seed 2.  Inputs (controls and
-range/bearing measurements to 4 landmarks) are synthetic, generated from
-the seed.  A "step" is one full filter step over all 2^20 particles.
+Default workload (N=1, --workload plain): the large unicycle filter -- 2^20
+particles as 2048 sub-filters of 512 on a 32 x 64 torus, top-2 exchange with
+each neighbour, systematic (--resampler vose: Vose alias) resampling every
+step, FP32 state and log-weights, FP64 normalisation and cumulative sums,
+seed 2, 1000 steps.  Inputs (controls and range/bearing measurements to 4
+landmarks) are synthetic, generated from the seed.  A "step" is one full
+filter step over all 2^20 particles.
+--workload arm: the 6-joint DH arm, 2^18 particles = 1024 x 256 on a 32 x 32
+torus, t = 1, seed 3.  --workload batched / served: the batched uneven
+filters and the served tracking load (their own JSON lines).
 
 value:  device-timed (CUDA events on the filter's stream), inputs resident
         in HBM, one CUDA-graph replay per step, L2 flushed (256 MB write)
         before every timed step.  value = particles * steps / sum(step time).
 e2e:    the same through pf_step() with host inputs: H2D of the 128-byte
         step input and D2H of the estimate inside each timed step.
-roofline: 24 algorithmic bytes per particle-step (12 B state read + 12 B
-        state write) over the step's device time, against the measured HBM
-        copy bandwidth.
+roofline: the dominant kernel's algorithmic bytes (the sampling kernel reads
+        the state, 12 B per unicycle particle; the resampling kernel writes
+        it) over its CUDA-event time, against the measured HBM copy
+        bandwidth; `step` gives the whole step (24 B per particle-step).
+        traffic: the kernel's DRAM bytes per launch from the committed ncu
+        summary.
 
-Multi-GPU (torchrun): each rank runs its own 2^20-particle filter (weak
-scaling, no data-path collective); time = max over ranks.
+Multi-GPU (torchrun): each rank runs its own filter (weak scaling, replicas,
+no data-path collective); time = max over ranks.
 --impl reference: the CPU restatement of the reference step (the reference's
 OpenCL path cannot run here) on all host cores, on a bounded sample.
 """
@@ -37,10 +44,15 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-M, NSUB, T_EXCH = 512, 2048, 2
-PARTICLES = M * NSUB
-ALG_BYTES = 24  # per particle-step
-SEED = 2
+ALG_BYTES = 24  # unicycle, per particle-step
+# single-filter workloads: model, sub-filter size, sub-filters, torus transfer,
+# seed, algorithmic bytes per particle-step (state read + write)
+WORKLOADS = {
+    "plain": dict(model=0, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(),
+                  desc="unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2"),
+    "arm": dict(model=1, m=256, nsub=1024, t=1, seed=3, alg=96, angles=(0, 1, 2, 3, 4, 5),
+                desc="6-joint DH arm 2^18 particles = 1024 sub-filters x 256, torus 32x32, t=1"),
+}
 CONFIGS = {
     "systematic": 1,
     "vose": 2,
@@ -60,7 +72,7 @@ def clock_sampler(gpu_index):
            "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-           "--format=csv,noheader,nounits", "-lms", "200"]
+           "--format=csv,noheader,nounits", "-lms", "20"]
     try:
         return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
     except OSError:
@@ -104,18 +116,24 @@ def visible_gpu_index(local_rank):
     return str(local_rank)
 
 
-def cpu_baseline(steps, resampler, threads=0, budget_s=20.0):
+def model_params(E, W):
+    return E.unicycle_params(W["seed"]) if W["model"] == 0 else E.dharm_params(W["seed"])
+
+
+def cpu_baseline(steps, resampler, threads=0, budget_s=20.0, W=None):
     """The oracle's whole step (C, OpenMP over sub-filters) on a sample of the
-    workload: 256 sub-filters of 512 (2^17 particles) on a 16 x 16 torus."""
+    workload: 256 sub-filters (a 16 x 16 torus) of the workload's size."""
+    W = W or WORKLOADS["plain"]
     sys.path.insert(0, str(ROOT / "oracle"))
     import esthera_b200 as E
     import oracle as O
-    nsub = 256
-    p = E.unicycle_params(SEED)
-    inputs, _ = E.make_trace(E.MODEL_UNICYCLE, p, SEED, steps)
-    md = O.model_from_params(O.MODEL_UNICYCLE, p)
-    f = O.Filter(md, M, nsub, T_EXCH, O.EXCH_TORUS, resampler, O.RNG_SUBFILTER, 96, 2, 1, 1.0, SEED, 0,
-                 np.zeros(3, np.float32))
+    nsub, m = 256, W["m"]
+    p = model_params(E, W)
+    inputs, _ = E.make_trace(W["model"], p, W["seed"], steps)
+    md = O.model_from_params(W["model"], p)
+    S = E.model_info(W["model"])[0]
+    f = O.Filter(md, m, nsub, W["t"], O.EXCH_TORUS, resampler, O.RNG_SUBFILTER, 96, 2, 1, 1.0, W["seed"], 0,
+                 np.array(p.init_state[:S], np.float32))
     f.step(inputs["control"][0], inputs["meas"][0], threads)  # warm-up
     done, t0 = 0, time.perf_counter()
     for k in range(1, steps):
@@ -126,21 +144,21 @@ def cpu_baseline(steps, resampler, threads=0, budget_s=20.0):
     dt = time.perf_counter() - t0
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     f.close()
-    return {"value": M * nsub * done / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-            "sample": "%d steps of %d sub-filters x %d particles (2^17 of the 2^20 workload), torus 16x16, t=%d"
-                      % (done, nsub, M, T_EXCH)}
+    return {"value": m * nsub * done / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": "%d steps of %d sub-filters x %d particles (of the %s workload), torus 16x16, t=%d"
+                      % (done, nsub, m, W["desc"].split(" = ")[0], W["t"])}
 
 
 def reference_arm(args, rank, world):
     resampler = CONFIGS[args.resampler]
     if rank != 0:
         return 0
-    base = cpu_baseline(args.warmup + args.steps + 1, resampler, 0, budget_s=60.0)
+    W = WORKLOADS.get(args.workload, WORKLOADS["plain"])
+    base = cpu_baseline(args.warmup + args.steps + 1, resampler, 0, budget_s=60.0, W=W)
     line = {"metric": "particle-steps/s", "value": base["value"], "unit": "particle-steps/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace)",
-            "config": {"workload": "unicycle 2^20 particles = 2048x512, torus 32x64, t=2, %s resampling"
-                                   % args.resampler, "sample": base["sample"]},
+            "config": {"workload": "%s, %s resampling" % (W["desc"], args.resampler), "sample": base["sample"]},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -161,7 +179,7 @@ def run_batched(E, torch, args, local):
     counts, params, inputs, truth = W.batched_unicycle(args.batch_filters, steps)
     F = len(counts)
     P = int(counts.sum())
-    base = dict(num_transfer=2, exchange=E.EXCHANGE_RING, resampler=E.RESAMPLE_SYSTEMATIC, seed=SEED, device=local)
+    base = dict(num_transfer=2, exchange=E.EXCHANGE_RING, resampler=E.RESAMPLE_SYSTEMATIC, seed=4, device=local)
     # autotune on an evenly spaced slice of the filters, 16 steps
     sl = np.arange(0, F, max(1, F // 256))[:256]
     t0 = time.time()
@@ -285,7 +303,7 @@ def run_served(E, args, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--resampler", default="systematic", choices=sorted(CONFIGS))
@@ -293,7 +311,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "arm", "batched", "served"])
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--batch-filters", type=int, default=4096)
@@ -336,11 +354,13 @@ def main():
             print(json.dumps(line), flush=True)
         return 0
     resampler = CONFIGS[args.resampler]
-    p = E.unicycle_params(SEED)
+    W = WORKLOADS[args.workload]
+    m, nsub, particles = W["m"], W["nsub"], W["m"] * W["nsub"]
+    p = model_params(E, W)
     total_steps = args.warmup + args.steps
-    inputs, truth = E.make_trace(E.MODEL_UNICYCLE, p, SEED, total_steps + args.e2e_steps)
-    f = E.ParticleFilter(E.MODEL_UNICYCLE, p, particles_per_subfilter=M, num_subfilters=NSUB, num_transfer=T_EXCH,
-                         exchange=E.EXCHANGE_TORUS, resampler=resampler, seed=SEED + 1000 * rank, device=local,
+    inputs, truth = E.make_trace(W["model"], p, W["seed"], total_steps + args.e2e_steps)
+    f = E.ParticleFilter(W["model"], p, particles_per_subfilter=m, num_subfilters=nsub, num_transfer=W["t"],
+                         exchange=E.EXCHANGE_TORUS, resampler=resampler, seed=W["seed"] + 1000 * rank, device=local,
                          particles_per_thread=args.ppt if args.pipeline == "split" else 0,
                          pipeline={"fused": E.PIPELINE_FUSED, "split": E.PIPELINE_SPLIT}[args.pipeline])
     info = f.info()
@@ -382,7 +402,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE)
-    value = world * PARTICLES * args.steps / (total_ms * 1e-3)
+    value = world * particles * args.steps / (total_ms * 1e-3)
 
     # end to end through pf_step(): host input -> H2D, kernels, D2H of the estimate, per step
     e2e_ms = []
@@ -399,7 +419,7 @@ def main():
         t = torch.tensor([e2e_total], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * PARTICLES * args.e2e_steps / (e2e_total * 1e-3) if args.e2e_steps > 0 else None
+    e2e_value = world * particles * args.e2e_steps / (e2e_total * 1e-3) if args.e2e_steps > 0 else None
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -409,23 +429,29 @@ def main():
         # algorithmic bytes per particle by kernel: the sampling kernel reads the
         # state (12 B), the resampling kernel writes it (12 B), the single-kernel
         # step does both
-        kernel_alg = {"sample_sort": 12, "exchange_resample": 12, "step": 24}.get(dom, ALG_BYTES)
-        achieved = kernel_alg * PARTICLES / (phases[dom] * 1e-3) / 1e9
-        step_achieved = ALG_BYTES * PARTICLES / (float(np.mean(step_ms)) * 1e-3) / 1e9
+        alg = W["alg"]
+        kernel_alg = {"sample_sort": alg // 2, "exchange_resample": alg // 2, "step": alg}.get(dom, alg)
+        achieved = kernel_alg * particles / (phases[dom] * 1e-3) / 1e9
+        step_achieved = alg * particles / (float(np.mean(step_ms)) * 1e-3) / 1e9
         traffic, prof = None, {}
         tp = ROOT / "profiles" / "traffic.json"
         if tp.exists():
-            prof = json.loads(tp.read_text()).get("%s ppt%d" % (args.pipeline, info["particles_per_thread"]), {})
+            prof = json.loads(tp.read_text()).get("%s %s ppt%d" % (args.workload, args.pipeline,
+                                                                   info["particles_per_thread"]), {})
             traffic = prof.get(dom, {}).get("dram_bytes_per_launch")
-        rmse = float(np.sqrt(np.mean(np.sum((est["mean"][:, :2] - truth[:total_steps, :2]) ** 2, axis=1))))
+        if W["angles"]:  # joint angles, wrapped
+            d = est["mean"][:, list(W["angles"])] - truth[:total_steps, list(W["angles"])]
+            d = np.remainder(d + np.pi, 2 * np.pi) - np.pi
+        else:  # position
+            d = est["mean"][:, :2] - truth[:total_steps, :2]
+        rmse = float(np.sqrt(np.mean(np.sum(d ** 2, axis=1))))
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace, seed 2)",
-            "config": {"workload": "unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2, "
-                                   "%s resampling every step, FP32 state/log-weights, FP64 normalisation+cumsum"
-                                   % args.resampler,
-                       "particles": PARTICLES, "subfilters": NSUB, "particles_per_subfilter": M,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace, seed %d)" % W["seed"],
+            "config": {"workload": "%s, %s resampling every step, FP32 state/log-weights, FP64 "
+                                   "normalisation+cumsum" % (W["desc"], args.resampler),
+                       "particles": particles, "subfilters": nsub, "particles_per_subfilter": m,
                        "particles_per_thread": info["particles_per_thread"], "rng": "MTGP32 per sub-filter",
                        "pipeline": {0: "fused (one kernel per step)", 1: "phased", 2: "split"}[info["pipeline"]],
                        "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas" if world > 1
@@ -433,19 +459,19 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "kernel": dom, "kernel_ms": phases[dom], "share": phases[dom] / sum(phases.values()),
-                         "alg_bytes_per_launch": kernel_alg * PARTICLES,
+                         "alg_bytes_per_launch": kernel_alg * particles,
                          "ncu": prof.get(dom, {}).get("summary"),
                          "step": {"achieved": step_achieved, "frac": step_achieved / peak,
-                                  "alg_bytes_per_particle_step": ALG_BYTES, "phase_ms": phases}},
+                                  "alg_bytes_per_particle_step": alg, "phase_ms": phases}},
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 128,
                     "d2h_bytes_per_step": int(E.ESTIMATE_DTYPE.itemsize),
                     "ms_per_step": e2e_total / args.e2e_steps if args.e2e_steps > 0 else None},
             "gpu_launches": int(args.steps * len(phases)),
             "clocks": clocks,
-            "rmse_xy": rmse,
+            "rmse": {"value": rmse, "of": "joint angles (rad)" if W["angles"] else "x, y position (m)"},
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(40, resampler, 0, budget_s=15.0)
+            line["cpu_baseline"] = cpu_baseline(40, resampler, 0, budget_s=15.0, W=W)
         print(json.dumps(line), flush=True)
     f.close()
     if dist:
