@@ -1,0 +1,137 @@
+"""Row sharding of the 2D-torus exchange across ranks (one process per GPU).
+
+The torus of N sub-filters has dx = 2^floor(log2 sqrt N) columns and
+dy = N / dx rows; sub-filter b sits at column b % dx, row b // dx.  Each
+sub-filter's weakest 4t slots take the top-t particles of its right, left,
+bottom and top neighbours (slot m-1-j-k*t from neighbour k, the torus routing
+of the single-GPU engine).  With `world` ranks each rank owns dy / world
+consecutive rows.  Left/right neighbours are always on the same rank; the top
+neighbour of a rank's first row is the last row of the rank above, and the
+bottom neighbour of its last row is the first row of the rank below.  Per
+step every rank therefore sends two halos -- the top-t particles of its first
+row (to the rank above) and of its last row (to the rank below), dx * t
+particles each -- and receives two: one point-to-point exchange with each
+neighbouring rank, no collective over the particles.  The global estimate
+needs one small all-reduce of the FP64 partials.
+
+`halo_exchange` works with any torch.distributed backend (gloo on CPU tensors,
+NCCL on CUDA tensors).
+"""
+import numpy as np
+
+
+def torus_dims(N):
+    dx = 1
+    while (2 * dx) * (2 * dx) <= N:
+        dx *= 2
+    return dx, N // dx
+
+
+class TorusShard:
+    """Rank `rank`'s block of rows of an N-sub-filter torus (m particles each, t transferred)."""
+
+    def __init__(self, N, m, t, world, rank):
+        self.N, self.m, self.t, self.world, self.rank = N, m, t, world, rank
+        self.dx, self.dy = torus_dims(N)
+        if self.dx * self.dy != N:
+            raise ValueError("torus exchange needs N = dx * dy (N=%d)" % N)
+        if self.dy % world:
+            raise ValueError("%d torus rows do not split over %d ranks" % (self.dy, world))
+        if 5 * t > m:
+            raise ValueError("torus exchange needs 5 t <= m")
+        self.rows = self.dy // world
+        self.row0 = rank * self.rows
+        self.up = (rank - 1) % world    # owns the row above row0
+        self.down = (rank + 1) % world  # owns the row below the last row
+
+    @property
+    def first_subfilter(self):
+        return self.row0 * self.dx
+
+    @property
+    def num_subfilters(self):
+        return self.rows * self.dx
+
+    def halos_out(self, sorted_state, sorted_keys):
+        """(to_up, to_down): top-t particles of the first and last local row,
+        each (state [S, dx*t], keys [dx*t]) from the local sorted copy
+        (state [S, n*m], keys [n*m], sub-filters in local order)."""
+        m, t, dx = self.m, self.t, self.dx
+        out = []
+        for r in (0, self.rows - 1):
+            idx = np.array([(r * dx + c) * m + j for c in range(dx) for j in range(t)], np.int64)
+            out.append((sorted_state[:, idx], sorted_keys[idx]))
+        return out[0], out[1]
+
+    def sources(self):
+        """For every local sub-filter b and slot x < 4t (slot m-1-x): (where, index),
+        where 0 = local sorted copy (particle index), 1 = halo from the rank
+        above, 2 = halo from the rank below (index into the halo)."""
+        m, t, dx, dy = self.m, self.t, self.dx, self.dy
+        src = np.zeros((self.num_subfilters, 4 * t, 2), np.int64)
+        for lb in range(self.num_subfilters):
+            gb = self.first_subfilter + lb
+            x, y = gb % dx, gb // dx
+            for k in range(4):
+                if k == 0:
+                    fy, fx = y, (x + 1) % dx
+                elif k == 1:
+                    fy, fx = y, (x - 1) % dx
+                elif k == 2:
+                    fy, fx = (y + 1) % dy, x
+                else:
+                    fy, fx = (y - 1) % dy, x
+                for j in range(t):
+                    local_row = fy - self.row0
+                    if 0 <= local_row < self.rows:
+                        src[lb, k * t + j] = (0, (local_row * dx + fx) * m + j)
+                    elif k == 2:
+                        src[lb, k * t + j] = (2, fx * t + j)
+                    else:
+                        src[lb, k * t + j] = (1, fx * t + j)
+        return src
+
+    def apply_exchange(self, sorted_state, sorted_keys, halo_up, halo_down):
+        """The exchange on the local sorted copy: returns (state, keys) with each
+        sub-filter's weakest 4t slots replaced (the pre-resampling particles)."""
+        m, t = self.m, self.t
+        st, ks = sorted_state.copy(), sorted_keys.copy()
+        src = self.sources()
+        halos = {1: halo_up, 2: halo_down}
+        for lb in range(self.num_subfilters):
+            for x in range(4 * t):
+                where, i = src[lb, x]
+                dst = lb * m + m - 1 - x
+                if where == 0:
+                    st[:, dst] = sorted_state[:, i]
+                    ks[dst] = sorted_keys[i]
+                else:
+                    st[:, dst] = halos[where][0][:, i]
+                    ks[dst] = halos[where][1][i]
+        return st, ks
+
+
+def halo_exchange(dist, shard, to_up, to_down):
+    """Send this rank's first-row halo up and last-row halo down, receive the
+    neighbours' (torch tensors (state, keys)); returns (from_up, from_down).
+    Sends are posted down-halo first and receives up-halo first, so that with
+    two ranks (the same peer above and below) the messages pair up in order
+    on backends without tags; the tags say the same for those that use them.
+    With one rank both halos are the rank's own rows."""
+    import torch
+    if shard.world == 1:
+        return to_down, to_up
+    from_up = (torch.empty_like(to_up[0]), torch.empty_like(to_up[1]))
+    from_down = (torch.empty_like(to_down[0]), torch.empty_like(to_down[1]))
+    ops = []
+    for x in to_down:
+        ops.append(dist.P2POp(dist.isend, x.contiguous(), shard.down, tag=1))
+    for x in to_up:
+        ops.append(dist.P2POp(dist.isend, x.contiguous(), shard.up, tag=2))
+    for x in from_up:
+        ops.append(dist.P2POp(dist.irecv, x, shard.up, tag=1))
+    for x in from_down:
+        ops.append(dist.P2POp(dist.irecv, x, shard.down, tag=2))
+    for r in dist.batch_isend_irecv(ops):
+        r.wait()
+    return from_up, from_down
