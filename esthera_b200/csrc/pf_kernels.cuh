@@ -607,7 +607,47 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
     const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;
-    const float dec = (D.rng_fused ? U[0] : U[T + b]) - 1.0f;
+    // Every global read of the CTA is issued before the first barrier: the
+    // decision and resampling uniforms, the sorted keys and state of this
+    // sub-filter, and -- for the slots in the exchange range -- the
+    // neighbours' top-t (the slot's owner loads them, so each shared-memory
+    // slot has one writer).
+    const float dec_u = D.rng_fused ? U[0] : U[T + b];
+    float ur[RES == PF_RESAMPLE_VOSE ? 2 * E : E];
+    if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
+        ur[0] = D.rng_fused ? U[1] : U[(int64_t)b * M];
+    } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) ur[e] = D.rng_fused ? U[1 + E * tid + e] : U[(int64_t)b * M + E * tid + e];
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int64_t i = E * tid + e;
+            ur[2 * e] = D.rng_fused ? U[1 + 2 * i] : U[2 * ((int64_t)b * M + i)];
+            ur[2 * e + 1] = D.rng_fused ? U[2 + 2 * i] : U[2 * ((int64_t)b * M + i) + 1];
+        }
+    }
+    float okey[E], ost[S][E];
+    ldv<E>(D.tkey + base, okey);
+#pragma unroll
+    for (int v = 0; v < S; ++v) ldv<E>(D.tmp + v * T + base, ost[v]);
+    if (virt) {
+        int nx = exchange_count(D);
+        if (D.exch_period > 1 && (run_step(in) % D.exch_period) != 0) nx = 0;
+        if (E * tid + E - 1 >= M - nx) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int x = M - 1 - (E * tid + e);
+                if (x < nx) {
+                    const int64_t g = exchange_source(D, b, x);
+                    okey[e] = D.tkey[g];
+#pragma unroll
+                    for (int v = 0; v < S; ++v) ost[v][e] = D.tmp[v * T + g];
+                }
+            }
+        }
+    }
+    const float dec = dec_u - 1.0f;
     if (dec > D.freq) {
         if (D.sel) {
 #pragma unroll
@@ -618,31 +658,13 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     float* kb = reinterpret_cast<float*>(smem);
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
-    {
-        float o[E];
-        ldv<E>(D.tkey + base, o);
 #pragma unroll
-        for (int e = 0; e < E; ++e) kb[E * tid + e] = o[e];
+    for (int e = 0; e < E; ++e) kb[E * tid + e] = okey[e];
 #pragma unroll
-        for (int v = 0; v < S; ++v) {
-            ldv<E>(D.tmp + v * T + base, o);
+    for (int v = 0; v < S; ++v)
 #pragma unroll
-            for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = o[e];
-        }
-    }
+        for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = ost[v][e];
     __syncthreads();
-    if (virt) {
-        int nx = exchange_count(D);
-        if (D.exch_period > 1 && (run_step(in) % D.exch_period) != 0) nx = 0;
-        for (int x = tid; x < nx; x += NT) {
-            const int64_t g = exchange_source(D, b, x);
-            const int s = M - 1 - x;
-            kb[s] = D.tkey[g];
-#pragma unroll
-            for (int v = 0; v < S; ++v) tile[v * M + s] = D.tmp[v * T + g];
-        }
-        __syncthreads();
-    }
     float w[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) w[e] = kb[E * tid + e];
@@ -658,7 +680,7 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(scratch);
         const double tot = scan_f64<M, E>(w, cum, dred);
-        const float u0 = (D.rng_fused ? U[1] : U[(int64_t)b * M]) - 1.0f;
+        const float u0 = ur[0] - 1.0f;
         const double step = tot / (double)M;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -672,9 +694,7 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
         const float tot = blelloch_scan<M>(ex);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int i = E * tid + e;
-            const float u = D.rng_fused ? U[1 + i] : U[(int64_t)b * M + i];
-            sel[e] = ref_binary_search(ex, (u - 1.0f) * tot, M);
+            sel[e] = ref_binary_search(ex, (ur[e] - 1.0f) * tot, M);
         }
     } else {
         float* prob = reinterpret_cast<float*>(scratch);
@@ -684,10 +704,7 @@ __global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* _
         vose_build<M, E>(w, prob, alias, sl, scr, ired);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int64_t i = E * tid + e;
-            const float ux = (D.rng_fused ? U[1 + 2 * i] : U[2 * ((int64_t)b * M + i)]) - 1.0f;
-            const float uy = (D.rng_fused ? U[2 + 2 * i] : U[2 * ((int64_t)b * M + i) + 1]) - 1.0f;
-            sel[e] = (int)vose_draw<M>(prob, alias, ux, uy);
+            sel[e] = (int)vose_draw<M>(prob, alias, ur[2 * e] - 1.0f, ur[2 * e + 1] - 1.0f);
         }
     }
 #pragma unroll
