@@ -6,6 +6,7 @@
 // strides and the scans, one MTGP32 stream per CTA generating straight into
 // shared memory.  Citations are to the Esthera source tree.
 #pragma once
+#include <type_traits>
 
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -594,6 +595,51 @@ struct Unicycle {
         }
         return -0.5f * acc;
     }
+    // E particles at once: the same per-particle arithmetic as step() in the
+    // same order (bit-identical results), with the landmark loop outside the
+    // particle loop so each landmark's constants are read once per thread and
+    // the E likelihood chains interleave.  noise(e, v) gives particle e's v-th
+    // normal.
+    template <int E, class Noise>
+    __device__ static __forceinline__ void step_batch(const Consts& c, float (&s)[E][S], Noise noise,
+                                                      float (&sn)[E][NA], float (&cs)[E][NA], float (&ll)[E])
+    {
+        float s2[E], c2[E], acc[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            float st, ct;
+            __sincosf(s[e][2], &st, &ct);
+            const float nx = fmaf(c.sq0, noise(e, 0), fmaf(c.A, ct, fmaf(-c.B, st, s[e][0])));
+            const float ny = fmaf(c.sq1, noise(e, 1), fmaf(c.A, st, fmaf(c.B, ct, s[e][1])));
+            const float nt = wrap_pi(fmaf(c.sq2, noise(e, 2), s[e][2] + c.wd));
+            s[e][0] = nx;
+            s[e][1] = ny;
+            s[e][2] = nt;
+            __sincosf(nt, &s2[e], &c2[e]);
+            sn[e][0] = s2[e];
+            cs[e][0] = c2[e];
+            acc[e] = 0.0f;
+        }
+        const int L = c.L;
+        const float isr = c.isr, isb = c.isb;
+#pragma unroll 1
+        for (int j = 0; j < L; ++j) {
+            const float lx = c.lx[j], ly = c.ly[j], rm = c.rm[j], cb = c.cb[j], sb = c.sb[j];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const float dx = lx - s[e][0], dy = ly - s[e][1];
+                const float r = pf_sqrt(fmaf(dx, dx, dy * dy));
+                const float er = (rm - r) * isr;
+                const float cp = fmaf(c2[e], cb, -(s2[e] * sb));
+                const float sp = fmaf(s2[e], cb, c2[e] * sb);
+                const float eb = pf_atan2(fmaf(sp, dx, -(cp * dy)), fmaf(cp, dx, sp * dy)) * isb;
+                acc[e] = fmaf(er, er, acc[e]);
+                acc[e] = fmaf(eb, eb, acc[e]);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) ll[e] = -0.5f * acc[e];
+    }
 };
 
 struct DhArm {
@@ -729,6 +775,32 @@ __host__ __device__ constexpr bool is_angle_var(int v)
     for (int i = 0; i < Mdl::NA; ++i)
         if (Mdl::angle_var(i) == v) return true;
     return false;
+}
+
+
+// E particles of a model at once: Mdl::step_batch when the model has one,
+// otherwise step() particle by particle.  noise(e, v): particle e's v-th normal.
+template <class Mdl, class = void>
+struct HasStepBatch : std::false_type {};
+template <class Mdl>
+struct HasStepBatch<Mdl, std::void_t<decltype(&Mdl::template step_batch<1, float (*)(int, int)>)>> : std::true_type {};
+
+template <class Mdl, int E, class Noise>
+__device__ __forceinline__ void model_step_batch(const typename Mdl::Consts& c, float (&s)[E][Mdl::S], Noise noise,
+                                                 float (&sn)[E][Mdl::NA > 0 ? Mdl::NA : 1],
+                                                 float (&cs)[E][Mdl::NA > 0 ? Mdl::NA : 1], float (&ll)[E])
+{
+    if constexpr (HasStepBatch<Mdl>::value) {
+        Mdl::template step_batch<E>(c, s, noise, sn, cs, ll);
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            float n[Mdl::K];
+#pragma unroll
+            for (int v = 0; v < Mdl::K; ++v) n[v] = noise(e, v);
+            ll[e] = Mdl::step(c, s[e], n, sn[e], cs[e]);
+        }
+    }
 }
 
 }  // namespace pfdev

@@ -247,14 +247,13 @@ __global__ void __launch_bounds__(M / E) k_sample_sort(const FilterDesc* __restr
         for (int e = 0; e < E; ++e) st[e][v] = o[e];
     }
     float okey[E], sn[E][NANG], cs[E][NANG];
+    {
+        float ll[E];
+        model_step_batch<Mdl, E>(
+            cst, st,
+            [&](int e, int v) { return FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e]; }, sn, cs, ll);
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-        float n[K];
-#pragma unroll
-        for (int v = 0; v < K; ++v)
-            n[v] = FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e];
-        const float ll = Mdl::step(cst, st[e], n, sn[e], cs[e]);
-        okey[e] = D.log_weights ? ll : __expf(ll);
+        for (int e = 0; e < E; ++e) okey[e] = D.log_weights ? ll[e] : __expf(ll[e]);
     }
     if (D.inplace) {
 #pragma unroll
