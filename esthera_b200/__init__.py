@@ -17,7 +17,7 @@ from pathlib import Path
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libesthera_b200.so"
+LIB_PATH = Path(os.environ["ESTHERA_B200_LIB"]) if os.environ.get("ESTHERA_B200_LIB") else _PKG / "libesthera_b200.so"
 
 # enums (include/esthera_b200.h)
 PF_OK, PF_ERR_INVALID, PF_ERR_CUDA, PF_ERR_NOMEM, PF_ERR_UNSUPPORTED, PF_ERR_IO = 0, 1, 2, 3, 4, 5

@@ -48,6 +48,32 @@ struct FilterDesc {
     ModelParams mp;
 };
 
+// Register budgets of the split pipeline's kernels, as resident warps per SM
+// asked of the compiler: __launch_bounds__(threads, ceil(warps * 32 / threads))
+// caps the registers at 65536 / (that many threads).  Small states (the
+// unicycle's 3 variables) take 36 / 32 warps: the sampling kernel at m = 512,
+// 4 particles per thread runs 53 us capped at 56 registers against 59 us at
+// the compiler's own 83.  The arms' states (9-12 variables, forward
+// kinematics) need ~128 registers per thread; capping them lower spills.
+#ifndef PF_K1_WARPS_SMALL
+#define PF_K1_WARPS_SMALL 36
+#endif
+#ifndef PF_K1_WARPS_LARGE
+#define PF_K1_WARPS_LARGE 16
+#endif
+#ifndef PF_K2_WARPS_SMALL
+#define PF_K2_WARPS_SMALL 32
+#endif
+#ifndef PF_K2_WARPS_LARGE
+#define PF_K2_WARPS_LARGE 16
+#endif
+__host__ __device__ constexpr int pf_min_blocks(int threads, int warps)
+{
+    return (warps * 32 + threads - 1) / threads > 32 ? 32 : (warps * 32 + threads - 1) / threads;
+}
+__host__ __device__ constexpr int pf_k1_warps(int S) { return S <= 3 ? PF_K1_WARPS_SMALL : PF_K1_WARPS_LARGE; }
+__host__ __device__ constexpr int pf_k2_warps(int S) { return S <= 3 ? PF_K2_WARPS_SMALL : PF_K2_WARPS_LARGE; }
+
 struct InputRef {
     const pf_step_input* base;
     int64_t filter_stride;   // inputs per filter (batched: [filter][step])
@@ -187,7 +213,7 @@ __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float
 // stream in the kernel; otherwise read reference-layout normals from rbuf.
 // ---------------------------------------------------------------------------
 template <class Mdl, int M, int E, bool FR>
-__global__ void __launch_bounds__(M / E) k_sample_sort(const FilterDesc* __restrict__ descs,
+__global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S))) k_sample_sort(const FilterDesc* __restrict__ descs,
                                                        const int2* __restrict__ cta_map, InputRef in)
 {
     constexpr int NT = M / E, S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
@@ -590,7 +616,7 @@ constexpr size_t k2_smem()
 }
 
 template <int S, int M, int E, int RES>
-__global__ void __launch_bounds__(M / E) k_exchange_resample(const FilterDesc* __restrict__ descs,
+__global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k_exchange_resample(const FilterDesc* __restrict__ descs,
                                                              const int2* __restrict__ cta_map, InputRef in,
                                                              int32_t* step_ctr, int virt)
 {
