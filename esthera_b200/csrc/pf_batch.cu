@@ -302,9 +302,15 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
     }
     {
-        std::vector<int2> map((size_t)NS);
+        // group leaders (sub-filters 0, 32, 64, ... of each filter) first: the
+        // resampling kernel's CTAs that combine the estimates run in its first wave
+        std::vector<int2> map;
+        map.reserve((size_t)NS);
         for (int f = 0; f < num_filters; ++f)
-            for (int b = 0; b < B->nsub[f]; ++b) map[(size_t)B->sub_off[f] + b] = make_int2(f, b);
+            for (int b = 0; b < B->nsub[f]; b += 32) map.push_back(make_int2(f, b));
+        for (int f = 0; f < num_filters; ++f)
+            for (int b = 0; b < B->nsub[f]; ++b)
+                if (b & 31) map.push_back(make_int2(f, b));
         if (cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
             launch_mtgp_init(B->mtgp, (int)NS, cfg->stream_offset, cfg->seed, B->stream) != cudaSuccess ||
             cudaStreamSynchronize(B->stream) != cudaSuccess) {

@@ -136,6 +136,20 @@ __device__ __forceinline__ void cta_target(const int2* __restrict__ cta_map, int
     }
 }
 
+// The resampling kernel's CTA order puts the first sub-filter of every group of
+// 32 (the CTAs that combine the estimate partials, the last of them also the
+// global estimate) ahead of the rest, so the estimate runs in the first wave
+// instead of delaying a CTA of the last one.  Without a CTA map: CTA i < ng
+// takes sub-filter 32 i, CTA ng + j takes the j-th of the others.  Maps built
+// by the batch and the server list the group leaders first in the same way.
+__device__ __forceinline__ int leaders_first(int i, int N)
+{
+    const int ng = (N + 31) >> 5;
+    if (i < ng) return i << 5;
+    const int j = i - ng;
+    return j + j / 31 + 1;
+}
+
 __device__ __forceinline__ const pf_step_input* input_of(const InputRef& in, int f)
 {
     return in.base + (int64_t)f * in.filter_stride + step_index(in);
@@ -625,7 +639,14 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
     __shared__ double dred[33];
     __shared__ int ired[34];
     int f, b;
-    cta_target(cta_map, f, b);
+    if (cta_map) {
+        const int2 c = cta_map[blockIdx.x];
+        f = c.x;
+        b = c.y;
+    } else {
+        f = 0;
+        b = leaders_first(blockIdx.x, descs[0].N);
+    }
     const FilterDesc& D = descs[f];
     const int tid = threadIdx.x;
     estimate_groups<S>(D, b, in, step_ctr);

@@ -30,13 +30,16 @@ using namespace pfhost;
 
 namespace {
 
-struct Pending {        // one update in a batch (host -> device)
+struct Pending {         // one update in a batch (host -> device)
     int32_t slot;
-    int32_t first_cta;  // position of the slot's first sub-filter in its model's CTA map
+    int32_t first_lead;  // position of the slot's group leaders in its model's CTA map
+    int32_t first_rest;  // position of its other sub-filters, after all groups' leaders
 };
 
 // One block per batched update: copy its input into the slot's input entry
-// and write the slot's CTA map entries.
+// and write the slot's CTA map entries -- group leaders (sub-filters 0, 32,
+// ...) in the map's leader region, the rest after all leaders, so that the
+// resampling kernel combines the estimates in its first wave.
 __global__ void k_srv_expand(const Pending* __restrict__ pend, const pf_step_input* __restrict__ in, int n,
                              const FilterDesc* __restrict__ descs, pf_step_input* __restrict__ slot_in,
                              int2* __restrict__ map)
@@ -45,7 +48,10 @@ __global__ void k_srv_expand(const Pending* __restrict__ pend, const pf_step_inp
     if (i >= n) return;
     const Pending p = pend[i];
     const int N = descs[p.slot].N;
-    for (int b = threadIdx.x; b < N; b += blockDim.x) map[p.first_cta + b] = make_int2(p.slot, b);
+    for (int b = threadIdx.x; b < N; b += blockDim.x) {
+        const int at = (b & 31) == 0 ? p.first_lead + (b >> 5) : p.first_rest + b - (b >> 5) - 1;
+        map[at] = make_int2(p.slot, b);
+    }
     const uint32_t* src = reinterpret_cast<const uint32_t*>(in + i);
     uint32_t* dst = reinterpret_cast<uint32_t*>(slot_in + p.slot);
     for (int w = threadIdx.x; w < (int)(sizeof(pf_step_input) / 4); w += blockDim.x) dst[w] = src[w];
@@ -443,19 +449,29 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     s->batch_slots.clear();
     s->batch_tags.clear();
     // group the batch by model so each model's kernels see one contiguous CTA map
-    for (int m = 0; m < 3; ++m)
+    for (int m = 0; m < 3; ++m) {
+        const int first = n;
+        int64_t leads = 0;
         for (int i = 0; i < s->max_filters; ++i) {
             Slot& sl = s->slots[i];
             if (!sl.open || sl.model != m || sl.in_flight || sl.queue.empty()) continue;
-            s->h_pend[n] = Pending{i, (int32_t)ctas[m]};
+            s->h_pend[n] = Pending{i, (int32_t)leads, 0};
             s->h_in[n] = sl.queue.front().first;
             s->batch_slots.push_back(i);
             s->batch_tags.push_back(sl.queue.front().second);
             sl.queue.pop_front();
             sl.in_flight = true;
+            leads += (sl.N + 31) / 32;
             ctas[m] += sl.N;
             ++n;
         }
+        int64_t rest = leads;  // the other sub-filters follow all of the group's leaders
+        for (int q = first; q < n; ++q) {
+            s->h_pend[q].first_rest = (int32_t)rest;
+            const int N = s->slots[s->h_pend[q].slot].N;
+            rest += N - (N + 31) / 32;
+        }
+    }
     if (n == 0) return PF_OK;
     const int M = s->cfg.particles_per_subfilter, E = s->E;
     cudaStream_t st = s->stream;
