@@ -253,7 +253,7 @@ static int default_ppt(int M)
 {
     if (M <= 32) return 1;
     if (M <= 64) return 2;
-    return 2;
+    return 4;
 }
 
 void pfhost::torus_dims(int N, int* dx, int* dy)
@@ -302,11 +302,8 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
         return fail(PF_ERR_INVALID, "the phased pipeline uses the reference RNG layout (rng = PF_RNG_REFLAYOUT)");
     if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED && c->pipeline != PF_PIPELINE_SPLIT)
         return fail(PF_ERR_INVALID, "unknown pipeline");
-    const bool fused = c->pipeline == PF_PIPELINE_FUSED && c->rng == PF_RNG_SUBFILTER && step_supported(M) &&
-                       c->exchange_period <= 1 &&
-                       (c->particles_per_thread == 0 || c->particles_per_thread == M / 32);
-    *E = fused ? M / 32 : (c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M));
-    if (!fused && !me_supported(M, *E))
+    *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M);
+    if (!me_supported(M, *E))
         return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", *E, M);
     (void)model;
     (void)mi;
@@ -411,8 +408,7 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     memcpy(&f->mp, params, params_size);
     f->mi = mi;
     f->ops = model_ops(model);
-    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER && cfg->exchange_period <= 1 &&
-               step_supported(cfg->particles_per_subfilter) && E == cfg->particles_per_subfilter / 32)
+    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER && cfg->exchange_period <= 1)
                   ? PF_PIPELINE_FUSED
                   : (cfg->pipeline == PF_PIPELINE_PHASED ? PF_PIPELINE_PHASED : PF_PIPELINE_SPLIT);
     f->angle_mask = angle_mask_of(model);
@@ -523,7 +519,7 @@ static pf_status materialise(pf_filter* f)
 {
     if (f->pipe != PF_PIPELINE_FUSED) return PF_OK;
     InputRef none{nullptr, 0, nullptr, 0};
-    CU(f->ops.step(f->M, f->cfg.resampler, f->N, f->stream, f->d_desc, f->X, none, nullptr, true));
+    CU(f->ops.step(f->M, f->E, f->cfg.resampler, f->N, f->stream, f->d_desc, f->X, none, nullptr, true));
     CU(cudaStreamSynchronize(f->stream));
     return PF_OK;
 }
@@ -638,7 +634,7 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
         CU(mark("boxmuller"));
     }
     if (f->pipe == PF_PIPELINE_FUSED) {
-        CU(f->ops.step(M, c.resampler, N, st, desc, f->X, in, ctr_inc, false));
+        CU(f->ops.step(M, E, c.resampler, N, st, desc, f->X, in, ctr_inc, false));
         CU(mark("step"));
         if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
             CU(launch_a2a_merge_step(desc, f->X, st));

@@ -43,7 +43,8 @@ struct ModelOps {
     cudaError_t (*exchange_inplace)(int, int, cudaStream_t, const FilterDesc*, const int2*);
     cudaError_t (*test_model)(const ModelParams&, const pf_step_input*, int, float*, const float*, float*,
                               cudaStream_t);
-    cudaError_t (*step)(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+    cudaError_t (*step)(int, int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*,
+                        bool);
 };
 ModelOps model_ops(int model);
 

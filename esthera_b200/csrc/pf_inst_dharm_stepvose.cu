@@ -2,5 +2,5 @@
 #define PF_PART_STEPVOSE
 #include "pf_launch_impl.cuh"
 namespace pfdev {
-template cudaError_t Launch<DhArm>::step_vose(int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+template cudaError_t Launch<DhArm>::step_vose(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
 }  // namespace pfdev

@@ -7,5 +7,5 @@ template cudaError_t Launch<RefArm>::block_sort(int, int, int, cudaStream_t, con
 template cudaError_t Launch<RefArm>::exchange_resample(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef, int32_t*, int);
 template cudaError_t Launch<RefArm>::exchange_inplace(int, int, cudaStream_t, const FilterDesc*, const int2*);
 template cudaError_t Launch<RefArm>::test_model(const ModelParams&, const pf_step_input*, int, float*, const float*, float*, cudaStream_t);
-template cudaError_t Launch<RefArm>::step(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+template cudaError_t Launch<RefArm>::step(int, int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
 }  // namespace pfdev

@@ -2,5 +2,5 @@
 #define PF_PART_STEPSYS
 #include "pf_launch_impl.cuh"
 namespace pfdev {
-template cudaError_t Launch<Unicycle>::step_sys(int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
+template cudaError_t Launch<Unicycle>::step_sys(int, int, int, cudaStream_t, const FilterDesc*, const StepState&, InputRef, int32_t*, bool);
 }  // namespace pfdev

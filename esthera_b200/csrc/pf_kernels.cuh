@@ -629,35 +629,30 @@ constexpr size_t k2_smem()
     return s;
 }
 
+// Resampling of sub-filter b from a sorted copy (src_tmp, src_key: this
+// filter's arrays, sorted per sub-filter) with the exchange applied virtually
+// (nx weakest slots take the neighbours' top-t, read from the same sorted
+// copy).  U: the sub-filter's uniforms (decision first).  Returns false when
+// the decision uniform exceeds resampling_freq (the sub-filter keeps its
+// propagated particles); otherwise st holds this thread's E resampled
+// particles (positions E*tid+e) and sel their source slots.  Every thread of
+// the CTA must call it (it synchronises the CTA).  Restates resampling
+// (pf_generic_soa.cu:415-453) for PF_RESAMPLE_REFERENCE and resampling_valias
+// (resampling-valias.cl:214-300) for PF_RESAMPLE_VOSE; PF_RESAMPLE_SYSTEMATIC
+// uses the FP64 scan.
 template <int S, int M, int E, int RES>
-__global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k_exchange_resample(const FilterDesc* __restrict__ descs,
-                                                             const int2* __restrict__ cta_map, InputRef in,
-                                                             int32_t* step_ctr, int virt)
+__device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const float* __restrict__ src_tmp,
+                                              const float* __restrict__ src_key, const float* __restrict__ U,
+                                              int nx, unsigned char* smem, double* dred, int* ired,
+                                              float (&st)[E][S], int (&sel)[E])
 {
-    constexpr int NT = M / E;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double dred[33];
-    __shared__ int ired[34];
-    int f, b;
-    if (cta_map) {
-        const int2 c = cta_map[blockIdx.x];
-        f = c.x;
-        b = c.y;
-    } else {
-        f = 0;
-        b = leaders_first(blockIdx.x, descs[0].N);
-    }
-    const FilterDesc& D = descs[f];
     const int tid = threadIdx.x;
-    estimate_groups<S>(D, b, in, step_ctr);
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
-    const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;
-    // Every global read of the CTA is issued before the first barrier: the
-    // decision and resampling uniforms, the sorted keys and state of this
-    // sub-filter, and -- for the slots in the exchange range -- the
-    // neighbours' top-t (the slot's owner loads them, so each shared-memory
-    // slot has one writer).
+    // Every global read is issued before the first barrier: the decision and
+    // resampling uniforms, the sorted keys and state of this sub-filter, and --
+    // for the slots in the exchange range -- the neighbours' top-t (the slot's
+    // owner loads them, so each shared-memory slot has one writer).
     const float dec_u = D.rng_fused ? U[0] : U[T + b];
     float ur[RES == PF_RESAMPLE_VOSE ? 2 * E : E];
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
@@ -674,33 +669,22 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
         }
     }
     float okey[E], ost[S][E];
-    ldv<E>(D.tkey + base, okey);
+    ldv<E>(src_key + base, okey);
 #pragma unroll
-    for (int v = 0; v < S; ++v) ldv<E>(D.tmp + v * T + base, ost[v]);
-    if (virt) {
-        int nx = exchange_count(D);
-        if (D.exch_period > 1 && (run_step(in) % D.exch_period) != 0) nx = 0;
-        if (E * tid + E - 1 >= M - nx) {
+    for (int v = 0; v < S; ++v) ldv<E>(src_tmp + v * T + base, ost[v]);
+    if (E * tid + E - 1 >= M - nx) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const int x = M - 1 - (E * tid + e);
-                if (x < nx) {
-                    const int64_t g = exchange_source(D, b, x);
-                    okey[e] = D.tkey[g];
+        for (int e = 0; e < E; ++e) {
+            const int x = M - 1 - (E * tid + e);
+            if (x < nx) {
+                const int64_t g = exchange_source(D, b, x);
+                okey[e] = src_key[g];
 #pragma unroll
-                    for (int v = 0; v < S; ++v) ost[v][e] = D.tmp[v * T + g];
-                }
+                for (int v = 0; v < S; ++v) ost[v][e] = src_tmp[v * T + g];
             }
         }
     }
-    const float dec = dec_u - 1.0f;
-    if (dec > D.freq) {
-        if (D.sel) {
-#pragma unroll
-            for (int e = 0; e < E; ++e) D.sel[base + e] = -1;
-        }
-        return;  // the propagated state was written in place by the sampling kernel
-    }
+    if (dec_u - 1.0f > D.freq) return false;
     float* kb = reinterpret_cast<float*>(smem);
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
@@ -722,7 +706,6 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
 #pragma unroll
         for (int e = 0; e < E; ++e) w[e] = __expf(w[e] - mx);
     }
-    int sel[E];
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(scratch);
         const double tot = scan_f64<M, E>(w, cum, dred);
@@ -739,9 +722,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
         for (int e = 0; e < E; ++e) ex[E * tid + e] = w[e];
         const float tot = blelloch_scan<M>(ex);
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            sel[e] = ref_binary_search(ex, (ur[e] - 1.0f) * tot, M);
-        }
+        for (int e = 0; e < E; ++e) sel[e] = ref_binary_search(ex, (ur[e] - 1.0f) * tot, M);
     } else {
         float* prob = reinterpret_cast<float*>(scratch);
         unsigned* alias = reinterpret_cast<unsigned*>(prob + M);
@@ -749,15 +730,58 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
         float* scr = reinterpret_cast<float*>(sl + M);
         vose_build<M, E>(w, prob, alias, sl, scr, ired);
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
+        for (int e = 0; e < E; ++e)
             sel[e] = (int)vose_draw<M>(prob, alias, ur[2 * e] - 1.0f, ur[2 * e + 1] - 1.0f);
+    }
+#pragma unroll
+    for (int v = 0; v < S; ++v)
+#pragma unroll
+        for (int e = 0; e < E; ++e) st[e][v] = tile[v * M + sel[e]];
+    return true;
+}
+
+template <int S, int M, int E, int RES>
+__global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k_exchange_resample(const FilterDesc* __restrict__ descs,
+                                                             const int2* __restrict__ cta_map, InputRef in,
+                                                             int32_t* step_ctr, int virt)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double dred[33];
+    __shared__ int ired[34];
+    int f, b;
+    if (cta_map) {
+        const int2 c = cta_map[blockIdx.x];
+        f = c.x;
+        b = c.y;
+    } else {
+        f = 0;
+        b = leaders_first(blockIdx.x, descs[0].N);
+    }
+    const FilterDesc& D = descs[f];
+    const int tid = threadIdx.x;
+    estimate_groups<S>(D, b, in, step_ctr);
+    const int64_t T = D.T;
+    const int64_t base = (int64_t)b * M + E * tid;
+    const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;
+    int nx = 0;
+    if (virt) {
+        nx = exchange_count(D);
+        if (D.exch_period > 1 && (run_step(in) % D.exch_period) != 0) nx = 0;
+    }
+    float st[E][S];
+    int sel[E];
+    if (!resample_from<S, M, E, RES>(D, b, D.tmp, D.tkey, U, nx, smem, dred, ired, st, sel)) {
+        if (D.sel) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) D.sel[base + e] = -1;
         }
+        return;  // the propagated state was written in place by the sampling kernel
     }
 #pragma unroll
     for (int v = 0; v < S; ++v) {
         float o[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) o[e] = tile[v * M + sel[e]];
+        for (int e = 0; e < E; ++e) o[e] = st[e][v];
         stv<E>(D.state + v * T + base, o);
     }
     if (D.sel) {

@@ -2,7 +2,7 @@
 // thread, resampler) onto the compiled kernel instantiations.
 #pragma once
 
-#include "pf_step.cuh"
+#include "pf_step_cta.cuh"
 
 namespace pfdev {
 
@@ -50,13 +50,13 @@ struct Launch {
                                          const int2* map, InputRef in, int32_t* ctr, int virt);
     static cudaError_t exchange_inplace(int grid, int threads, cudaStream_t st, const FilterDesc* d,
                                         const int2* map);
-    static cudaError_t step_ref(int M, int N, cudaStream_t st, const FilterDesc* d, const StepState& X, InputRef in,
-                                int32_t* ctr, bool ro);
-    static cudaError_t step_sys(int M, int N, cudaStream_t st, const FilterDesc* d, const StepState& X, InputRef in,
-                                int32_t* ctr, bool ro);
-    static cudaError_t step_vose(int M, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
+    static cudaError_t step_ref(int M, int E, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
+                                InputRef in, int32_t* ctr, bool ro);
+    static cudaError_t step_sys(int M, int E, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
+                                InputRef in, int32_t* ctr, bool ro);
+    static cudaError_t step_vose(int M, int E, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
                                  InputRef in, int32_t* ctr, bool ro);
-    static cudaError_t step(int M, int res, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
+    static cudaError_t step(int M, int E, int res, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
                             InputRef in, int32_t* ctr, bool resample_only);
     static cudaError_t test_model(const ModelParams& mp, const pf_step_input* in, int n, float* state,
                                   const float* noise, float* ll, cudaStream_t st);
@@ -77,6 +77,5 @@ cudaError_t launch_a2a_merge(int nfilters, const FilterDesc* d, cudaStream_t st)
 cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStream_t st);
 cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st);
 
-inline bool step_supported(int M) { return M == 128 || M == 256 || M == 512; }
 
 }  // namespace pfdev

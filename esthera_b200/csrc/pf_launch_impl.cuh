@@ -117,12 +117,12 @@ cudaError_t Launch<Mdl>::exchange_inplace(int grid, int threads, cudaStream_t st
 }
 
 template <class Mdl>
-cudaError_t Launch<Mdl>::step(int M, int res, int N, cudaStream_t st, const FilterDesc* d, const StepState& X,
-                              InputRef in, int32_t* ctr, bool resample_only)
+cudaError_t Launch<Mdl>::step(int M, int E, int res, int N, cudaStream_t st, const FilterDesc* d,
+                              const StepState& X, InputRef in, int32_t* ctr, bool resample_only)
 {
-    if (res == PF_RESAMPLE_SYSTEMATIC) return step_sys(M, N, st, d, X, in, ctr, resample_only);
-    if (res == PF_RESAMPLE_REFERENCE) return step_ref(M, N, st, d, X, in, ctr, resample_only);
-    return step_vose(M, N, st, d, X, in, ctr, resample_only);
+    if (res == PF_RESAMPLE_SYSTEMATIC) return step_sys(M, E, N, st, d, X, in, ctr, resample_only);
+    if (res == PF_RESAMPLE_REFERENCE) return step_ref(M, E, N, st, d, X, in, ctr, resample_only);
+    return step_vose(M, E, N, st, d, X, in, ctr, resample_only);
 }
 
 template <class Mdl>
@@ -135,32 +135,32 @@ cudaError_t Launch<Mdl>::test_model(const ModelParams& mp, const pf_step_input* 
 #endif
 
 #if defined(PF_PART_STEPREF) || defined(PF_PART_STEPSYS) || defined(PF_PART_STEPVOSE)
-#define PF_STEP_CASE(m, RES)                                                             \
-    if (M == m) {                                                                        \
-        constexpr size_t sm = kWarpsPerCta * StepSmem<Mdl, m, RES>::kPerWarp;            \
-        const int grid = (N + kWarpsPerCta - 1) / kWarpsPerCta;                          \
-        if (ro) {                                                                        \
-            auto fn = k_resample_only<Mdl, m, RES>;                                      \
-            cudaError_t r = allow_smem(fn, sm);                                          \
-            if (r != cudaSuccess) return r;                                              \
-            fn<<<grid, 32 * kWarpsPerCta, sm, st>>>(d, X);                                             \
-        } else {                                                                         \
-            auto fn = k_step<Mdl, m, RES>;                                               \
-            cudaError_t r = allow_smem(fn, sm);                                          \
-            if (r != cudaSuccess) return r;                                              \
-            fn<<<grid, 32 * kWarpsPerCta, sm, st>>>(d, X, nullptr, in, ctr);                           \
-        }                                                                                \
-        return cudaGetLastError();                                                       \
+#define PF_STEP_CASE(m, e, RES)                                      \
+    if (M == m && E == e) {                                          \
+        constexpr size_t sm = step_cta_smem<Mdl, m, e, RES>();       \
+        if (ro) {                                                    \
+            auto fn = k_resample_only_cta<Mdl, m, e, RES>;           \
+            cudaError_t r = allow_smem(fn, sm);                      \
+            if (r != cudaSuccess) return r;                          \
+            fn<<<N, m / e, sm, st>>>(d, X);                          \
+        } else {                                                     \
+            auto fn = k_step_cta<Mdl, m, e, RES>;                    \
+            cudaError_t r = allow_smem(fn, sm);                      \
+            if (r != cudaSuccess) return r;                          \
+            fn<<<N, m / e, sm, st>>>(d, X, in, ctr);                 \
+        }                                                            \
+        return cudaGetLastError();                                   \
     }
-#define PF_STEP_DEF(NAME, RES)                                                                             \
-    template <class Mdl>                                                                                   \
-    cudaError_t Launch<Mdl>::NAME(int M, int N, cudaStream_t st, const FilterDesc* d, const StepState& X, \
-                                  InputRef in, int32_t* ctr, bool ro)                                     \
-    {                                                                                                      \
-        PF_STEP_CASE(128, RES)                                                                             \
-        PF_STEP_CASE(256, RES)                                                                             \
-        PF_STEP_CASE(512, RES)                                                                             \
-        return cudaErrorInvalidValue;                                                                      \
+#define PF_STEP_CASE_0(m, e) PF_STEP_CASE(m, e, 0)
+#define PF_STEP_CASE_1(m, e) PF_STEP_CASE(m, e, 1)
+#define PF_STEP_CASE_2(m, e) PF_STEP_CASE(m, e, 2)
+#define PF_STEP_DEF(NAME, RES)                                                                                 \
+    template <class Mdl>                                                                                       \
+    cudaError_t Launch<Mdl>::NAME(int M, int E, int N, cudaStream_t st, const FilterDesc* d, const StepState& X, \
+                                  InputRef in, int32_t* ctr, bool ro)                                         \
+    {                                                                                                          \
+        PF_ME_LIST(PF_STEP_CASE_##RES)                                                                         \
+        return cudaErrorInvalidValue;                                                                          \
     }
 #if defined(PF_PART_STEPREF)
 PF_STEP_DEF(step_ref, 0)

@@ -40,16 +40,16 @@ def test_phased_equals_split(gpu, res, exch, t):
         assert np.allclose(x["mean"], y["mean"], rtol=1e-12, atol=1e-12)
 
 
-@pytest.mark.parametrize("m", [128, 256, 512])
+@pytest.mark.parametrize("m,ppt", [(128, 4), (256, 8), (512, 16), (512, 4), (256, 2), (64, 2)])
 @pytest.mark.parametrize("res", [0, 1, 2])
 @pytest.mark.parametrize("exch,t", [(0, 0), (1, 3), (2, 2), (3, 4)])
-def test_fused_equals_split(gpu, m, res, exch, t):
-    """The single-kernel step (one warp per sub-filter, resampling deferred to the
+def test_fused_equals_split(gpu, m, ppt, res, exch, t):
+    """The single-kernel step (one CTA per sub-filter, resampling deferred to the
     next launch) against the split pipeline with the same particles per thread."""
     E = gpu
     p, inputs, _ = uni_setup()
     common = dict(particles_per_subfilter=m, num_subfilters=16, num_transfer=t, exchange=exch, resampler=res,
-                  particles_per_thread=m // 32)
+                  particles_per_thread=ppt)
     fa, ea = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_SPLIT, **common)
     fb, eb = run(E, UNI, p, inputs, 6, pipeline=E.PIPELINE_FUSED, **common)
     assert fb.info()["pipeline"] == E.PIPELINE_FUSED and fa.info()["pipeline"] == E.PIPELINE_SPLIT
