@@ -446,12 +446,69 @@ __device__ void vose_build(const float (&w)[E], float* prob, unsigned* alias, un
     unsigned large_rend = small_end - 1u;  // = M-1 - n_large
     unsigned small_begin = 0;
     __syncthreads();
-    // pairing rounds; each round retires >= 1 small entry, so <= M rounds
-    for (int round = 0; round < M; ++round) {
+    // Pairing rounds; each retires >= 1 small entry, so <= M rounds.  Round:
+    // the first `nactive` smalls take the `nactive` larges at the bottom of the
+    // large list as aliases, the larges' reduced probabilities are appended to
+    // the small list (ascending) or pushed back on the large list, in pair
+    // order.  Rounds of at most 32 pairs (the common case once the few large
+    // weights are being used up) run in warp 0 alone, without CTA barriers.
+    const int lane = tid & 31;
+    for (int round = 0; round < M;) {
         const unsigned se = small_end;
         const unsigned a = se - small_begin, b = (unsigned)M - se;
         const unsigned nactive = a < b ? a : b;
         if (nactive == 0) break;
+        if (nactive <= 32) {
+            if (tid < 32) {
+                unsigned sb = small_begin, sen = small_end, lr = large_rend;
+                int rr = round;
+                for (; rr < M; ++rr) {
+                    const unsigned aa = sen - sb, bb = (unsigned)M - sen;
+                    const unsigned na = aa < bb ? aa : bb;
+                    if (na == 0 || na > 32) break;
+                    lr += na;
+                    const bool act = (unsigned)lane < na;
+                    unsigned li = 0;
+                    float nl = 0.0f;
+                    bool small = false;
+                    if (act) {
+                        const unsigned si2 = sl[sb + lane];
+                        li = sl[sen + lane];
+                        alias[si2] = li;
+                        nl = (prob[li] + prob[si2]) - 1.0f;
+                        small = nl <= 1.0f;
+                    }
+                    __syncwarp();  // every read of this round's list entries precedes the writes
+                    const unsigned bs = __ballot_sync(kFull, act && small);
+                    const unsigned bl = __ballot_sync(kFull, act && !small);
+                    const unsigned below = (1u << lane) - 1u;
+                    if (act) {
+                        const unsigned dst = small ? sen + (unsigned)__popc(bs & below)
+                                                   : lr - (unsigned)__popc(bl & below);
+                        sl[dst] = li;
+                        prob[li] = nl;
+                    }
+                    sen += (unsigned)__popc(bs);
+                    lr -= (unsigned)__popc(bl);
+                    sb += na;
+                    __syncwarp();
+                }
+                if (lane == 0) {
+                    red[0] = (int)sb;
+                    red[1] = (int)sen;
+                    red[2] = (int)lr;
+                    red[3] = rr;
+                }
+            }
+            __syncthreads();
+            small_begin = (unsigned)red[0];
+            small_end = (unsigned)red[1];
+            large_rend = (unsigned)red[2];
+            round = red[3];
+            __syncthreads();
+            continue;
+        }
+        ++round;
         large_rend += nactive;
         constexpr int R = (M / 2 + 31) / 32 + 1;  // upper bound on items per thread
         unsigned lidx[R];
