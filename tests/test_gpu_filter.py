@@ -40,7 +40,7 @@ def test_phased_equals_split(gpu, res, exch, t):
         assert np.allclose(x["mean"], y["mean"], rtol=1e-12, atol=1e-12)
 
 
-@pytest.mark.parametrize("m,ppt", [(128, 4), (256, 8), (512, 16), (512, 4), (256, 2), (64, 2)])
+@pytest.mark.parametrize("m,ppt", [(128, 4), (256, 8), (512, 16), (512, 4), (256, 4), (256, 2), (64, 2)])
 @pytest.mark.parametrize("res", [0, 1, 2])
 @pytest.mark.parametrize("exch,t", [(0, 0), (1, 3), (2, 2), (3, 4)])
 def test_fused_equals_split(gpu, m, ppt, res, exch, t):
