@@ -309,6 +309,7 @@ def main():
     ap.add_argument("--resampler", default="systematic", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--phase-steps", type=int, default=100, help="steps of the per-kernel timing pass")
     ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
     ap.add_argument("--workload", default="plain", choices=["plain", "arm", "batched", "served"])
@@ -368,10 +369,9 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     d_in = torch.from_numpy(inputs[:total_steps].view(np.uint8).copy()).cuda()
     d_est = torch.zeros(total_steps * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
-    f.set_timing(True)
     torch.cuda.synchronize()
 
-    # warm-up: builds the graph and runs W steps
+    # warm-up: builds the graph and runs W steps (no per-launch events in the timed graph)
     f.run_device(d_in.data_ptr(), d_est.data_ptr(), total_steps, args.warmup)
     f.synchronize()
 
@@ -390,8 +390,6 @@ def main():
         ev1.record(stream)
         ev1.synchronize()
         step_ms.append(ev0.elapsed_time(ev1))
-        for name, ms in f.last_step_timing():
-            phase_ms.setdefault(name, []).append(ms)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -403,6 +401,19 @@ def main():
         total_ms = float(t.item())
     est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE)
     value = world * particles * args.steps / (total_ms * 1e-3)
+
+    # per-kernel times: a separate pass with an event recorded around every
+    # launch (event nodes in the graph), same L2 flush before each step
+    f.set_timing(True)
+    f.run_device(d_in.data_ptr(), d_est.data_ptr(), total_steps, 1)
+    f.synchronize()
+    for k in range(args.phase_steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        f.run_continue(1)
+        for name, ms in f.last_step_timing():
+            phase_ms.setdefault(name, []).append(ms)
+    f.set_timing(False)
 
     # end to end through pf_step(): host input -> H2D, kernels, D2H of the estimate, per step
     e2e_ms = []
@@ -467,6 +478,8 @@ def main():
                     "d2h_bytes_per_step": int(E.ESTIMATE_DTYPE.itemsize),
                     "ms_per_step": e2e_total / args.e2e_steps if args.e2e_steps > 0 else None},
             "gpu_launches": int(args.steps * len(phases)),
+            "timing": "value: CUDA events around each step's graph launch (no events inside); kernel times: "
+                      "a separate %d-step pass with events between the launches" % args.phase_steps,
             "clocks": clocks,
             "rmse": {"value": rmse, "of": "joint angles (rad)" if W["angles"] else "x, y position (m)"},
         }

@@ -159,8 +159,10 @@ static void srv_release(pf_server* s)
     for (auto& sl : s->slots)
         if (sl.mem) cudaFreeAsync(sl.mem, s->stream);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* dev[] = {s->d_desc, s->d_slot_in, s->d_est_tab, s->d_map[0], s->d_map[1], s->d_map[2],
-                   s->d_pend, s->d_in, s->d_out};
+    for (int m = 0; m < 3; ++m)
+        if (s->d_map[m]) cudaFreeAsync(s->d_map[m], s->stream);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    void* dev[] = {s->d_desc, s->d_slot_in, s->d_est_tab, s->d_pend, s->d_in, s->d_out};
     for (void* p : dev)
         if (p) cudaFree(p);
     void* host[] = {s->h_pend, s->h_in, s->h_out};
@@ -170,6 +172,8 @@ static void srv_release(pf_server* s)
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
+
+static pf_status ensure_map(pf_server* s, int64_t need);
 
 extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, int32_t max_filters,
                                       pf_server** out)
@@ -233,6 +237,13 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     STRY(cudaMallocHost(&s->h_in, sizeof(pf_step_input) * max_filters));
     STRY(cudaMallocHost(&s->h_out, sizeof(pf_estimate) * max_filters));
 #undef STRY
+    {
+        const pf_status ms = ensure_map(s, 1 << 20);  // 8 MB per model: a few growths at most afterwards
+        if (ms != PF_OK) {
+            srv_release(s);
+            return ms;
+        }
+    }
     // Warm-up: reserve pool memory up front (growing the pool later stalls the
     // stream) and run one update of each served model, so that loading the
     // kernels does not land on the first requests.
@@ -285,15 +296,17 @@ extern "C" pf_status pf_server_destroy(pf_server* s)
 }
 
 // CTA-map capacity: every open filter's sub-filters fit in each model's map.
+// The maps come from the stream-ordered pool: a grown map replaces the old one
+// in stream order (the batches already queued keep reading the old one), so
+// admission never waits for the GPU.
 static pf_status ensure_map(pf_server* s, int64_t need)
 {
     if (need <= s->map_cap) return PF_OK;
-    int64_t cap = std::max<int64_t>(need, 2 * s->map_cap);
-    CU(cudaStreamSynchronize(s->stream));  // the old maps may be in use
+    const int64_t cap = std::max<int64_t>(need, 4 * s->map_cap);
     for (int m = 0; m < 3; ++m) {
-        if (s->d_map[m]) CU(cudaFree(s->d_map[m]));
+        if (s->d_map[m]) CU(cudaFreeAsync(s->d_map[m], s->stream));
         s->d_map[m] = nullptr;
-        CU(cudaMalloc(&s->d_map[m], sizeof(int2) * cap));
+        CU(cudaMallocAsync(reinterpret_cast<void**>(&s->d_map[m]), sizeof(int2) * cap, s->pool, s->stream));
     }
     s->map_cap = cap;
     return PF_OK;
