@@ -403,7 +403,10 @@ def main():
     value = world * particles * args.steps / (total_ms * 1e-3)
 
     # per-kernel times: a separate pass with an event recorded around every
-    # launch (event nodes in the graph), same L2 flush before each step
+    # launch (event nodes in the graph), same L2 flush before each step; the
+    # pass replays the trace from its start, so the particles restart from the
+    # initial state (the Vose build's cost depends on the weights)
+    f.set_initial_state(np.array(p.init_state[:E.model_info(W["model"])[0]], np.float32))
     f.set_timing(True)
     f.run_device(d_in.data_ptr(), d_est.data_ptr(), total_steps, 1)
     f.synchronize()

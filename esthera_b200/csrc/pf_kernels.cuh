@@ -569,20 +569,28 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
             bi = oi;
         }
     }
-    double acc[NVMAX];
+    // sums of the group partials, four values at a time (few live registers);
+    // each value keeps the order of the one-pass version: lanes over groups,
+    // then the xor-shuffle tree
+    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
+    for (int j0 = 1; j0 < NV; j0 += 4) {
+        double a4[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int q = lane; q < ng; q += 32) {
+            const double* gq = D.gpart + (int64_t)q * kPartStride;
+            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
 #pragma unroll
-    for (int j = 0; j < NVMAX; ++j) acc[j] = 0.0;
-    for (int q = lane; q < ng; q += 32) {
-        const double* gq = D.gpart + (int64_t)q * kPartStride;
-        const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
+            for (int c = 0; c < 4; ++c)
+                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
+        }
 #pragma unroll
-        for (int j = 1; j < NVMAX; ++j)
-            if (j < NV) acc[j] += sq * __ldcg(gq + j);
+        for (int c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
+            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
+        }
     }
-#pragma unroll
-    for (int j = 1; j < NVMAX; ++j)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(kFull, acc[j], o);
+    __syncwarp();
+    const double* acc = s_acc;
     if (lane == 0) {
         const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
         const double lg = D.log_weights ? gm : 0.0;
@@ -629,6 +637,31 @@ constexpr size_t k2_smem()
     return s;
 }
 
+// E consecutive floats global -> shared without passing through registers
+// (cp.async; both addresses aligned to 4E bytes).  cp_async_wait() waits for
+// this thread's copies.
+template <int E>
+__device__ __forceinline__ void cp_async_floats(float* dst, const float* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (E % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < E; q += 4)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d + 4 * q), "l"(src + q) : "memory");
+    } else if constexpr (E == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    } else {
+#pragma unroll
+        for (int q = 0; q < E; ++q)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d + 4 * q), "l"(src + q) : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // Resampling of sub-filter b from a sorted copy (src_tmp, src_key: this
 // filter's arrays, sorted per sub-filter) with the exchange applied virtually
 // (nx weakest slots take the neighbours' top-t, read from the same sorted
@@ -668,32 +701,56 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
             ur[2 * e + 1] = D.rng_fused ? U[2 + 2 * i] : U[2 * ((int64_t)b * M + i) + 1];
         }
     }
-    float okey[E], ost[S][E];
-    ldv<E>(src_key + base, okey);
-#pragma unroll
-    for (int v = 0; v < S; ++v) ldv<E>(src_tmp + v * T + base, ost[v]);
-    if (E * tid + E - 1 >= M - nx) {
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int x = M - 1 - (E * tid + e);
-            if (x < nx) {
-                const int64_t g = exchange_source(D, b, x);
-                okey[e] = src_key[g];
-#pragma unroll
-                for (int v = 0; v < S; ++v) ost[v][e] = src_tmp[v * T + g];
-            }
-        }
-    }
-    if (dec_u - 1.0f > D.freq) return false;
     float* kb = reinterpret_cast<float*>(smem);
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
+    const bool xch = E * tid + E - 1 >= M - nx;  // this thread owns slots in the exchange range
+    if constexpr (S <= 3) {
+        // small states: through registers
+        float okey[E], ost[S][E];
+        ldv<E>(src_key + base, okey);
 #pragma unroll
-    for (int e = 0; e < E; ++e) kb[E * tid + e] = okey[e];
+        for (int v = 0; v < S; ++v) ldv<E>(src_tmp + v * T + base, ost[v]);
+        if (xch) {
 #pragma unroll
-    for (int v = 0; v < S; ++v)
+            for (int e = 0; e < E; ++e) {
+                const int x = M - 1 - (E * tid + e);
+                if (x < nx) {
+                    const int64_t g = exchange_source(D, b, x);
+                    okey[e] = src_key[g];
 #pragma unroll
-        for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = ost[v][e];
+                    for (int v = 0; v < S; ++v) ost[v][e] = src_tmp[v * T + g];
+                }
+            }
+        }
+        if (dec_u - 1.0f > D.freq) return false;
+#pragma unroll
+        for (int e = 0; e < E; ++e) kb[E * tid + e] = okey[e];
+#pragma unroll
+        for (int v = 0; v < S; ++v)
+#pragma unroll
+            for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = ost[v][e];
+    } else {
+        // large states: straight into shared memory (cp.async), the
+        // exchanged slots overwritten by their owner once its copies landed
+        cp_async_floats<E>(kb + E * tid, src_key + base);
+#pragma unroll
+        for (int v = 0; v < S; ++v) cp_async_floats<E>(tile + v * M + E * tid, src_tmp + v * T + base);
+        cp_async_wait();
+        if (dec_u - 1.0f > D.freq) return false;
+        if (xch) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int x = M - 1 - (E * tid + e);
+                if (x < nx) {
+                    const int64_t g = exchange_source(D, b, x);
+                    kb[E * tid + e] = src_key[g];
+#pragma unroll
+                    for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = src_tmp[v * T + g];
+                }
+            }
+        }
+    }
     __syncthreads();
     float w[E];
 #pragma unroll

@@ -100,20 +100,28 @@ __device__ __forceinline__ void estimate_last_done(const FilterDesc& D, const St
             bi = oi;
         }
     }
-    double acc[NVMAX];
+    // sums of the group partials, four values at a time (few live registers);
+    // each value keeps the order of the one-pass version: lanes over groups,
+    // then the xor-shuffle tree
+    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
+    for (int j0 = 1; j0 < NV; j0 += 4) {
+        double a4[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int q = lane; q < ng; q += 32) {
+            const double* gq = D.gpart + (int64_t)q * kPartStride;
+            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
 #pragma unroll
-    for (int j = 0; j < NVMAX; ++j) acc[j] = 0.0;
-    for (int q = lane; q < ng; q += 32) {
-        const double* gq = D.gpart + (int64_t)q * kPartStride;
-        const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
+            for (int c = 0; c < 4; ++c)
+                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
+        }
 #pragma unroll
-        for (int j = 1; j < NVMAX; ++j)
-            if (j < NV) acc[j] += sq * __ldcg(gq + j);
+        for (int c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
+            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
+        }
     }
-#pragma unroll
-    for (int j = 1; j < NVMAX; ++j)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(kFull, acc[j], o);
+    __syncwarp();
+    const double* acc = s_acc;
     if (lane == 0) {
         const int best = (bi >= 0 && bi < D.N) ? bi : 0;
         const double lg = D.log_weights ? gm : 0.0;
