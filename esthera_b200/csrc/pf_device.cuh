@@ -117,6 +117,67 @@ __device__ __forceinline__ void box_muller(float x, float y, float& z1, float& z
     z2 = -r * s;
 }
 
+// mtgp_generate for float output with the first nbm words (nbm even) turned
+// into normals by Box-Muller on the fly: each thread produces the adjacent
+// words (k, k+1) of a round, so the pair's recursion inputs come in 64-bit
+// shared loads and the normals go out as one 64-bit store to nz[k], nz[k+1]
+// (the same values as mtgp_generate followed by box_muller on nz[2q], nz[2q+1]).
+// Words k >= nbm (k < n) go to emit(k, word).  Ends with a barrier.
+template <class Emit>
+__device__ __forceinline__ void mtgp_generate_bm(MtgpSmem& s, int n, int nbm, float* __restrict__ nz, Emit emit)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t pos = s.pos, sh1 = s.sh1, sh2 = s.sh2, mask = s.mask;
+    const uint32_t* ring = s.ring;
+    auto ld2 = [&](int i) { return *reinterpret_cast<const uint2*>(ring + (i & 1023)); };  // i even
+    for (int base = 0; base < n; base += kMtgpLanes) {
+        for (int l2 = tid; l2 < kMtgpLanes / 2; l2 += nt) {
+            const int k = base + 2 * l2;  // even
+            const uint2 x01 = ld2(k), x23 = ld2(k + 2);
+            uint32_t t0, y0, y1;
+            if ((pos & 1u) == 0) {
+                const uint2 yy = ld2(k + (int)pos);
+                y0 = yy.x;
+                y1 = yy.y;
+                t0 = ld2(k + (int)pos - 2).y;
+            } else {
+                const uint2 ty = ld2(k + (int)pos - 1), y2 = ld2(k + (int)pos + 1);
+                t0 = ty.x;
+                y0 = ty.y;
+                y1 = y2.x;
+            }
+            const uint32_t t1 = y0;
+            uint32_t xa = (x01.x & mask) ^ x01.y;
+            xa ^= xa << sh1;
+            uint32_t ya = xa ^ (y0 >> sh2);
+            const uint32_t r0 = ya ^ s.tbl[ya & 0x0f];
+            uint32_t xb = (x01.y & mask) ^ x23.x;
+            xb ^= xb << sh1;
+            uint32_t yb = xb ^ (y1 >> sh2);
+            const uint32_t r1 = yb ^ s.tbl[yb & 0x0f];
+            s.ring[(k + kMtgpN) & 1023] = r0;
+            s.ring[(k + kMtgpN + 1) & 1023] = r1;
+            uint32_t ta = t0;
+            ta ^= ta >> 16;
+            ta ^= ta >> 8;
+            uint32_t tb = t1;
+            tb ^= tb >> 16;
+            tb ^= tb >> 8;
+            const uint32_t o0 = (r0 >> 9) ^ s.ttb[ta & 0x0f];
+            const uint32_t o1 = (r1 >> 9) ^ s.ttb[tb & 0x0f];
+            if (k < nbm) {
+                float z1, z2;
+                box_muller(__uint_as_float(o0), __uint_as_float(o1), z1, z2);
+                *reinterpret_cast<float2*>(nz + k) = make_float2(z1, z2);
+            } else {
+                if (k < n) emit(k, o0);
+                if (k + 1 < n) emit(k + 1, o1);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // atan2 from an odd polynomial for atan on [0, 1] -- degree 15 in a, i.e. 8
 // coefficients in a^2, fitted for this project by least squares on 4000
 // Chebyshev nodes refined with Lawson iterations towards the minimax fit

@@ -264,17 +264,8 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         mtgp_load(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, true);
         const int nbm = D.nbm;
         float* ru = D.ru + (int64_t)b * D.ru_stride;
-        mtgp_generate(*ms, D.draws, true, [&](int k, uint32_t o) {
-            if (k < nbm) nz[k] = __uint_as_float(o);
-            else ru[k - nbm] = __uint_as_float(o);
-        });
+        mtgp_generate_bm(*ms, D.draws, nbm, nz, [&](int k, uint32_t o) { ru[k - nbm] = __uint_as_float(o); });
         mtgp_store(*ms, gst, D.draws);
-        for (int q = tid; q < nbm / 2; q += NT) {
-            float z1, z2;
-            box_muller(nz[2 * q], nz[2 * q + 1], z1, z2);
-            nz[2 * q] = z1;
-            nz[2 * q + 1] = z2;
-        }
     }
     __syncthreads();
 
