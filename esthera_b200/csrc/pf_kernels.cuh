@@ -168,57 +168,54 @@ constexpr size_t k1_smem()
     return s;
 }
 
-// FP64 block sum of NV values per thread into out[0..NV) (thread 0 writes).
-template <int NV>
-__device__ __forceinline__ void block_sum_f64(double (&a)[NV], double* red, double* out)
-{
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int i = 0; i < NV; ++i)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_xor_sync(kFull, a[i], o);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-        for (int i = 0; i < NV; ++i) red[wp * NV + i] = a[i];
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        double s = red[threadIdx.x];
-        for (int w = 1; w < nw; ++w) s += red[w * NV + threadIdx.x];
-        out[threadIdx.x] = s;
-    }
-}
-
 // Estimate partials of one sub-filter from particles in any order:
 // [0] key max, [1] sum w, [2+v] sum w x_v (angles: sum w sin), [2+S+a] sum w cos.
+// One value at a time (few live registers): each thread sums its E particles
+// in order, lanes combine with the xor-shuffle tree, warps in index order.
+// sin/cos of the angular variables are taken from the (already propagated)
+// state, the values the model returned for them.
 template <class Mdl, int E>
 __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float lmax,
-                                               const float (&okey)[E], const float (&st)[E][Mdl::S],
-                                               const float (&sn)[E][Mdl::NA], const float (&cs)[E][Mdl::NA],
-                                               double* red)
+                                               const float (&okey)[E], const float (&st)[E][Mdl::S], double* red)
 {
     constexpr int S = Mdl::S, NA = Mdl::NA, NV = 1 + S + NA;
-    double acc[NV];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double w[E];
 #pragma unroll
-    for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+    for (int e = 0; e < E; ++e) w[e] = D.log_weights ? (double)__expf(okey[e] - lmax) : (double)okey[e];
+    __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const double w = D.log_weights ? (double)__expf(okey[e] - lmax) : (double)okey[e];
-        acc[0] += w;
-        int a = 0;
+    for (int i = 0; i < NV; ++i) {
+        double a = 0.0;
 #pragma unroll
-        for (int v = 0; v < S; ++v) {
-            if (is_angle_var<Mdl>(v)) {
-                acc[1 + v] += w * (double)sn[e][a];
-                acc[1 + S + a] += w * (double)cs[e][a];
-                ++a;
+        for (int e = 0; e < E; ++e) {
+            if (i == 0) {
+                a += w[e];
+            } else if (i <= S) {
+                const int v = i - 1;
+                float x = st[e][v];
+                if (is_angle_var<Mdl>(v)) {
+                    float c;
+                    __sincosf(st[e][v], &x, &c);
+                }
+                a += w[e] * (double)x;
             } else {
-                acc[1 + v] += w * (double)st[e][v];
+                float sn, cs;
+                __sincosf(st[e][Mdl::angle_var(i - 1 - S)], &sn, &cs);
+                a += w[e] * (double)cs;
             }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
+        if (lane == 0) red[wp * NV + i] = a;
     }
+    __syncthreads();
     double* out = D.part + (int64_t)b * kPartStride;
-    block_sum_f64<NV>(acc, red, out + 1);
+    if (threadIdx.x < NV) {
+        double sum = red[threadIdx.x];
+        for (int q = 1; q < nw; ++q) sum += red[q * NV + threadIdx.x];
+        out[1 + threadIdx.x] = sum;
+    }
     if (threadIdx.x == 0) out[0] = (double)lmax;
 }
 
@@ -321,7 +318,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(D.tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs, red);
+    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
 }
 
 // ---------------------------------------------------------------------------
@@ -427,7 +424,7 @@ __global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restri
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(D.tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs, red);
+    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
 }
 
 // ---------------------------------------------------------------------------

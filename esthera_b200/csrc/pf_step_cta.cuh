@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(cur_tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs, red);
+    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
 
     // ---- E (warp 0 wrote the partials)
     if (tid < 32) estimate_last_done<S>(D, X, b, in, step_ctr, tid);
