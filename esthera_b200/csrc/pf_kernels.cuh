@@ -487,6 +487,80 @@ __global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const i
 // starts); the last group to finish (atomic ticket) combines the groups in
 // index order and writes the estimate.  Deterministic for a given N.
 // ---------------------------------------------------------------------------
+// The global estimate from the group partials gpart[0..ng) (one warp, after
+// the global maximum gm and the winner (bk, bi) are known): the FP64 sums of
+// the NV values, then the fields written by different lanes at once -- lane v
+// the mean (or circular mean) of variable v, lane 16 + v the winner's
+// variable v from best_src, lane 0 the rest.  Each sum keeps one order: a
+// lane's groups ascending, then the xor-shuffle tree.
+template <int S>
+__device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, int ng, int NV, double gm, float bk,
+                                               int bi, const float* __restrict__ best_src, pf_estimate& E,
+                                               int32_t step_no)
+{
+    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
+    double sqv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int q = lane + 32 * r;
+        sqv[r] = q < ng ? (D.log_weights ? exp(__ldcg(D.gpart + (int64_t)q * kPartStride) - gm) : 1.0) : 0.0;
+    }
+    for (int j0 = 1; j0 < NV; j0 += 4) {
+        double a4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = lane + 32 * r;
+            if (q < ng) {
+                const double* gq = D.gpart + (int64_t)q * kPartStride;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (j0 + c < NV) a4[c] += sqv[r] * __ldcg(gq + j0 + c);
+            }
+        }
+        for (int q = lane + 128; q < ng; q += 32) {
+            const double* gq = D.gpart + (int64_t)q * kPartStride;
+            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
+            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
+        }
+    }
+    __syncwarp();
+    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
+    const double W = s_acc[1];
+    if (lane < PF_MAX_STATE) {
+        const int v = lane;
+        double m = 0.0;
+        if (v < S) {
+            if ((D.angle_mask >> v) & 1u) {
+                const int a = __popc(D.angle_mask & ((1u << v) - 1u));
+                m = atan2(s_acc[2 + v], s_acc[2 + S + a]);
+            } else {
+                m = s_acc[2 + v] / W;
+            }
+        }
+        E.mean[v] = m;
+    } else {
+        const int v = lane - PF_MAX_STATE;
+        E.best[v] = v < S ? __ldcg(best_src + v * D.T + (int64_t)best * D.M) : 0.0f;
+    }
+    if (lane == 0) {
+        const double lg = D.log_weights ? gm : 0.0;
+        E.log_norm = lg + log(W);
+        E.best_key = bk;
+        E.best_subfilter = best;
+        E.step = step_no;
+        E.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
+    }
+    __syncwarp();
+}
+
 template <int S>
 __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, const InputRef& in, int32_t* step_ctr)
 {
@@ -557,51 +631,8 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
             bi = oi;
         }
     }
-    // sums of the group partials, four values at a time (few live registers);
-    // each value keeps the order of the one-pass version: lanes over groups,
-    // then the xor-shuffle tree
-    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
-    for (int j0 = 1; j0 < NV; j0 += 4) {
-        double a4[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int q = lane; q < ng; q += 32) {
-            const double* gq = D.gpart + (int64_t)q * kPartStride;
-            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
-            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
-        }
-    }
-    __syncwarp();
-    const double* acc = s_acc;
+    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, D.tmp, D.est[step_index(in)], in.ctr ? *in.ctr + 1 : 0);
     if (lane == 0) {
-        const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
-        const double lg = D.log_weights ? gm : 0.0;
-        const int64_t idx = step_index(in);
-        pf_estimate& E = D.est[idx];
-        const double W = acc[1];
-        int a = 0;
-        for (int v = 0; v < PF_MAX_STATE; ++v) E.mean[v] = 0.0;
-#pragma unroll
-        for (int v = 0; v < S; ++v) {
-            if ((D.angle_mask >> v) & 1u) {
-                E.mean[v] = atan2(acc[2 + v], acc[2 + S + a]);
-                ++a;
-            } else {
-                E.mean[v] = acc[2 + v] / W;
-            }
-        }
-        E.log_norm = lg + log(W);
-        for (int v = 0; v < PF_MAX_STATE; ++v) E.best[v] = v < S ? D.tmp[v * D.T + (int64_t)best * D.M] : 0.0f;
-        E.best_key = bk;
-        E.best_subfilter = best;
-        E.step = in.ctr ? *in.ctr + 1 : 0;
-        E.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
         *D.est_ctr = 0;
         __threadfence();
         if (step_ctr) *step_ctr += 1;

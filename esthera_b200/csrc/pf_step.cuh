@@ -100,54 +100,10 @@ __device__ __forceinline__ void estimate_last_done(const FilterDesc& D, const St
             bi = oi;
         }
     }
-    // sums of the group partials, four values at a time (few live registers);
-    // each value keeps the order of the one-pass version: lanes over groups,
-    // then the xor-shuffle tree
-    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
-    for (int j0 = 1; j0 < NV; j0 += 4) {
-        double a4[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int q = lane; q < ng; q += 32) {
-            const double* gq = D.gpart + (int64_t)q * kPartStride;
-            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
-            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
-        }
-    }
-    __syncwarp();
-    const double* acc = s_acc;
+    const int par = (*X.steps) & 1;
+    const float* cur_tmp = par ? X.tmp2 : D.tmp;
+    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, cur_tmp, D.est[step_index(in)], in.ctr ? *in.ctr + 1 : 0);
     if (lane == 0) {
-        const int best = (bi >= 0 && bi < D.N) ? bi : 0;
-        const double lg = D.log_weights ? gm : 0.0;
-        const int64_t idx = step_index(in);
-        pf_estimate& Eo = D.est[idx];
-        const double W = acc[1];
-        const int par = (*X.steps) & 1;
-        const float* cur_tmp = par ? X.tmp2 : D.tmp;
-        int a = 0;
-        for (int v = 0; v < PF_MAX_STATE; ++v) Eo.mean[v] = 0.0;
-#pragma unroll
-        for (int v = 0; v < S; ++v) {
-            if ((D.angle_mask >> v) & 1u) {
-                Eo.mean[v] = atan2(acc[2 + v], acc[2 + S + a]);
-                ++a;
-            } else {
-                Eo.mean[v] = acc[2 + v] / W;
-            }
-        }
-        Eo.log_norm = lg + log(W);
-        for (int v = 0; v < PF_MAX_STATE; ++v)
-            Eo.best[v] = v < S ? __ldcg(cur_tmp + v * D.T + (int64_t)best * D.M) : 0.0f;
-        Eo.best_key = bk;
-        Eo.best_subfilter = best;
-        Eo.step = in.ctr ? *in.ctr + 1 : 0;
-        Eo.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
         *D.est_ctr = 0;
         *X.need_init = 0;
         __threadfence();
