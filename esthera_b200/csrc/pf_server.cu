@@ -7,11 +7,13 @@
 // pf_server_launch takes the oldest queued update of every filter that has
 // none in flight and runs all of them as one batch: one host->device copy of
 // the compact (slot, input) list, an expand kernel writing the CTA ->
-// (slot, sub-filter) maps, the split pipeline's two kernels per model, and a
+// (slot, sub-filter) maps, the split pipeline's two kernels per model (each
+// model on its own stream, forked from the server's stream after the copies
+// and joined back before the gather, so the models' grids overlap), and a
 // gather of the batch's estimates copied back in one transfer.  Filters are
-// opened, closed and updated while batches run; all device work of the server
-// is ordered on its one stream, so memory released by a closed filter is
-// reused only after the batches that touched it.
+// opened, closed and updated while batches run; everything else is ordered on
+// the server's stream, so memory released by a closed filter is reused only
+// after the batches that touched it.
 //
 // Filter memory comes from a stream-ordered pool (cudaMallocAsync), one block
 // per filter; admission charges the block's size against the budget.  Each
@@ -130,6 +132,10 @@ struct pf_server {
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
     cudaEvent_t done = nullptr;
+    // each model's kernels run on their own stream, forked from and joined
+    // back into `stream`, so the models' grids of a batch overlap
+    cudaStream_t side[3] = {};
+    cudaEvent_t fork = nullptr, join[3] = {};
     std::vector<Slot> slots;
     std::vector<int> free_slots;
     // device tables
@@ -169,6 +175,11 @@ static void srv_release(pf_server* s)
     for (void* p : host)
         if (p) cudaFreeHost(p);
     if (s->done) cudaEventDestroy(s->done);
+    if (s->fork) cudaEventDestroy(s->fork);
+    for (int m = 0; m < 3; ++m) {
+        if (s->join[m]) cudaEventDestroy(s->join[m]);
+        if (s->side[m]) cudaStreamDestroy(s->side[m]);
+    }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -222,6 +233,11 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     } while (0)
     STRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     STRY(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
+    STRY(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+    for (int m = 0; m < 3; ++m) {
+        STRY(cudaStreamCreateWithFlags(&s->side[m], cudaStreamNonBlocking));
+        STRY(cudaEventCreateWithFlags(&s->join[m], cudaEventDisableTiming));
+    }
     STRY(cudaDeviceGetDefaultMemPool(&s->pool, cfg->device));
     {
         uint64_t keep = UINT64_MAX;  // keep freed blocks in the pool for the next admission
@@ -490,21 +506,30 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     cudaStream_t st = s->stream;
     CU(cudaMemcpyAsync(s->d_pend, s->h_pend, sizeof(Pending) * n, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(s->d_in, s->h_in, sizeof(pf_step_input) * n, cudaMemcpyHostToDevice, st));
-    // one expand launch per model group (each writes its own map)
+    // one expand launch per model group (each writes its own map), each group
+    // on its model's stream after everything queued on `stream` so far
+    CU(cudaEventRecord(s->fork, st));
+    bool used[3] = {false, false, false};
     int first = 0;
     for (int m = 0; m < 3; ++m) {
         int cnt = 0;
         while (first + cnt < n && s->slots[s->h_pend[first + cnt].slot].model == m) ++cnt;
         if (cnt == 0) continue;
-        k_srv_expand<<<cnt, 128, 0, st>>>(s->d_pend + first, s->d_in + first, cnt, s->d_desc, s->d_slot_in,
+        cudaStream_t ms = s->side[m];
+        CU(cudaStreamWaitEvent(ms, s->fork, 0));
+        k_srv_expand<<<cnt, 128, 0, ms>>>(s->d_pend + first, s->d_in + first, cnt, s->d_desc, s->d_slot_in,
                                           s->d_map[m]);
         CU(cudaGetLastError());
         const ModelOps ops = model_ops(m);
         InputRef ir{s->d_slot_in, 1, nullptr, 0, 0};
-        CU(ops.sample_sort(M, E, true, (int)ctas[m], st, s->d_desc, s->d_map[m], ir));
-        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)ctas[m], st, s->d_desc, s->d_map[m], ir, nullptr, 1));
+        CU(ops.sample_sort(M, E, true, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir));
+        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir, nullptr, 1));
+        CU(cudaEventRecord(s->join[m], ms));
+        used[m] = true;
         first += cnt;
     }
+    for (int m = 0; m < 3; ++m)
+        if (used[m]) CU(cudaStreamWaitEvent(st, s->join[m], 0));
     k_srv_gather<<<n, 64, 0, st>>>(s->d_pend, n, s->d_est_tab, s->d_out);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(pf_estimate) * n, cudaMemcpyDeviceToHost, st));
