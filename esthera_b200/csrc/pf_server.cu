@@ -116,6 +116,7 @@ struct Slot {
     size_t bytes = 0;
     char* mem = nullptr;
     bool in_flight = false;
+    bool in_ready = false;  // listed in its model's ready list
     int32_t steps = 0;
     std::deque<std::pair<pf_step_input, uint64_t>> queue;  // (input, caller tag)
 };
@@ -138,6 +139,10 @@ struct pf_server {
     cudaEvent_t fork = nullptr, join[3] = {};
     std::vector<Slot> slots;
     std::vector<int> free_slots;
+    // slots with a queued update and none in flight, per model, in the order
+    // they became ready (entries of closed slots are dropped at the launch)
+    std::vector<int> ready[3];
+    int64_t n_open = 0, resident_T = 0, resident_sub = 0, queued = 0;
     // device tables
     FilterDesc* d_desc = nullptr;
     pf_step_input* d_slot_in = nullptr;
@@ -368,10 +373,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
         return fail(PF_ERR_ADMISSION, "filter needs %zu bytes, %lld of %lld in use", L.total, (long long)s->used,
                     (long long)s->budget);
     CU(cudaSetDevice(s->device));
-    int64_t resident = 0;
-    for (auto& sl : s->slots)
-        if (sl.open) resident += sl.N;
-    pf_status st = ensure_map(s, resident + N);
+    pf_status st = ensure_map(s, s->resident_sub + N);
     if (st != PF_OK) return st;
     void* mem = nullptr;
     cudaError_t e = cudaMallocAsync(&mem, L.total, s->pool, s->stream);
@@ -439,9 +441,13 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     sl.bytes = L.total;
     sl.mem = base;
     sl.in_flight = false;
+    sl.in_ready = false;
     sl.steps = 0;
     sl.queue.clear();
     s->used += (int64_t)L.total;
+    s->n_open++;
+    s->resident_T += D.T;
+    s->resident_sub += N;
     *id = slot;
     return PF_OK;
 }
@@ -454,6 +460,10 @@ extern "C" pf_status pf_server_close(pf_server* s, int32_t id)
     if (sl.in_flight) return fail(PF_ERR_BUSY, "filter %d has an update in flight (poll first)", id);
     CU(cudaFreeAsync(sl.mem, s->stream));  // stream-ordered: reused only after the work queued before
     s->used -= (int64_t)sl.bytes;
+    s->n_open--;
+    s->resident_T -= sl.T;
+    s->resident_sub -= sl.N;
+    s->queued -= (int64_t)sl.queue.size();
     sl = Slot();
     s->free_slots.push_back(id);
     return PF_OK;
@@ -463,7 +473,13 @@ extern "C" pf_status pf_server_update(pf_server* s, int32_t id, const pf_step_in
 {
     if (!s || !in) return fail(PF_ERR_INVALID, "null argument");
     if (id < 0 || id >= s->max_filters || !s->slots[id].open) return fail(PF_ERR_NOT_FOUND, "no open filter %d", id);
-    s->slots[id].queue.emplace_back(*in, tag);
+    Slot& sl = s->slots[id];
+    sl.queue.emplace_back(*in, tag);
+    s->queued++;
+    if (!sl.in_flight && !sl.in_ready) {
+        s->ready[sl.model].push_back(id);
+        sl.in_ready = true;
+    }
     return PF_OK;
 }
 
@@ -481,19 +497,22 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     for (int m = 0; m < 3; ++m) {
         const int first = n;
         int64_t leads = 0;
-        for (int i = 0; i < s->max_filters; ++i) {
+        for (const int i : s->ready[m]) {
             Slot& sl = s->slots[i];
-            if (!sl.open || sl.model != m || sl.in_flight || sl.queue.empty()) continue;
+            sl.in_ready = false;
+            if (!sl.open || sl.model != m || sl.in_flight || sl.queue.empty()) continue;  // closed since
             s->h_pend[n] = Pending{i, (int32_t)leads, 0};
             s->h_in[n] = sl.queue.front().first;
             s->batch_slots.push_back(i);
             s->batch_tags.push_back(sl.queue.front().second);
             sl.queue.pop_front();
+            s->queued--;
             sl.in_flight = true;
             leads += (sl.N + 31) / 32;
             ctas[m] += sl.N;
             ++n;
         }
+        s->ready[m].clear();
         int64_t rest = leads;  // the other sub-filters follow all of the group's leaders
         for (int q = first; q < n; ++q) {
             s->h_pend[q].first_rest = (int32_t)rest;
@@ -562,6 +581,10 @@ extern "C" pf_status pf_server_poll(pf_server* s, int32_t wait, pf_server_result
         Slot& sl = s->slots[s->batch_slots[i]];
         sl.in_flight = false;
         sl.steps++;
+        if (!sl.queue.empty() && !sl.in_ready) {
+            s->ready[sl.model].push_back(s->batch_slots[i]);
+            sl.in_ready = true;
+        }
         out[i].filter = s->batch_slots[i];
         out[i].step = sl.steps;
         out[i].tag = s->batch_tags[i];
@@ -580,12 +603,9 @@ extern "C" pf_status pf_server_stats_get(pf_server* s, pf_server_stats* st)
 {
     if (!s || !st) return fail(PF_ERR_INVALID, "null argument");
     memset(st, 0, sizeof(*st));
-    for (auto& sl : s->slots)
-        if (sl.open) {
-            st->open_filters++;
-            st->resident_particles += sl.T;
-            st->queued_updates += (int64_t)sl.queue.size();
-        }
+    st->open_filters = (int32_t)s->n_open;
+    st->resident_particles = s->resident_T;
+    st->queued_updates = s->queued;
     st->bytes_in_use = s->used;
     st->budget = s->budget;
     st->launches = s->launches;
