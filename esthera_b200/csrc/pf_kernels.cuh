@@ -1,17 +1,19 @@
 // pf_kernels.cuh -- kernels of the particle-filter step (sm_100a).
 //
-// Fused pipeline (the production path), per step:
-//   k_sample_sort      one CTA per sub-filter: MTGP32 stream -> Box-Muller in
-//                      shared memory -> propagate + log-weight (float2/float4
-//                      SoA loads) -> bitonic sort -> sorted state/keys,
-//                      winner, FP64 estimate partials
-//   k_a2a_merge        (all-to-all exchange only) global top-t of the sorted lists
-//   k_estimate         one CTA per filter: winner + FP64 posterior mean
-//   k_exchange_resample one CTA per sub-filter: neighbours' top-t into the
-//                      weakest slots, weights, resampling, gather, store
+// Split pipeline (two launches per step; batches and the server use it too):
+//   k_sample_sort       one CTA per sub-filter: MTGP32 stream -> Box-Muller in
+//                       shared memory -> propagate + log-weight (float4 SoA
+//                       loads) -> bitonic sort -> sorted state/keys, winner,
+//                       FP64 estimate partials
+//   k_a2a_merge         (all-to-all exchange only) global top-t of the sorted lists
+//   k_exchange_resample one CTA per sub-filter, estimate-combining group
+//                       leaders first: neighbours' top-t into the weakest
+//                       slots, weights, resampling, gather, store
+// Single-kernel pipeline: k_step_cta (pf_step_cta.cuh), the same phases in one
+// launch with the resampling deferred to the next step.
 // Phased pipeline (the reference's kernel sequence, pf_generic_soa.cu:842-1234):
 //   k_mtgp_blocks -> k_boxmuller -> k_sample_weight -> k_block_sort ->
-//   k_estimate -> k_exchange_inplace -> k_exchange_resample (no exchange)
+//   k_exchange_inplace -> k_exchange_resample (estimate combined at its start)
 #pragma once
 
 #include "pf_device.cuh"

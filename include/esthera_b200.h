@@ -69,8 +69,9 @@ typedef enum {
 } pf_rng_layout;
 
 typedef enum {
-    PF_PIPELINE_FUSED = 0,  /* one kernel per step, one warp per sub-filter (m = 128, 256, 512 with
-                               PF_RNG_SUBFILTER; other configurations run PF_PIPELINE_SPLIT) */
+    PF_PIPELINE_FUSED = 0,  /* one kernel per step, one CTA per sub-filter, the resampling deferred to
+                               the next step (needs PF_RNG_SUBFILTER and exchange_period <= 1;
+                               other configurations run PF_PIPELINE_SPLIT) */
     PF_PIPELINE_PHASED = 1, /* one kernel per reference phase */
     PF_PIPELINE_SPLIT = 2   /* sample+weight+sort kernel, then exchange+resample+estimate kernel */
 } pf_pipeline;
