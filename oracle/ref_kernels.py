@@ -1,0 +1,71 @@
+"""Test infrastructure: ctypes bindings of oracle/_ref/libref_kernels.so, the
+reference's own CUDA block_sort / resampling / exchange_ring kernels (built by
+oracle/build_ref_kernels.sh from the Esthera tree).  Needs a GPU; used only by
+tests and the fixture script tests/golden/make_ref_kernel_golden.py."""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libref_kernels.so"
+_lib = None
+
+
+def available():
+    return LIB_PATH.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(str(LIB_PATH))
+        fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int32)
+        L.ref_block_sort.argtypes = [fp, C.c_int, C.c_int, ip]
+        L.ref_resampling.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, ip]
+        L.ref_exchange_ring.argtypes = [fp, C.c_int, C.c_int, C.c_int, ip]
+        for f in (L.ref_block_sort, L.ref_resampling, L.ref_exchange_ring):
+            f.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _i(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError("%s failed (%d)" % (what, rc))
+
+
+def block_sort(keys, m):
+    """(sorted keys, permutation within each sub-filter) of nsub = len/m descending sorts."""
+    k = np.array(keys, np.float32, copy=True)
+    perm = np.zeros(len(k), np.int32)
+    _check(lib().ref_block_sort(_f(k), m, len(k) // m, _i(perm)), "ref_block_sort")
+    return k, perm
+
+
+def resampling(weights, u_particles, m, u_decision=None, freq=1.0):
+    """Multinomial selections (slot within the sub-filter, -1 where skipped).
+    u_particles / u_decision: the MTGP-style uniforms in [1, 2); the reference's
+    cuRAND build takes them minus 1 (exact in FP32)."""
+    w = np.ascontiguousarray(weights, np.float32)
+    nsub = len(w) // m
+    ud = np.ones(nsub, np.float32) if u_decision is None else np.asarray(u_decision, np.float32)
+    r = np.concatenate([np.asarray(u_particles, np.float32) - np.float32(1.0), ud - np.float32(1.0)]).astype(np.float32)
+    sel = np.zeros(len(w), np.int32)
+    _check(lib().ref_resampling(_f(w), _f(r), m, nsub, float(freq), _i(sel)), "ref_resampling")
+    return sel
+
+
+def exchange_ring(keys, m, t):
+    """(keys after the exchange, source slot of every slot)."""
+    k = np.array(keys, np.float32, copy=True)
+    src = np.zeros(len(k), np.int32)
+    _check(lib().ref_exchange_ring(_f(k), m, len(k) // m, t, _i(src)), "ref_exchange_ring")
+    return k, src

@@ -1,0 +1,76 @@
+"""The engine's CUDA sort, multinomial resampling and ring routing -- and the
+CPU oracle -- against the reference's OWN CUDA kernels (block_sort with its
+bitonic network, resampling with prefix_sum + binary_search, exchange_ring from
+pf_generic_soa.cu / bitonic-sort.cu), built from the Esthera tree into
+oracle/_ref/libref_kernels.so by oracle/build_ref_kernels.sh and run on the
+same GPU.  Inputs: seeded random keys with heavy ties, positive weights with
+zeros, MTGP-style uniforms in [1, 2)."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
+import ref_kernels as R  # noqa: E402
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="oracle/_ref/libref_kernels.so not built "
+                                                           "(oracle/build_ref_kernels.sh needs the reference tree)")]
+
+PPT = {32: [1], 64: [2], 128: [2, 4], 256: [2, 4, 8], 512: [2, 4, 16], 1024: [2, 4]}
+
+
+def _uniforms_1_2(rng, n):
+    return (1.0 + rng.integers(0, 1 << 23, n) / float(1 << 23)).astype(np.float32)  # exact in FP32
+
+
+@pytest.mark.parametrize("m", [32, 64, 128, 256, 512, 1024])
+def test_sort_equals_reference_kernel(gpu, O, m):
+    E = gpu
+    rng = np.random.default_rng(100 + m)
+    nsub = 6
+    keys = np.round(rng.standard_normal(nsub * m) * 3).astype(np.float32) / 3  # ties
+    keys[::7] = -np.inf
+    rk, rp = R.block_sort(keys, m)
+    ok, op = O.bitonic_sort(keys, m)
+    assert np.array_equal(rk, ok) and np.array_equal(rp, op)
+    for ppt in PPT[m]:
+        k, p = E.bitonic_sort(keys, m, ppt)
+        assert np.array_equal(k, rk) and np.array_equal(p, rp), ppt
+
+
+@pytest.mark.parametrize("m", [32, 64, 128, 256, 512, 1024])
+def test_multinomial_equals_reference_kernel(gpu, O, m):
+    E = gpu
+    rng = np.random.default_rng(200 + m)
+    nsub = 6
+    w = rng.exponential(1.0, nsub * m).astype(np.float32)
+    w[rng.random(nsub * m) < 0.3] = 0.0
+    u = _uniforms_1_2(rng, nsub * m)
+    ref = R.resampling(w, u, m)
+    assert np.array_equal(O.resample(O.RES_REF, w, u, m, 2), ref)
+    for ppt in PPT[m]:
+        assert np.array_equal(E.resample(E.RESAMPLE_REFERENCE, w, u, m, ppt), ref), ppt
+
+
+def test_multinomial_skip_rule_of_reference_kernel(gpu):
+    """A sub-filter whose decision uniform exceeds resampling_freq is left alone
+    (pf_generic_soa.cu:423-429): -1 here, as the engine records it."""
+    rng = np.random.default_rng(3)
+    m, nsub = 64, 4
+    w = rng.exponential(1.0, nsub * m).astype(np.float32)
+    u = _uniforms_1_2(rng, nsub * m)
+    dec = np.array([1.1, 1.9, 1.5, 1.2], np.float32)
+    sel = R.resampling(w, u, m, dec, freq=0.5).reshape(nsub, m)
+    assert np.all(sel[1] == -1) and np.all(sel[[0, 2, 3]] >= 0)
+
+
+@pytest.mark.parametrize("N,m,t", [(8, 32, 3), (16, 256, 2), (5, 64, 32)])
+def test_ring_routing_equals_reference_kernel(gpu, O, N, m, t):
+    E = gpu
+    keys = -np.sort(-np.random.default_rng(N + m).standard_normal((N, m)).astype(np.float32), axis=1).reshape(-1)
+    rk, rsrc = R.exchange_ring(keys, m, t)
+    assert np.array_equal(E.exchange_sources(E.EXCHANGE_RING, N, m, t), rsrc)
+    assert np.array_equal(O.exchange_sources(O.EXCH_RING, N, m, t), rsrc)
+    assert np.array_equal(rk, keys[rsrc])

@@ -1,5 +1,8 @@
-"""The oracle's sub-filter primitives: committed golden vectors and
+"""The oracle's sub-filter primitives: committed golden vectors (the sort,
+multinomial and ring vectors pinned to the reference's own CUDA kernels) and
 independent pure-Python restatements of the reference loops."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -151,3 +154,19 @@ def test_boxmuller_formula(O):
     r = np.sqrt(-2 * np.log(u1))
     assert np.allclose(z[0::2], r * np.cos(2 * np.pi * u2), atol=1e-6)
     assert np.allclose(z[1::2], r * np.sin(2 * np.pi * u2), atol=1e-6)
+
+
+@pytest.mark.parametrize("m", [32, 64, 256, 512])
+def test_golden_pinned_to_reference_kernels(golden, m):
+    """The committed sort / multinomial golden vectors equal what the
+    reference's own CUDA kernels (block_sort, resampling) produced on the same
+    inputs (tests/golden/make_ref_kernel_golden.py, run on a GPU)."""
+    ref = np.load(Path(__file__).resolve().parent / "golden" / "ref_kernels.npz")
+    assert np.array_equal(golden["sort_key_%d" % m], ref["sort_key_%d" % m])
+    assert np.array_equal(golden["sort_idx_%d" % m], ref["sort_idx_%d" % m])
+    assert np.array_equal(golden["res_ref_%d" % m], ref["res_ref_%d" % m])
+
+
+def test_ring_golden_pinned_to_reference_kernel(golden):
+    ref = np.load(Path(__file__).resolve().parent / "golden" / "ref_kernels.npz")
+    assert np.array_equal(golden["exch_src_1_8_32_3"], ref["exch_src_1_8_32_3"])
