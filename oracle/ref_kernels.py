@@ -23,7 +23,8 @@ def lib():
         L.ref_block_sort.argtypes = [fp, C.c_int, C.c_int, ip]
         L.ref_resampling.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, ip]
         L.ref_exchange_ring.argtypes = [fp, C.c_int, C.c_int, C.c_int, ip]
-        for f in (L.ref_block_sort, L.ref_resampling, L.ref_exchange_ring):
+        L.ref_sampling_importance.argtypes = [fp, fp, fp, fp, C.c_float, C.c_int, fp]
+        for f in (L.ref_block_sort, L.ref_resampling, L.ref_exchange_ring, L.ref_sampling_importance):
             f.restype = C.c_int
         _lib = L
     return _lib
@@ -69,3 +70,16 @@ def exchange_ring(keys, m, t):
     src = np.zeros(len(k), np.int32)
     _check(lib().ref_exchange_ring(_f(k), m, len(k) // m, t, _i(src)), "ref_exchange_ring")
     return k, src
+
+
+def sampling_importance(state, normals, control, meas, dt):
+    """The reference's robot-arm propagate + weight: (new state [9][n], linear weights [n])."""
+    st = np.array(state, np.float32, copy=True)
+    nz = np.ascontiguousarray(normals, np.float32)
+    ctl = np.zeros(7, np.float32)
+    ctl[:5] = np.asarray(control, np.float32)[:5]
+    z = np.ascontiguousarray(meas, np.float32)[:7].copy()
+    w = np.zeros(st.shape[1], np.float32)
+    _check(lib().ref_sampling_importance(_f(st), _f(nz), _f(ctl), _f(z), float(dt), st.shape[1], _f(w)),
+           "ref_sampling_importance")
+    return st, w

@@ -1,9 +1,10 @@
 // ref_kernels_harness.cu -- test infrastructure only: a C-ABI around the
-// reference's OWN CUDA kernels for the sort, the multinomial resampling and the
-// ring exchange (block_sort, resampling, exchange_ring with its bitonic_sort,
-// prefix_sum and binary_search: src/partfilt/cuda/pf_generic_soa.cu:169-240,
-// 289-323, 400-453 and bitonic-sort.cu:11-61, robot-arm model types from
-// src/models/robotarm/cuda/pf_model_soa.cuh:33-110), so that the engine's
+// reference's OWN CUDA kernels for the sort, the multinomial resampling, the
+// ring exchange and the robot-arm propagate + weight (block_sort, resampling,
+// exchange_ring with its bitonic_sort, prefix_sum and binary_search,
+// sampling_importance: src/partfilt/cuda/pf_generic_soa.cu:169-323, 400-453 and
+// bitonic-sort.cu:11-61; the robot-arm model's types and sampling_iw,
+// src/models/robotarm/cuda/pf_model_soa.cuh:33-184), so that the engine's
 // kernels and the CPU oracle can be checked against the reference itself on a
 // GPU.  Built by oracle/build_ref_kernels.sh straight from the reference tree
 // (its main() renamed) into oracle/_ref/; the reference sources are not copied.
@@ -121,5 +122,36 @@ extern "C" int ref_exchange_ring(float* keys, int m, int nsub, int t, int32_t* s
     exchange_ring<<<nsub, t>>>(data.d, (float*)w.p, m, nsub);
     if (cudaDeviceSynchronize() != cudaSuccess) return 3;
     if (cudaMemcpy(keys, w.p, (size_t)T * 4, cudaMemcpyDeviceToHost) != cudaSuccess || !data.read_x(src)) return 2;
+    return 0;
+}
+
+// The reference's sampling_importance (robot-arm sampling_iw, pf_model_soa.cuh:
+// 114-184) over n particles: state SoA [9][n] in/out (angles[5], x, y, vX, vY),
+// normals [9][n] (the same variable-major layout), control angle rates [5],
+// measurement (angles[5], x, y); weights[n] receives the linear weights.
+extern "C" int ref_sampling_importance(float* state, const float* normals, const float* control7,
+                                       const float* meas7, float dt, int n, float* weights)
+{
+    if (n < 1 || n % 64) return 1;
+    Soa data;
+    Buf w, r;
+    if (!data.alloc(n)) return 2;
+    if (cudaMalloc(&w.p, (size_t)n * 4) != cudaSuccess || cudaMalloc(&r.p, (size_t)n * 9 * 4) != cudaSuccess) return 2;
+    if (cudaMemcpy(data.base, state, (size_t)n * 9 * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(r.p, normals, (size_t)n * 9 * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return 2;
+    control c;
+    measurement z;
+    for (int i = 0; i < NUM_ANGLES; ++i) {
+        c.angles[i] = control7[i];
+        z.angles[i] = meas7[i];
+    }
+    z.x = meas7[5];
+    z.y = meas7[6];
+    sampling_importance<<<n / 64, 64>>>(data.d, (float*)w.p, c, z, (const float*)r.p, dt);
+    if (cudaDeviceSynchronize() != cudaSuccess) return 3;
+    if (cudaMemcpy(state, data.base, (size_t)n * 9 * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(weights, w.p, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return 2;
     return 0;
 }

@@ -74,3 +74,32 @@ def test_ring_routing_equals_reference_kernel(gpu, O, N, m, t):
     assert np.array_equal(E.exchange_sources(E.EXCHANGE_RING, N, m, t), rsrc)
     assert np.array_equal(O.exchange_sources(O.EXCH_RING, N, m, t), rsrc)
     assert np.array_equal(rk, keys[rsrc])
+
+
+def test_refarm_model_equals_reference_kernel(gpu):
+    """The engine's reference-arm model (propagate + log-likelihood) against the
+    reference's sampling_importance / sampling_iw on the same particles, normals,
+    controls and measurements: states within 2e-5, log-likelihoods within
+    1e-4 relative + 5e-3 absolute (FP32, different operation order)."""
+    E = gpu
+    rng = np.random.default_rng(11)
+    n = 2048
+    p = E.refarm_params(1.0)
+    st = np.zeros((9, n), np.float32)
+    st[:5] = (0.75 * np.pi + 0.3 * rng.standard_normal((5, n))).astype(np.float32)
+    st[5] = (7.0 + rng.standard_normal(n)).astype(np.float32)
+    st[6] = rng.standard_normal(n).astype(np.float32)
+    st[7:] = rng.standard_normal((2, n)).astype(np.float32)
+    nz = rng.standard_normal((9, n)).astype(np.float32)
+    inp = np.zeros(1, E.STEP_INPUT_DTYPE)[0]
+    inp["dt"] = 0.1
+    inp["control"][:5] = rng.uniform(-0.5, 0.5, 5)
+    inp["meas"][:5] = (0.75 * np.pi + 0.2 * rng.standard_normal(5)).astype(np.float32)
+    inp["meas"][5:7] = [7.0, 0.5]
+    so, ll = E.model_step(E.MODEL_REFARM, p, inp, st, nz)
+    sr, w = R.sampling_importance(st, nz, inp["control"], inp["meas"], 0.1)
+    assert np.allclose(so, sr, atol=2e-5, rtol=0)
+    ok = w > 1e-30
+    assert ok.mean() > 0.5
+    lr = np.log(w[ok].astype(np.float64))
+    assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
