@@ -95,7 +95,9 @@ typedef struct {
     uint32_t mtgp_mask;              /* PF_MTGP_MASK_PARAMS or PF_MTGP_MASK_CUDA_REF */
     int32_t log_weights;             /* 1: FP32 max-subtracted log weights; 0: linear FP32 weights */
     int32_t pipeline;                /* pf_pipeline */
-    int32_t particles_per_thread;    /* 0 = pick; 1, 2, 4 (8, 16 for m = 256, 512) */
+    int32_t particles_per_thread;    /* 0 = pick (1 for m = 32, 2 for m = 64, else 4); built pairs
+                                        (m, ppt): (32,1) (64,2) (128,2|4) (256,2|4|8) (512,2|4|16)
+                                        (1024,2|4) */
     int32_t device;                  /* CUDA device ordinal */
     int32_t stream_offset;           /* PF_RNG_SUBFILTER: sub-filter b uses stream offset + b (parameter
                                         set (offset + b) mod 200, seed + offset + b + 1); 0 by default */
