@@ -37,7 +37,7 @@ class PFConfig(C.Structure):
                 ("resampling_freq", C.c_float), ("seed", C.c_uint32), ("rng", C.c_int32),
                 ("mtgp_streams", C.c_int32), ("mtgp_mask", C.c_uint32), ("log_weights", C.c_int32),
                 ("pipeline", C.c_int32), ("particles_per_thread", C.c_int32), ("device", C.c_int32),
-                ("stream_offset", C.c_int32), ("exchange_period", C.c_int32)]
+                ("stream_offset", C.c_int32), ("exchange_period", C.c_int32), ("ess_fraction", C.c_float)]
 
 
 class StepInput(C.Structure):

@@ -246,6 +246,7 @@ extern "C" pf_status pf_config_default(pf_config* c)
     c->device = 0;
     c->stream_offset = 0;
     c->exchange_period = 1;
+    c->ess_fraction = 0.0f;
     return PF_OK;
 }
 
@@ -291,6 +292,8 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
         return fail(PF_ERR_INVALID, "unknown resampler %d", c->resampler);
     if (!(c->resampling_freq >= 0.0f && c->resampling_freq <= 1.0f))
         return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
+    if (!(c->ess_fraction >= 0.0f && c->ess_fraction <= 1.0f))
+        return fail(PF_ERR_INVALID, "ess_fraction must be in [0, 1]");
     if (c->rng != PF_RNG_SUBFILTER && c->rng != PF_RNG_REFLAYOUT) return fail(PF_ERR_INVALID, "unknown rng layout");
     if (c->stream_offset < 0) return fail(PF_ERR_INVALID, "stream_offset must be >= 0");
     if (c->exchange_period < 0) return fail(PF_ERR_INVALID, "exchange_period must be >= 0");
@@ -334,7 +337,7 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.dx = f->dx;
     D.dy = f->dy;
     D.log_weights = f->cfg.log_weights ? 1 : 0;
-    D.inplace = (f->cfg.resampling_freq < 1.0f || f->pipe == PF_PIPELINE_PHASED) ? 1 : 0;
+    D.inplace = (f->cfg.resampling_freq < 1.0f || f->cfg.ess_fraction > 0.0f || f->pipe == PF_PIPELINE_PHASED) ? 1 : 0;
     D.rng_fused = f->cfg.rng == PF_RNG_SUBFILTER ? 1 : 0;
     D.draws = (int32_t)f->draws;
     D.nbm = (int32_t)f->nbm;
@@ -343,6 +346,7 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.stream_base = f->cfg.stream_offset;
     D.exch_period = f->cfg.exchange_period;
     D.freq = f->cfg.resampling_freq;
+    D.ess_frac = f->cfg.ess_fraction;
     D.nnorm = (int64_t)f->mi.K * f->T;
     D.est_ctr = f->est_ctr;
     D.gpart = f->gpart;

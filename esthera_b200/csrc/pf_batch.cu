@@ -138,7 +138,7 @@ static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate
     D.resampler = B->cfg.resampler;
     torus_dims(N, &D.dx, &D.dy);
     D.log_weights = B->cfg.log_weights ? 1 : 0;
-    D.inplace = B->cfg.resampling_freq < 1.0f ? 1 : 0;
+    D.inplace = (B->cfg.resampling_freq < 1.0f || B->cfg.ess_fraction > 0.0f) ? 1 : 0;
     D.rng_fused = 1;
     D.draws = (int32_t)B->draws;
     D.nbm = (int32_t)B->nbm;
@@ -147,6 +147,7 @@ static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate
     D.stream_base = B->cfg.stream_offset + (int32_t)s0;
     D.exch_period = B->cfg.exchange_period;
     D.freq = B->cfg.resampling_freq;
+    D.ess_frac = B->cfg.ess_fraction;
     D.nnorm = (int64_t)B->mi.K * D.T;
     D.est_ctr = B->est_ctr + f;
     D.gpart = B->gpart + (int64_t)B->grp_off[f] * kPartStride;
@@ -209,6 +210,8 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         return fail(PF_ERR_INVALID, "unknown resampler %d", cfg->resampler);
     if (!(cfg->resampling_freq >= 0.0f && cfg->resampling_freq <= 1.0f))
         return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
+    if (!(cfg->ess_fraction >= 0.0f && cfg->ess_fraction <= 1.0f))
+        return fail(PF_ERR_INVALID, "ess_fraction must be in [0, 1]");
     if (cfg->stream_offset < 0 || cfg->exchange_period < 0)
         return fail(PF_ERR_INVALID, "stream_offset and exchange_period must be >= 0");
     int64_t P = 0, NS = 0;

@@ -41,6 +41,7 @@ struct FilterDesc {
     uint32_t mask;
     int32_t stream_base;
     float freq;
+    float ess_frac;    // > 0: a sub-filter resamples only while its ESS < ess_frac * m
     int64_t nnorm;     // normals in rbuf before the uniforms (K*T)
     int32_t* est_ctr;  // ticket counter of the two-level estimate (0 between steps)
     double* gpart;     // ceil(N/32) * kPartStride group partials
@@ -783,6 +784,36 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
         mx = block_max(mx, reinterpret_cast<float*>(ired));
 #pragma unroll
         for (int e = 0; e < E; ++e) w[e] = __expf(w[e] - mx);
+    }
+    if (D.ess_frac > 0.0f) {
+        // effective sample size (sum w)^2 / sum w^2 in FP64; a sub-filter whose
+        // weights are still spread out keeps its propagated particles
+        static_assert(M / E <= 16 * 32, "two 16-warp partial arrays in dred");
+        const int lane = tid & 31, wp = tid >> 5, nw = (M / E + 31) >> 5;
+        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            s1 += (double)w[e];
+            s2 += (double)w[e] * (double)w[e];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_xor_sync(kFull, s1, o);
+            s2 += __shfl_xor_sync(kFull, s2, o);
+        }
+        if (lane == 0) {
+            dred[wp] = s1;
+            dred[16 + wp] = s2;
+        }
+        __syncthreads();
+        double t1 = 0.0, t2 = 0.0;
+        for (int q = 0; q < nw; ++q) {
+            t1 += dred[q];
+            t2 += dred[16 + q];
+        }
+        __syncthreads();
+        // all-zero weights count as uniform (ESS = m): no resampling
+        if (!(t2 > 0.0) || t1 * t1 >= (double)D.ess_frac * (double)M * t2) return false;
     }
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(scratch);

@@ -211,6 +211,8 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
         return fail(PF_ERR_INVALID, "unknown resampler %d", cfg->resampler);
     if (!(cfg->resampling_freq >= 0.0f && cfg->resampling_freq <= 1.0f))
         return fail(PF_ERR_INVALID, "resampling_freq must be in [0, 1]");
+    if (!(cfg->ess_fraction >= 0.0f && cfg->ess_fraction <= 1.0f))
+        return fail(PF_ERR_INVALID, "ess_fraction must be in [0, 1]");
     pf_status st = require_gpu(cfg->device);
     if (st != PF_OK) return st;
     pf_server* s = new pf_server();
@@ -403,7 +405,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     D.resampler = s->cfg.resampler;
     torus_dims(N, &D.dx, &D.dy);
     D.log_weights = s->cfg.log_weights ? 1 : 0;
-    D.inplace = s->cfg.resampling_freq < 1.0f ? 1 : 0;
+    D.inplace = (s->cfg.resampling_freq < 1.0f || s->cfg.ess_fraction > 0.0f) ? 1 : 0;
     D.rng_fused = 1;
     D.draws = (int32_t)s->draws[model];
     D.nbm = (int32_t)s->nbm[model];
@@ -412,6 +414,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     D.stream_base = 0;
     D.exch_period = 1;
     D.freq = s->cfg.resampling_freq;
+    D.ess_frac = s->cfg.ess_fraction;
     D.nnorm = (int64_t)mi.K * D.T;
     D.angle_mask = angle_mask_of(model);
     D.na = angle_count_of(model);

@@ -105,6 +105,11 @@ typedef struct {
                                         s counts pf_step calls since the initial state was set, or the
                                         steps of the current pf_run_device run); single-kernel and
                                         split pipelines only */
+    float ess_fraction;              /* > 0: a sub-filter resamples only while its effective sample
+                                        size (sum w)^2 / sum w^2 (FP64) is below ess_fraction * m,
+                                        otherwise it keeps its propagated particles; 0: always (the
+                                        reference's ADAPTIVE_RESAMPLING test sum p^2 <= thr,
+                                        resampling-valias.cl:273-284, is ess_fraction = 1 / (thr m)) */
 } pf_config;
 
 /* One step's inputs.  control/meas are interpreted by the model:

@@ -36,7 +36,7 @@ class OrcFilter(C.Structure):
                 ("log_weights", C.c_int), ("freq", C.c_float), ("seed", C.c_uint32), ("mask", C.c_uint32),
                 ("T", C.c_int64), ("state", C.POINTER(C.c_float)), ("tmp", C.POINTER(C.c_float)),
                 ("tkey", C.POINTER(C.c_float)), ("mtgp", C.POINTER(C.c_uint32)), ("streams", C.c_int),
-                ("rbuf", C.POINTER(C.c_float)), ("rtotal", C.c_int64)]
+                ("rbuf", C.POINTER(C.c_float)), ("rtotal", C.c_int64), ("ess_frac", C.c_float)]
 
 
 class OrcEstimate(C.Structure):

@@ -680,6 +680,19 @@ int orc_filter_step(orc_filter* f, const float* control, const float* meas, orc_
         }
         if (f->log_weights)
             for (int s = 0; s < m; ++s) w[s] = expf(w[s] - mx);
+        if (f->ess_frac > 0.0f) {
+            /* effective sample size in FP64; all-zero weights count as uniform */
+            double s1 = 0.0, s2 = 0.0;
+            for (int s = 0; s < m; ++s) {
+                s1 += (double)w[s];
+                s2 += (double)w[s] * (double)w[s];
+            }
+            if (!(s2 > 0.0) || s1 * s1 >= (double)f->ess_frac * (double)m * s2) {
+                if (sel_out)
+                    for (int i = 0; i < m; ++i) sel_out[base + i] = -1;
+                continue;
+            }
+        }
         if (f->resampler == ORC_RES_REF) {
             for (int i = 0; i < m; ++i) uu[i] = U ? U[base + i] : sb[1 + i];
             orc_resample_ref(w, uu, m, sel);

@@ -152,6 +152,9 @@ typedef struct {
     int streams;
     float* rbuf;      /* random buffer (reference layout) */
     int64_t rtotal;
+    float ess_frac;   /* > 0: a sub-filter resamples only while (sum w)^2 / sum w^2 < ess_frac * m
+                         (the reference's ADAPTIVE_RESAMPLING test, resampling-valias.cl:273-284,
+                         with its threshold thr = 1 / (ess_frac * m)); 0 after init */
 } orc_filter;
 
 typedef struct {

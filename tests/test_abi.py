@@ -51,6 +51,7 @@ def test_model_info(E):
     (dict(exchange=2, num_subfilters=7, num_transfer=1), "dx*dy"),
     (dict(exchange=1, num_transfer=300), "2*t"),
     (dict(resampling_freq=1.5), "resampling_freq"),
+    (dict(ess_fraction=-0.1), "ess_fraction"),
     (dict(pipeline=1, rng=0), "phased"),
     (dict(rng=1, mtgp_streams=201), "mtgp_streams"),
     (dict(particles_per_thread=3), "not built"),

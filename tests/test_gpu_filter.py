@@ -151,6 +151,47 @@ def test_skipped_subfilters_keep_propagated_state(gpu, O, m):
             assert np.array_equal(np.sort(st[0, b]), np.sort(srt[0, b]))
 
 
+@pytest.mark.parametrize("pipe", [0, 1, 2])
+@pytest.mark.parametrize("res", [0, 1, 2])
+def test_ess_gate_vs_oracle(gpu, O, pipe, res):
+    """ESS-gated resampling on a torus with exchange: the engine's per
+    sub-filter decisions and selections against the oracle on the same
+    particles (decisions within 1e-5 of the threshold may differ: FP32 exp)."""
+    E = gpu
+    p, inputs, _ = uni_setup()
+    m, N, t = 256, 64, 2
+    rng = E.RNG_REFLAYOUT if pipe == E.PIPELINE_PHASED else E.RNG_SUBFILTER
+    orng = O.RNG_REFLAYOUT if rng == E.RNG_REFLAYOUT else O.RNG_SUBFILTER
+    md = O.model_from_params(UNI, p)
+    probe = O.Filter(md, m, 32, 0, O.EXCH_NONE, res, O.RNG_SUBFILTER, 96, 2, 1, 1.0, 0xF000000D, 0,
+                     np.zeros(3, np.float32))
+    probe.step(inputs["control"][0], inputs["meas"][0])
+    k = probe.sorted()[1].reshape(32, m).astype(np.float64)
+    w = np.exp(k - k.max(axis=1, keepdims=True))
+    frac = float(np.median(w.sum(axis=1) ** 2 / (w * w).sum(axis=1) / m))
+    f = E.ParticleFilter(UNI, p, particles_per_subfilter=m, num_subfilters=N, num_transfer=t, exchange=2,
+                         resampler=res, rng=rng, mtgp_streams=96, pipeline=pipe, ess_fraction=frac)
+    assert f.info()["pipeline"] == pipe
+    f.record_selection(True)
+    of = O.Filter(md, m, N, t, O.EXCH_TORUS, res, orng, 96, f.info()["particles_per_thread"], 1, 1.0, 0xF000000D,
+                  0, np.zeros(3, np.float32))
+    of.f.ess_frac = frac
+    mixed = 0
+    for k in range(3):
+        if k > 0:
+            f.set_particles(of.state())
+        f.step(inputs[k])
+        _, osel = of.step(inputs["control"][k], inputs["meas"][k], want_sel=True)
+        gsel, osel = f.selection().reshape(N, m), osel.reshape(N, m)
+        gskip, oskip = np.all(gsel == -1, axis=1), np.all(osel == -1, axis=1)
+        assert np.mean(gskip == oskip) > 0.95, (gskip.sum(), oskip.sum())
+        both = ~gskip & ~oskip
+        assert np.all((gsel[both] >= 0) & (gsel[both] < m))
+        assert np.mean(gsel[both] == osel[both]) > 0.97
+        mixed += 0 < oskip.sum() < N
+    assert mixed >= 1
+
+
 def rmse_xy(ests, truth):
     m = np.array([e["mean"][:2] for e in ests])
     return float(np.sqrt(np.mean(np.sum((m - truth[:, :2]) ** 2, axis=1))))

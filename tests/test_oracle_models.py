@@ -100,3 +100,46 @@ def test_oracle_filter_tracks_unicycle(O, E, rng_mode):
         err.append((e.mean[0] - truth[k, 0]) ** 2 + (e.mean[1] - truth[k, 1]) ** 2)
     rmse = np.sqrt(np.mean(err))
     assert rmse < 0.25, rmse
+
+
+def ess_ratio(keys, m, log_weights=True):
+    """Per sub-filter effective sample size / m of sorted keys (FP64)."""
+    k = keys.reshape(-1, m).astype(np.float64)
+    w = np.exp(k - k.max(axis=1, keepdims=True)) if log_weights else k
+    return w.sum(axis=1) ** 2 / (w * w).sum(axis=1) / m
+
+
+@pytest.mark.parametrize("res", [0, 1, 2])
+def test_oracle_ess_gate(O, E, res):
+    """ESS-gated resampling in the oracle: a sub-filter resamples iff
+    (sum w)^2 / sum w^2 < f * m; f -> 0 never resamples, and the sub-filters
+    that do resample select exactly what the ungated filter selects."""
+    p = E.unicycle_params(1)
+    inputs, _ = E.make_trace(E.MODEL_UNICYCLE, p, 1, 3)
+    md = O.model_from_params(E.MODEL_UNICYCLE, p)
+    m, N = 128, 32
+
+    def mk(frac):
+        f = O.Filter(md, m, N, 0, O.EXCH_NONE, res, O.RNG_SUBFILTER, 96, 2, 1, 1.0, 0xF000000D, 0,
+                     np.zeros(3, np.float32))
+        f.f.ess_frac = frac
+        return f
+
+    base, never = mk(0.0), mk(1e-9)
+    _, sel0 = base.step(inputs["control"][0], inputs["meas"][0], want_sel=True)
+    _, seln = never.step(inputs["control"][0], inputs["meas"][0], want_sel=True)
+    assert np.all(seln == -1) and np.all(sel0 >= 0)
+    ratio = ess_ratio(base.sorted()[1], m)
+    frac = float(np.median(ratio))
+    gated = mk(frac)
+    _, sel = gated.step(inputs["control"][0], inputs["meas"][0], want_sel=True)
+    sel, sel0 = sel.reshape(N, m), sel0.reshape(N, m)
+    skipped = np.all(sel == -1, axis=1)
+    near = np.abs(ratio / frac - 1.0) < 1e-6
+    assert np.array_equal(skipped[~near], (ratio >= frac)[~near])
+    assert 0 < skipped.sum() < N
+    assert np.array_equal(sel[~skipped], sel0[~skipped])
+    # skipped sub-filters keep the propagated (unsorted) particles
+    st, srt = gated.state().reshape(3, N, m), gated.sorted()[0].reshape(3, N, m)
+    for b in np.flatnonzero(skipped):
+        assert np.array_equal(np.sort(st[0, b]), np.sort(srt[0, b]))
