@@ -15,8 +15,10 @@ filters and the served tracking load (their own JSON lines).
 value:  device-timed (CUDA events on the filter's stream), inputs resident
         in HBM, one CUDA-graph replay per step, L2 flushed (256 MB write)
         before every timed step.  value = particles * steps / sum(step time).
-e2e:    the same through pf_step() with host inputs: H2D of the 128-byte
-        step input and D2H of the estimate inside each timed step.
+e2e:    the same through the public API with host inputs: pf_step_submit /
+        pf_step_collect (pipelined; H2D of the 128-byte step input and D2H
+        of the estimate for every step inside the timed region, the L2 flush
+        time subtracted); e2e.sync: pf_step, one synchronous step at a time.
 roofline: the dominant kernel's algorithmic bytes (the sampling kernel reads
         the state, 12 B per unicycle particle; the resampling kernel writes
         it) over its CUDA-event time, against the measured HBM copy
@@ -308,7 +310,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--resampler", default="systematic", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--phase-steps", type=int, default=100, help="steps of the per-kernel timing pass")
     ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
@@ -419,21 +421,52 @@ def main():
     f.set_timing(False)
     f.set_initial_state(np.array(p.init_state[:E.model_info(W["model"])[0]], np.float32))
 
-    # end to end through pf_step(): host input -> H2D, kernels, D2H of the estimate, per step
-    e2e_ms = []
-    for k in range(args.e2e_steps):
+    # end to end through the public API, pipelined: pf_step_submit (host input
+    # -> pinned ring -> H2D on an upload stream, the step graph waiting for it)
+    # and pf_step_collect (estimate D2H on a download stream into a pinned
+    # ring).  L2 is flushed before every step on the filter's stream; the
+    # flushes carry events of their own and their time is subtracted.
+    K = args.e2e_steps
+    fl = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    got = []
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for k in range(K):
         with torch.cuda.stream(stream):
+            fl[k][0].record(stream)
             flush.fill_(float(k))
-            ev0.record(stream)
-        f.step(inputs[k])  # from the initial state again, the trace from its start
-        ev1.record(stream)
-        ev1.synchronize()
-        e2e_ms.append(ev0.elapsed_time(ev1))
-    e2e_total = float(np.sum(e2e_ms))
+            fl[k][1].record(stream)
+        if k - len(got) >= E.QUEUE_DEPTH:  # ring full: wait for the oldest step
+            got += list(f.collect(1))
+        f.submit(inputs[k])  # from the initial state again, the trace from its start
+        got += list(f.collect(wait=False))
+    got += list(f.collect())
+    ev1.record(stream)
+    ev1.synchronize()
+    assert len(got) == K and all(int(g["step"]) == k + 1 for k, g in enumerate(got))
+    e2e_total = ev0.elapsed_time(ev1) - float(sum(a.elapsed_time(b) for a, b in fl))
     if dist:
         t = torch.tensor([e2e_total], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
+
+    # the synchronous call, one step at a time (the step latency a caller of pf_step sees)
+    f.set_initial_state(np.array(p.init_state[:E.model_info(W["model"])[0]], np.float32))
+    sync_ms = []
+    for k in range(K):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev0.record(stream)
+        f.step(inputs[k])
+        ev1.record(stream)
+        ev1.synchronize()
+        sync_ms.append(ev0.elapsed_time(ev1))
+    sync_total = float(np.sum(sync_ms))
+    if dist:
+        t = torch.tensor([sync_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sync_total = float(t.item())
     e2e_value = world * particles * args.e2e_steps / (e2e_total * 1e-3) if args.e2e_steps > 0 else None
 
     if rank == 0:
@@ -480,7 +513,12 @@ def main():
                                   "alg_bytes_per_particle_step": alg, "phase_ms": phases}},
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 128,
                     "d2h_bytes_per_step": int(E.ESTIMATE_DTYPE.itemsize),
-                    "ms_per_step": e2e_total / args.e2e_steps if args.e2e_steps > 0 else None},
+                    "ms_per_step": e2e_total / args.e2e_steps if args.e2e_steps > 0 else None,
+                    "api": "pf_step_submit + pf_step_collect (pipelined, %d steps; L2 flush time subtracted)"
+                           % args.e2e_steps,
+                    "sync": {"value": world * particles * args.e2e_steps / (sync_total * 1e-3)
+                             if args.e2e_steps > 0 else None, "ms_per_step": sync_total / max(args.e2e_steps, 1),
+                             "api": "pf_step (synchronous, one step at a time)"}},
             "gpu_launches": int(args.steps * len(phases)),
             "timing": "value: CUDA events around each step's graph launch (no events inside); kernel times: "
                       "a separate %d-step pass with events between the launches" % args.phase_steps,

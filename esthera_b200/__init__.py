@@ -27,6 +27,7 @@ EXCHANGE_NONE, EXCHANGE_RING, EXCHANGE_TORUS, EXCHANGE_ALL2ALL = 0, 1, 2, 3
 RESAMPLE_REFERENCE, RESAMPLE_SYSTEMATIC, RESAMPLE_VOSE = 0, 1, 2
 RNG_SUBFILTER, RNG_REFLAYOUT = 0, 1
 PIPELINE_FUSED, PIPELINE_PHASED, PIPELINE_SPLIT = 0, 1, 2
+QUEUE_DEPTH = 64  # PF_QUEUE_DEPTH: steps pf_step_submit may keep pending
 MTGP_MASK_PARAMS, MTGP_MASK_CUDA_REF = 0, 0xFF800000
 MAX_STATE, MAX_CONTROL, MAX_MEAS = 16, 8, 16
 
@@ -118,6 +119,8 @@ def _declare(L):
         "pf_step": (C.c_int, [P, C.POINTER(StepInput), C.POINTER(Estimate)]),
         "pf_run_device": (C.c_int, [P, P, P, C.c_int32, C.c_int32]),
         "pf_run_device_continue": (C.c_int, [P, C.c_int32]),
+        "pf_step_submit": (C.c_int, [P, P]),
+        "pf_step_collect": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
         "pf_synchronize": (C.c_int, [P]),
         "pf_stream": (P, [P]),
         "pf_set_timing": (C.c_int, [P, C.c_int32]),
@@ -345,6 +348,19 @@ class ParticleFilter:
         e = Estimate()
         check(lib().pf_step(self._h, C.byref(s), C.byref(e)))
         return estimate_to_numpy(e)
+
+    def submit(self, inp):
+        """Enqueue one step with a host input; returns without waiting (pf_step_submit)."""
+        s = inp if isinstance(inp, StepInput) else step_input(inp)
+        check(lib().pf_step_submit(self._h, C.byref(s)))
+
+    def collect(self, max_n=None, wait=True):
+        """Estimates of submitted steps, oldest first (pf_step_collect): ESTIMATE_DTYPE [n]."""
+        max_n = QUEUE_DEPTH if max_n is None else int(max_n)
+        out = np.zeros(max(max_n, 1), ESTIMATE_DTYPE)
+        n = C.c_int32(0)
+        check(lib().pf_step_collect(self._h, out.ctypes.data_as(C.c_void_p), max_n, 1 if wait else 0, C.byref(n)))
+        return out[:n.value]
 
     def run_device(self, d_inputs_ptr, d_estimates_ptr, capacity, steps):
         """Reset the step counter and run `steps` steps over device arrays of `capacity` entries."""

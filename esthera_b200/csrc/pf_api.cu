@@ -186,6 +186,15 @@ struct pf_filter {
     const pf_step_input* graph_inputs = nullptr;
     pf_estimate* graph_est = nullptr;
     int32_t graph_cap = 0;
+    // submit / collect queue (pf_step_submit): pinned and device rings of
+    // inputs and estimates, an upload and a download stream, events per slot
+    pf_step_input *h_q_in = nullptr, *d_q_in = nullptr;
+    pf_estimate *h_q_est = nullptr, *d_q_est = nullptr;
+    cudaStream_t q_up = nullptr, q_down = nullptr;
+    cudaEvent_t q_ev_up[PF_QUEUE_DEPTH] = {}, q_ev_done[PF_QUEUE_DEPTH] = {}, q_ev_got[PF_QUEUE_DEPTH] = {};
+    int q_active = 0;   // the device counter holds q_next (else set it before the next submit)
+    int q_pending = 0;  // submitted, not yet collected
+    int32_t q_next = 0; // step number (and slot, modulo the depth) of the next submit
     // per-phase timing: events recorded between the launches of a step
     int timing = 0;
     cudaEvent_t ev[8] = {};
@@ -219,6 +228,15 @@ static void release(pf_filter* f)
     if (f->graph) cudaGraphExecDestroy(f->graph);
     for (cudaEvent_t e : f->ev)
         if (e) cudaEventDestroy(e);
+    for (int i = 0; i < PF_QUEUE_DEPTH; ++i) {
+        if (f->q_ev_up[i]) cudaEventDestroy(f->q_ev_up[i]);
+        if (f->q_ev_done[i]) cudaEventDestroy(f->q_ev_done[i]);
+        if (f->q_ev_got[i]) cudaEventDestroy(f->q_ev_got[i]);
+    }
+    if (f->q_up) cudaStreamDestroy(f->q_up);
+    if (f->q_down) cudaStreamDestroy(f->q_down);
+    if (f->h_q_in) cudaFreeHost(f->h_q_in);
+    if (f->h_q_est) cudaFreeHost(f->h_q_est);
     for (void* p : f->allocs) cudaFree(p);
     if (f->h_est) cudaFreeHost(f->h_est);
     if (f->h_in) cudaFreeHost(f->h_in);
@@ -535,8 +553,10 @@ extern "C" pf_status pf_set_initial_state(pf_filter* f, const float* state)
     std::vector<float> h((size_t)f->mi.S * f->T);
     for (int v = 0; v < f->mi.S; ++v)
         for (int64_t i = 0; i < f->T; ++i) h[(size_t)v * f->T + i] = state[v];
+    CU(cudaStreamSynchronize(f->stream));
     CU(cudaMemcpy(f->state, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
     f->steps_done = 0;
+    f->q_active = 0;
     return mark_need_init(f);
 }
 
@@ -651,8 +671,12 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
             CU(launch_a2a_merge(1, desc, st));
             CU(mark("a2a_merge"));
         }
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, ctr_inc, 1));
+        // with an exchange period every CTA of the resampling kernel reads the
+        // step counter, so it advances in a launch of its own after the kernel
+        const bool late = ctr_inc && c.exchange_period > 1;
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, 1));
         CU(mark("exchange_resample"));
+        if (late) CU(launch_counter_inc(ctr_inc, st));
     } else {
         CU(f->ops.sample_weight(M, E, N, st, desc, nullptr, in));
         CU(mark("sample_weight"));
@@ -725,41 +749,141 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     return PF_OK;
 }
 
+// The graph of one step reading inputs[ctr % capacity] and writing
+// estimates[ctr % capacity] (ctr: the filter's device step counter), rebuilt
+// when the arrays change.
+static pf_status ensure_run_graph(pf_filter* f, const pf_step_input* d_inputs, pf_estimate* d_estimates,
+                                  int32_t capacity)
+{
+    if (f->graph && f->graph_inputs == d_inputs && f->graph_est == d_estimates && f->graph_cap == capacity)
+        return PF_OK;
+    CU(cudaStreamSynchronize(f->stream));
+    if (f->graph) {
+        cudaGraphExecDestroy(f->graph);
+        f->graph = nullptr;
+    }
+    pf_status s = upload_descs(f, d_estimates);
+    if (s != PF_OK) return s;
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
+    InputRef ir{d_inputs, 0, f->ctr, capacity};
+    s = enqueue_step(f, f->d_desc + 1, ir, f->ctr);
+    cudaError_t e = cudaStreamEndCapture(f->stream, &g);
+    if (s != PF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&f->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        f->graph = nullptr;
+        return fail(PF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    f->graph_inputs = d_inputs;
+    f->graph_est = d_estimates;
+    f->graph_cap = capacity;
+    return PF_OK;
+}
+
 extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, pf_estimate* d_estimates,
                                    int32_t capacity, int32_t steps)
 {
     if (!f || !d_inputs || !d_estimates || capacity < 1 || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
     CU(cudaSetDevice(f->cfg.device));
-    if (!f->graph || f->graph_inputs != d_inputs || f->graph_est != d_estimates || f->graph_cap != capacity) {
-        if (f->graph) {
-            cudaGraphExecDestroy(f->graph);
-            f->graph = nullptr;
-        }
-        pf_status s = upload_descs(f, d_estimates);
-        if (s != PF_OK) return s;
-        cudaGraph_t g = nullptr;
-        CU(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
-        InputRef ir{d_inputs, 0, f->ctr, capacity};
-        s = enqueue_step(f, f->d_desc + 1, ir, f->ctr);
-        cudaError_t e = cudaStreamEndCapture(f->stream, &g);
-        if (s != PF_OK) {
-            if (g) cudaGraphDestroy(g);
-            return s;
-        }
-        if (e != cudaSuccess) return fail(PF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&f->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            f->graph = nullptr;
-            return fail(PF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-        }
-        f->graph_inputs = d_inputs;
-        f->graph_est = d_estimates;
-        f->graph_cap = capacity;
-    }
+    pf_status s = ensure_run_graph(f, d_inputs, d_estimates, capacity);
+    if (s != PF_OK) return s;
     CU(cudaMemsetAsync(f->ctr, 0, sizeof(int32_t), f->stream));
+    f->q_active = 0;
     for (int i = 0; i < steps; ++i) CU(cudaGraphLaunch(f->graph, f->stream));
     f->steps_done += steps;
+    return PF_OK;
+}
+
+static pf_status queue_setup(pf_filter* f)
+{
+    if (f->d_q_in) return PF_OK;
+    void* h = nullptr;
+    if (!f->h_q_in) {
+        CU(cudaMallocHost(&h, PF_QUEUE_DEPTH * sizeof(pf_step_input)));
+        f->h_q_in = static_cast<pf_step_input*>(h);
+    }
+    if (!f->h_q_est) {
+        CU(cudaMallocHost(&h, PF_QUEUE_DEPTH * sizeof(pf_estimate)));
+        f->h_q_est = static_cast<pf_estimate*>(h);
+    }
+    if (!f->q_up) CU(cudaStreamCreateWithFlags(&f->q_up, cudaStreamNonBlocking));
+    if (!f->q_down) CU(cudaStreamCreateWithFlags(&f->q_down, cudaStreamNonBlocking));
+    for (int i = 0; i < PF_QUEUE_DEPTH; ++i) {
+        if (!f->q_ev_up[i]) CU(cudaEventCreateWithFlags(&f->q_ev_up[i], cudaEventDisableTiming));
+        if (!f->q_ev_done[i]) CU(cudaEventCreateWithFlags(&f->q_ev_done[i], cudaEventDisableTiming));
+        if (!f->q_ev_got[i]) CU(cudaEventCreateWithFlags(&f->q_ev_got[i], cudaEventDisableTiming));
+    }
+    if (!f->d_q_est) {
+        pf_status s = dalloc(f, &f->d_q_est, PF_QUEUE_DEPTH);
+        if (s != PF_OK) return s;
+    }
+    pf_step_input* di = nullptr;
+    pf_status s = dalloc(f, &di, PF_QUEUE_DEPTH);
+    if (s != PF_OK) return s;
+    f->d_q_in = di;  // set last: marks the queue as set up
+    return PF_OK;
+}
+
+extern "C" pf_status pf_step_submit(pf_filter* f, const pf_step_input* in)
+{
+    if (!f || !in) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    pf_status s = queue_setup(f);
+    if (s != PF_OK) return s;
+    if (f->q_pending >= PF_QUEUE_DEPTH)
+        return fail(PF_ERR_BUSY, "%d steps pending: collect before submitting more", PF_QUEUE_DEPTH);
+    if (!f->q_active || f->q_next != f->steps_done) {
+        // another call stepped the filter or reset its counter since the last submit
+        if (f->q_pending > 0)
+            return fail(PF_ERR_BUSY, "collect the pending steps before submitting after another step call");
+        s = ensure_run_graph(f, f->d_q_in, f->d_q_est, PF_QUEUE_DEPTH);
+        if (s != PF_OK) return s;
+        CU(launch_counter_set(f->ctr, f->steps_done, f->stream));
+        f->q_next = f->steps_done;
+        f->q_active = 1;
+    }
+    const int slot = (int)(f->q_next % PF_QUEUE_DEPTH);
+    f->h_q_in[slot] = *in;
+    CU(cudaMemcpyAsync(f->d_q_in + slot, f->h_q_in + slot, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->q_up));
+    CU(cudaEventRecord(f->q_ev_up[slot], f->q_up));
+    CU(cudaStreamWaitEvent(f->stream, f->q_ev_up[slot], 0));
+    CU(cudaGraphLaunch(f->graph, f->stream));
+    CU(cudaEventRecord(f->q_ev_done[slot], f->stream));
+    CU(cudaStreamWaitEvent(f->q_down, f->q_ev_done[slot], 0));
+    CU(cudaMemcpyAsync(f->h_q_est + slot, f->d_q_est + slot, sizeof(pf_estimate), cudaMemcpyDeviceToHost,
+                       f->q_down));
+    CU(cudaEventRecord(f->q_ev_got[slot], f->q_down));
+    f->q_next++;
+    f->steps_done++;
+    f->q_pending++;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_step_collect(pf_filter* f, pf_estimate* out, int32_t max, int32_t wait, int32_t* count)
+{
+    if (!f || !count || (max > 0 && !out)) return fail(PF_ERR_INVALID, "null argument");
+    *count = 0;
+    if (f->q_pending == 0 || max <= 0) return PF_OK;
+    CU(cudaSetDevice(f->cfg.device));
+    while (*count < max && f->q_pending > 0) {
+        const int32_t k = f->q_next - f->q_pending;  // oldest pending step
+        const int slot = (int)(k % PF_QUEUE_DEPTH);
+        if (wait) {
+            CU(cudaEventSynchronize(f->q_ev_got[slot]));
+        } else {
+            const cudaError_t e = cudaEventQuery(f->q_ev_got[slot]);
+            if (e == cudaErrorNotReady) break;
+            CU(e);
+        }
+        out[(*count)++] = f->h_q_est[slot];
+        f->q_pending--;
+    }
     return PF_OK;
 }
 
@@ -843,6 +967,7 @@ extern "C" pf_status pf_restore(pf_filter* f, const void* buf)
     CU(cudaMemcpy(f->mtgp, p, mb, cudaMemcpyHostToDevice));
     p += mb;
     memcpy(&f->steps_done, p, 4);
+    f->q_active = 0;
     return mark_need_init(f);
 }
 

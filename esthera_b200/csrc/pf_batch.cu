@@ -37,12 +37,6 @@ __global__ void k_batch_fill(const FilterDesc* __restrict__ descs, const int2* _
     }
 }
 
-// Advances the run's step counter once every filter's step is enqueued before it.
-__global__ void k_counter_inc(int32_t* ctr)
-{
-    if (threadIdx.x == 0 && blockIdx.x == 0) *ctr += 1;
-}
-
 constexpr int kMaxGraphSteps = 256;
 
 }  // namespace
@@ -173,10 +167,7 @@ static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRe
     const int M = B->M, E = B->E;
     CU(B->ops.sample_sort(M, E, true, B->NS, B->stream, desc, B->map, in));
     CU(B->ops.exchange_resample(M, E, B->cfg.resampler, B->NS, B->stream, desc, B->map, in, nullptr, 1));
-    if (ctr_inc) {
-        k_counter_inc<<<1, 32, 0, B->stream>>>(ctr_inc);
-        CU(cudaGetLastError());
-    }
+    if (ctr_inc) CU(launch_counter_inc(ctr_inc, B->stream));
     return PF_OK;
 }
 

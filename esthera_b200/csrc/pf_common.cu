@@ -288,4 +288,23 @@ cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaS
     return cudaGetLastError();
 }
 
+// A run's device step counter, advanced (or set) by a launch of its own once
+// every kernel of the step that reads it is enqueued before it.
+__global__ void k_counter_update(int32_t* ctr, int32_t set, int32_t value)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *ctr = set ? value : *ctr + 1;
+}
+
+cudaError_t launch_counter_inc(int32_t* ctr, cudaStream_t st)
+{
+    k_counter_update<<<1, 32, 0, st>>>(ctr, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_counter_set(int32_t* ctr, int32_t value, cudaStream_t st)
+{
+    k_counter_update<<<1, 32, 0, st>>>(ctr, 1, value);
+    return cudaGetLastError();
+}
+
 }  // namespace pfdev

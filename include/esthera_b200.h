@@ -198,6 +198,24 @@ pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, pf_estimate
 /* Replays `steps` more steps of the run set up by pf_run_device (the step
  * counter continues), e.g. to time steps one at a time. */
 pf_status pf_run_device_continue(pf_filter* f, int32_t steps);
+/* Pipelined host stepping (no counterpart in the reference, whose driver loop
+ * copies each step's estimate back before the next step starts,
+ * pf_generic_soa.cu:858-1154).  pf_step_submit copies the input into a pinned
+ * ring slot and returns without waiting: the slot is uploaded on a copy stream,
+ * the step (the CUDA graph of pf_run_device, over device rings of
+ * PF_QUEUE_DEPTH inputs and estimates) runs on the filter's stream once the
+ * upload landed, and the estimate is downloaded into a pinned ring slot on a
+ * second copy stream, so uploads and downloads overlap the neighbouring steps.
+ * Results equal pf_step's on the same inputs (the step counter is the number of
+ * steps since the initial state, as for pf_step).  At most PF_QUEUE_DEPTH steps
+ * may be pending: a further submit returns PF_ERR_BUSY, as does a submit after
+ * another call stepped the filter while steps are pending.
+ * pf_step_collect returns up to `max` estimates in submission order; wait != 0
+ * blocks until that many are done (or all pending ones), wait == 0 returns the
+ * finished ones only.  One host thread per filter. */
+#define PF_QUEUE_DEPTH 64
+pf_status pf_step_submit(pf_filter* f, const pf_step_input* in);
+pf_status pf_step_collect(pf_filter* f, pf_estimate* out, int32_t max, int32_t wait, int32_t* count);
 pf_status pf_synchronize(pf_filter* f);
 /* Per-launch timing: with timing on, every step records a CUDA event before its
  * first launch and after each launch (graph replays included).

@@ -116,6 +116,74 @@ def test_graph_replay_equals_host_steps(gpu):
         assert est[k]["step"] == k + 1
 
 
+@pytest.mark.parametrize("period", [2, 3])
+def test_graph_replay_exchange_period(gpu, period):
+    """Graph replay with an exchange period: every resampling CTA reads the
+    device step counter, which must not advance before all of them did."""
+    import torch
+    E = gpu
+    steps = 9
+    p, inputs, _ = uni_setup(steps=steps)
+    cfg = dict(particles_per_subfilter=128, num_subfilters=2048, num_transfer=1, exchange=2,
+               exchange_period=period, pipeline=E.PIPELINE_SPLIT)
+    fa, ea = run(E, UNI, p, inputs, steps, **cfg)
+    fb = E.ParticleFilter(UNI, p, **cfg)
+    d_in = torch.from_numpy(inputs.view(np.uint8).copy()).cuda()
+    d_est = torch.zeros(steps * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    fb.run_device(d_in.data_ptr(), d_est.data_ptr(), steps, steps)
+    fb.synchronize()
+    est = d_est.cpu().numpy().view(E.ESTIMATE_DTYPE)
+    assert np.array_equal(fa.particles(), fb.particles())
+    for k in range(steps):
+        assert np.array_equal(est[k]["mean"], ea[k]["mean"]) and est[k]["step"] == k + 1
+
+
+@pytest.mark.parametrize("pipe,period", [(0, 1), (2, 1), (2, 2)])
+def test_submit_collect_equals_step(gpu, pipe, period):
+    """Pipelined submit / collect against synchronous pf_step on the same
+    inputs, past the ring depth, with a synchronous step and a
+    re-initialisation in between."""
+    E = gpu
+    steps = 150
+    p, inputs, _ = uni_setup(steps=steps)
+    cfg = dict(particles_per_subfilter=256, num_subfilters=64, num_transfer=2, exchange=2, pipeline=pipe,
+               exchange_period=period)
+    fa, ea = run(E, UNI, p, inputs, steps, **cfg)
+    fb = E.ParticleFilter(UNI, p, **cfg)
+    got = []
+    for k in range(E.QUEUE_DEPTH):
+        fb.submit(inputs[k])
+    with pytest.raises(E.PFError) as ei:
+        fb.submit(inputs[E.QUEUE_DEPTH])
+    assert ei.value.status == E.PF_ERR_BUSY
+    got += list(fb.collect(10))
+    k = E.QUEUE_DEPTH
+    while k < 100:
+        fb.submit(inputs[k])
+        k += 1
+        got += list(fb.collect(wait=False))
+    got += list(fb.collect())
+    assert len(got) == 100 and len(fb.collect(5, wait=False)) == 0
+    got.append(fb.step(inputs[100]))  # a synchronous step in between
+    for k in range(101, steps):
+        fb.submit(inputs[k])
+    got += list(fb.collect())
+    assert len(got) == steps
+    for k in range(steps):
+        assert got[k]["step"] == ea[k]["step"] == k + 1
+        assert np.array_equal(got[k]["mean"], ea[k]["mean"]) and got[k]["best_key"] == ea[k]["best_key"]
+    assert np.array_equal(fa.particles(), fb.particles())
+    # restart from the initial state: the queue re-reads the step counter
+    init = np.zeros(3, np.float32)
+    fa.set_initial_state(init)
+    fb.set_initial_state(init)
+    a = [fa.step(inputs[k]) for k in range(5)]
+    for k in range(5):
+        fb.submit(inputs[k])
+    b = fb.collect(5)
+    assert all(np.array_equal(x["mean"], y["mean"]) and x["step"] == y["step"] for x, y in zip(a, b))
+
+
 def test_snapshot_restore(gpu):
     E = gpu
     p, inputs, _ = uni_setup(steps=10)
