@@ -331,6 +331,18 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
     return PF_OK;
 }
 
+// The kernels' status word (PF_STATUS_* bits), stored right after the
+// estimate so that pf_step's estimate copy brings it along.
+static int32_t* status_word(pf_filter* f) { return reinterpret_cast<int32_t*>(f->d_est + 1); }
+
+static pf_status check_status(int32_t st)
+{
+    if (st & PF_STATUS_WAIT_TIMEOUT)
+        return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
+                                    "propagated particles)");
+    return PF_OK;
+}
+
 static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
 {
     memset(&D, 0, sizeof(D));
@@ -367,6 +379,7 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.ess_frac = f->cfg.ess_fraction;
     D.nnorm = (int64_t)f->mi.K * f->T;
     D.est_ctr = f->est_ctr;
+    D.status = status_word(f);
     D.gpart = f->gpart;
     D.angle_mask = f->angle_mask;
     D.na = f->na;
@@ -495,17 +508,18 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     TRY(dalloc(f, &f->ctr, 1));
     TRY(dalloc(f, &f->est_ctr, 1));
     TRY(dalloc(f, &f->gpart, (size_t)((f->N + 31) / 32) * kPartStride));
-    TRY(dalloc(f, &f->d_est, 1));
+    TRY(dalloc(f, &f->d_est, 2));  // [0] the estimate, then the kernels' status word
     TRY(dalloc(f, &f->d_in, 1));
     TRY(dalloc(f, &f->d_desc, 2));
-    if (cudaMallocHost(&f->h_est, sizeof(pf_estimate)) != cudaSuccess ||
+    if (cudaMallocHost(&f->h_est, 2 * sizeof(pf_estimate)) != cudaSuccess ||
         cudaMallocHost(&f->h_in, sizeof(pf_step_input)) != cudaSuccess) {
         cudaGetLastError();
         release(f);
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
     }
     TRY(init_streams(f));
-    if (cudaMemset(f->est_ctr, 0, 4) != cudaSuccess || cudaMemset(f->ctr, 0, 4) != cudaSuccess) {
+    if (cudaMemset(f->est_ctr, 0, 4) != cudaSuccess || cudaMemset(f->ctr, 0, 4) != cudaSuccess ||
+        cudaMemset(f->d_est, 0, 2 * sizeof(pf_estimate)) != cudaSuccess) {
         cudaGetLastError();
         release(f);
         return fail(PF_ERR_CUDA, "cudaMemset failed");
@@ -739,9 +753,12 @@ extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate*
     InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
     pf_status s = enqueue_step(f, f->d_desc, ir, nullptr);
     if (s != PF_OK) return s;
-    CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate), cudaMemcpyDeviceToHost, f->stream));
+    CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate) + sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       f->stream));
     CU(cudaStreamSynchronize(f->stream));
     f->steps_done++;
+    s = check_status(*reinterpret_cast<const int32_t*>(f->h_est + 1));
+    if (s != PF_OK) return s;
     if (out) {
         *out = *f->h_est;
         out->step = f->steps_done;
@@ -903,7 +920,9 @@ extern "C" pf_status pf_synchronize(pf_filter* f)
     if (!f) return fail(PF_ERR_INVALID, "null argument");
     CU(cudaSetDevice(f->cfg.device));
     CU(cudaStreamSynchronize(f->stream));
-    return PF_OK;
+    int32_t st = 0;
+    CU(cudaMemcpy(&st, status_word(f), sizeof(st), cudaMemcpyDeviceToHost));
+    return check_status(st);
 }
 
 extern "C" void* pf_stream(pf_filter* f) { return f ? (void*)f->stream : nullptr; }

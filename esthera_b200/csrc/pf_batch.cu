@@ -144,6 +144,7 @@ static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate
     D.ess_frac = B->cfg.ess_fraction;
     D.nnorm = (int64_t)B->mi.K * D.T;
     D.est_ctr = B->est_ctr + f;
+    D.status = reinterpret_cast<int32_t*>(B->d_est + B->F);
     D.gpart = B->gpart + (int64_t)B->grp_off[f] * kPartStride;
     D.angle_mask = angle_mask_of(B->model);
     D.na = angle_count_of(B->model);
@@ -159,6 +160,14 @@ static pf_status upload_batch_descs(pf_batch* B, pf_estimate* run_est, int32_t c
     }
     CU(cudaMemcpyAsync(B->d_desc, d.data(), d.size() * sizeof(FilterDesc), cudaMemcpyHostToDevice, B->stream));
     CU(cudaStreamSynchronize(B->stream));
+    return PF_OK;
+}
+
+static pf_status batch_status(int32_t st)
+{
+    if (st & PF_STATUS_WAIT_TIMEOUT)
+        return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
+                                    "propagated particles)");
     return PF_OK;
 }
 
@@ -288,9 +297,9 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     TRY(balloc(B, &B->map, (size_t)NS));
     TRY(balloc(B, &B->d_desc, 2 * (size_t)num_filters));
     TRY(balloc(B, &B->d_in, (size_t)num_filters));
-    TRY(balloc(B, &B->d_est, (size_t)num_filters));
+    TRY(balloc(B, &B->d_est, (size_t)num_filters + 1));  // + the kernels' status word
     if (cudaMallocHost(&B->h_in, sizeof(pf_step_input) * num_filters) != cudaSuccess ||
-        cudaMallocHost(&B->h_est, sizeof(pf_estimate) * num_filters) != cudaSuccess) {
+        cudaMallocHost(&B->h_est, sizeof(pf_estimate) * (num_filters + 1)) != cudaSuccess) {
         cudaGetLastError();
         release(B);
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
@@ -313,7 +322,8 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
             return fail(PF_ERR_CUDA, "initial upload failed");
         }
     }
-    if (cudaMemset(B->est_ctr, 0, 4 * (size_t)num_filters) != cudaSuccess || cudaMemset(B->ctr, 0, 4) != cudaSuccess) {
+    if (cudaMemset(B->est_ctr, 0, 4 * (size_t)num_filters) != cudaSuccess || cudaMemset(B->ctr, 0, 4) != cudaSuccess ||
+        cudaMemset(B->d_est + num_filters, 0, sizeof(pf_estimate)) != cudaSuccess) {
         cudaGetLastError();
         release(B);
         return fail(PF_ERR_CUDA, "cudaMemset failed");
@@ -380,9 +390,14 @@ extern "C" pf_status pf_batch_step(pf_batch* B, const pf_step_input* inputs, pf_
     InputRef ir{B->d_in, 1, nullptr, 0, B->steps_done};
     pf_status s = enqueue_batch_step(B, B->d_desc, ir, nullptr);
     if (s != PF_OK) return s;
-    if (out) CU(cudaMemcpyAsync(B->h_est, B->d_est, sizeof(pf_estimate) * B->F, cudaMemcpyDeviceToHost, B->stream));
+    // the estimates and the kernels' status word after them in one copy
+    CU(cudaMemcpyAsync(out ? (void*)B->h_est : (void*)(B->h_est + B->F), out ? (void*)B->d_est : (void*)(B->d_est + B->F),
+                       out ? sizeof(pf_estimate) * B->F + sizeof(int32_t) : sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       B->stream));
     CU(cudaStreamSynchronize(B->stream));
     B->steps_done++;
+    s = batch_status(*reinterpret_cast<const int32_t*>(B->h_est + B->F));
+    if (s != PF_OK) return s;
     if (out) {
         memcpy(out, B->h_est, sizeof(pf_estimate) * B->F);
         for (int f = 0; f < B->F; ++f) out[f].step = B->steps_done;
@@ -468,7 +483,9 @@ extern "C" pf_status pf_batch_synchronize(pf_batch* B)
     if (!B) return fail(PF_ERR_INVALID, "null argument");
     CU(cudaSetDevice(B->cfg.device));
     CU(cudaStreamSynchronize(B->stream));
-    return PF_OK;
+    int32_t st = 0;
+    CU(cudaMemcpy(&st, B->d_est + B->F, sizeof(st), cudaMemcpyDeviceToHost));
+    return batch_status(st);
 }
 
 extern "C" void* pf_batch_stream(pf_batch* B) { return B ? (void*)B->stream : nullptr; }

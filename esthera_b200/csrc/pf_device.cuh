@@ -361,6 +361,43 @@ __device__ __forceinline__ int upper_count(const double* cum, double x)
     return lo < M ? lo : M - 1;
 }
 
+// upper_count for E increasing positions x[0] <= x[1] <= ... (a thread's
+// consecutive systematic positions): a full binary search for x[0], then from
+// the previous count forward -- at most 4 single steps (the usual advance is
+// about one entry per position), else a binary search of the rest.  Same
+// results as upper_count on each position (cum is non-decreasing).
+template <int M, int E>
+__device__ __forceinline__ void upper_counts(const double* cum, const double (&x)[E], int (&out)[E])
+{
+    int lo = 0, hi = M;
+#pragma unroll
+    for (int it = 0; it < 11; ++it) {
+        if (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cum[mid] <= x[0]) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    out[0] = lo < M ? lo : M - 1;
+#pragma unroll
+    for (int e = 1; e < E; ++e) {
+        int n = 0;
+        while (n < 4 && lo < M && cum[lo] <= x[e]) {
+            ++lo;
+            ++n;
+        }
+        if (n == 4 && lo < M && cum[lo] <= x[e]) {
+            hi = M;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (cum[mid] <= x[e]) lo = mid + 1;
+                else hi = mid;
+            }
+        }
+        out[e] = lo < M ? lo : M - 1;
+    }
+}
+
 // FP32 Blelloch exclusive scan of M values in place (prefix_sum,
 // pf_generic_soa.cu:169-216); same tree, pairs shared out over the block.
 template <int M>
@@ -627,7 +664,9 @@ __device__ __forceinline__ unsigned vose_draw(const float* prob, const unsigned*
 // ---------------------------------------------------------------------------
 // Models.  Each provides S (state floats), K (normals per particle), NA
 // (angular state variables, reported as sin/cos for circular means),
-// prepare() (one thread, per-step constants) and step() (one particle:
+// prepare() (per-step constants, called by the 32 lanes of one warp: each
+// lane fills its own fields, the transcendental ones one per lane so the
+// FP64 chains run side by side instead of one after another) and step() (one particle:
 // propagate in place, return the FP32 log-likelihood, and sin/cos of the
 // angular variables of the new state).
 // ---------------------------------------------------------------------------
@@ -649,31 +688,34 @@ struct Unicycle {
     };
     // Exact-arc velocity model: x' = x + A cos th - B sin th, y' = y + A sin th + B cos th
     // with A = v sin(w dt)/w, B = v (1 - cos(w dt))/w (straight-line limit as w -> 0).
-    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    // lane 8: motion constants; lanes 0..7: landmark `lane`
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
     {
         const pf_unicycle_params& p = mp.uni;
-        const double dt = in.dt > 0.0f ? in.dt : p.dt;
-        const double v = in.control[0], w = in.control[1];
-        const double wd = w * dt;
-        double A, B;
-        if (fabs(wd) < 1e-4) {
-            A = v * dt * (1.0 - wd * wd / 6.0);
-            B = v * dt * (wd / 2.0);
-        } else {
-            A = v * sin(wd) / w;
-            B = v * (1.0 - cos(wd)) / w;
-        }
-        c.A = (float)A;
-        c.B = (float)B;
-        c.wd = (float)wd;
-        c.sq0 = p.sigma_q[0];
-        c.sq1 = p.sigma_q[1];
-        c.sq2 = p.sigma_q[2];
-        c.isr = 1.0f / p.sigma_range;
-        c.isb = 1.0f / p.sigma_bearing;
         const int L = p.num_landmarks < 1 ? 1 : (p.num_landmarks > 8 ? 8 : p.num_landmarks);
-        c.L = L;
-        for (int j = 0; j < 8; ++j) {
+        if (lane == 8) {
+            const double dt = in.dt > 0.0f ? in.dt : p.dt;
+            const double v = in.control[0], w = in.control[1];
+            const double wd = w * dt;
+            double A, B;
+            if (fabs(wd) < 1e-4) {
+                A = v * dt * (1.0 - wd * wd / 6.0);
+                B = v * dt * (wd / 2.0);
+            } else {
+                A = v * sin(wd) / w;
+                B = v * (1.0 - cos(wd)) / w;
+            }
+            c.A = (float)A;
+            c.B = (float)B;
+            c.wd = (float)wd;
+            c.sq0 = p.sigma_q[0];
+            c.sq1 = p.sigma_q[1];
+            c.sq2 = p.sigma_q[2];
+            c.isr = 1.0f / p.sigma_range;
+            c.isb = 1.0f / p.sigma_bearing;
+            c.L = L;
+        } else if (lane < 8) {
+            const int j = lane;
             c.lx[j] = p.landmarks[j][0];
             c.ly[j] = p.landmarks[j][1];
             c.rm[j] = j < L ? in.meas[j] : 0.0f;
@@ -767,14 +809,17 @@ struct DhArm {
         float dt, sqd, isp, isa;
         float a[6], d[6], ca[6], sa[6], z[6];
     };
-    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    // lane 6: scalars; lanes 0..5: joint `lane`
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
     {
         const pf_dharm_params& p = mp.arm;
-        c.dt = in.dt > 0.0f ? in.dt : p.dt;
-        c.sqd = p.sigma_qd;
-        c.isp = 1.0f / p.sigma_pos;
-        c.isa = 1.0f / p.sigma_ang;
-        for (int i = 0; i < 6; ++i) {
+        if (lane == 6) {
+            c.dt = in.dt > 0.0f ? in.dt : p.dt;
+            c.sqd = p.sigma_qd;
+            c.isp = 1.0f / p.sigma_pos;
+            c.isa = 1.0f / p.sigma_ang;
+        } else if (lane < 6) {
+            const int i = lane;
             c.a[i] = p.a[i];
             c.d[i] = p.d[i];
             c.ca[i] = (float)cos((double)p.alpha[i]);
@@ -843,8 +888,9 @@ struct RefArm {
         float cdt[5];
         float z[7];
     };
-    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp)
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
     {
+        if (lane != 0) return;
         c.dt = in.dt > 0.0f ? in.dt : mp.ref.dt;
         for (int i = 0; i < 5; ++i) c.cdt[i] = in.control[i] * c.dt;
         for (int i = 0; i < 7; ++i) c.z[i] = in.meas[i];

@@ -48,8 +48,28 @@ struct FilterDesc {
     uint32_t angle_mask;
     int32_t na;        // angular state variables (circular means)
     int32_t exch_period;  // exchange on steps with step % period == 0 (<= 1: every step)
+    int32_t* status;      // PF_STATUS_* bits set by the kernels (0: all well)
     ModelParams mp;
 };
+
+// status bits: a bounded wait on a bulk copy ran out (the sub-filter kept its
+// propagated particles)
+constexpr int PF_STATUS_WAIT_TIMEOUT = 1;
+
+// A CTA's filter descriptor, copied once into shared memory (all threads of
+// the CTA call this at their start).  The kernels read descriptor fields all
+// through their phases; read from global memory, a field whose line the
+// streamed particle tiles have evicted from L1 costs a round trip to L2 in
+// the middle of a dependent chain.
+__device__ __forceinline__ const FilterDesc& load_desc(FilterDesc& sd, const FilterDesc* g)
+{
+    static_assert(sizeof(FilterDesc) % 8 == 0, "descriptor copied in 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(g);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+    for (int i = threadIdx.x; i < (int)(sizeof(FilterDesc) / 8); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    return sd;
+}
 
 // Register budgets of the split pipeline's kernels, as resident warps per SM
 // asked of the compiler: __launch_bounds__(threads, ceil(warps * 32 / threads))
@@ -236,9 +256,10 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     __shared__ typename Mdl::Consts cst;
     __shared__ double red[(NT / 32) * (1 + S + NANG)];
     __shared__ float s_lmax;
+    __shared__ FilterDesc sdesc;
     int f, b;
     cta_target(cta_map, f, b);
-    const FilterDesc& D = descs[f];
+    const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
@@ -258,7 +279,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     float* sk = reinterpret_cast<float*>(p);
     int* si = reinterpret_cast<int*>(p + (size_t)M * 4);
 
-    if (tid == 0) Mdl::prepare(cst, *input_of(in, f), D.mp);
+    if (tid < 32) Mdl::prepare(cst, *input_of(in, f), D.mp, tid);
     if constexpr (FR) {
         uint32_t* gst = D.mtgp + (int64_t)b * kMtgpN;
         mtgp_load(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, true);
@@ -335,13 +356,14 @@ __global__ void __launch_bounds__(M / E) k_sample_weight(const FilterDesc* __res
     constexpr int S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
     constexpr int NANG = NA > 0 ? NA : 1;
     __shared__ typename Mdl::Consts cst;
+    __shared__ FilterDesc sdesc;
     int f, b;
     cta_target(cta_map, f, b);
-    const FilterDesc& D = descs[f];
+    const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
-    if (tid == 0) Mdl::prepare(cst, *input_of(in, f), D.mp);
+    if (tid < 32) Mdl::prepare(cst, *input_of(in, f), D.mp, tid);
     __syncthreads();
     float st[E][S];
 #pragma unroll
@@ -380,9 +402,10 @@ __global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restri
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double red[(NT / 32) * (1 + S + NANG)];
     __shared__ float s_lmax;
+    __shared__ FilterDesc sdesc;
     int f, b;
     cta_target(cta_map, f, b);
-    const FilterDesc& D = descs[f];
+    const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
@@ -684,6 +707,45 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Bulk copies global -> shared through the TMA engine (cp.async.bulk, no
+// multicast), completion counted in bytes on a shared-memory mbarrier.  Both
+// addresses 16-byte aligned, sizes multiples of 16.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init_expect(uint64_t* mbar, unsigned bytes)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
+                 "fence.mbarrier_init.release.cluster;\n"
+                 "fence.proxy.async.shared::cta;\n"
+                 "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+                 : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier, at most `limit` polls (each
+// try_wait may suspend the thread for a while); false when they ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity, int limit = 1 << 18)
+{
+    const unsigned a = smem_u32(mbar);
+    for (int i = 0; i < limit; ++i) {
+        unsigned done;
+        asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // Resampling of sub-filter b from a sorted copy (src_tmp, src_key: this
 // filter's arrays, sorted per sub-filter) with the exchange applied virtually
 // (nx weakest slots take the neighbours' top-t, read from the same sorted
@@ -699,7 +761,7 @@ template <int S, int M, int E, int RES>
 __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const float* __restrict__ src_tmp,
                                               const float* __restrict__ src_key, const float* __restrict__ U,
                                               int nx, unsigned char* smem, double* dred, int* ired,
-                                              float (&st)[E][S], int (&sel)[E])
+                                              uint64_t* mbar, float (&st)[E][S], int (&sel)[E])
 {
     const int tid = threadIdx.x;
     const int64_t T = D.T;
@@ -727,7 +789,62 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
     const bool xch = E * tid + E - 1 >= M - nx;  // this thread owns slots in the exchange range
-    if constexpr (S <= 3) {
+    const bool bulk = ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
+                        (uintptr_t)(T * 4)) & 15) == 0;
+    if (bulk) {
+        // the sub-filter's sorted keys and state rows by bulk copies (one
+        // thread issues them), the exchanged slots patched by their owners
+        // once the rows landed
+        if (tid == 0) {
+            mbar_init_expect(mbar, (unsigned)((1 + S) * M * 4));
+            bulk_g2s(kb, src_key + (int64_t)b * M, M * 4, mbar);
+#pragma unroll
+            for (int v = 0; v < S; ++v) bulk_g2s(tile + v * M, src_tmp + v * T + (int64_t)b * M, M * 4, mbar);
+        }
+        constexpr int XS = S <= 3 ? S : 1;
+        float xk[E], xs[E][XS];
+        if constexpr (S <= 3) {
+            // small states: the neighbours' values into registers while the rows are in flight
+            if (xch) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int x = M - 1 - (E * tid + e);
+                    if (x < nx) {
+                        const int64_t g = exchange_source(D, b, x);
+                        xk[e] = src_key[g];
+#pragma unroll
+                        for (int v = 0; v < XS; ++v) xs[e][v] = src_tmp[v * T + g];
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the mbarrier is initialised
+        bool ok = mbar_wait(mbar, 0);
+        if (!ok) {
+            ok = mbar_wait(mbar, 0);  // the copies in flight, once more
+            if (tid == 0 && D.status) atomicOr(D.status, PF_STATUS_WAIT_TIMEOUT);
+            if (!ok) return false;
+        }
+        if (dec_u - 1.0f > D.freq) return false;
+        if (xch) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int x = M - 1 - (E * tid + e);
+                if (x < nx) {
+                    if constexpr (S <= 3) {
+                        kb[E * tid + e] = xk[e];
+#pragma unroll
+                        for (int v = 0; v < XS; ++v) tile[v * M + E * tid + e] = xs[e][v];
+                    } else {
+                        const int64_t g = exchange_source(D, b, x);
+                        kb[E * tid + e] = src_key[g];
+#pragma unroll
+                        for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = src_tmp[v * T + g];
+                    }
+                }
+            }
+        }
+    } else if constexpr (S <= 3) {
         // small states: through registers
         float okey[E], ost[S][E];
         ldv<E>(src_key + base, okey);
@@ -820,11 +937,10 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
         const double tot = scan_f64<M, E>(w, cum, dred);
         const float u0 = ur[0] - 1.0f;
         const double step = tot / (double)M;
+        double pos[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const double pos = ((double)u0 + (double)(E * tid + e)) * step;
-            sel[e] = upper_count<M>(cum, pos);
-        }
+        for (int e = 0; e < E; ++e) pos[e] = ((double)u0 + (double)(E * tid + e)) * step;
+        upper_counts<M, E>(cum, pos, sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(scratch);
 #pragma unroll
@@ -866,7 +982,9 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
         f = 0;
         b = leaders_first(blockIdx.x, descs[0].N);
     }
-    const FilterDesc& D = descs[f];
+    __shared__ FilterDesc sdesc;
+    __shared__ uint64_t mbar;
+    const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     estimate_groups<S>(D, b, in, step_ctr);
     const int64_t T = D.T;
@@ -879,7 +997,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
     }
     float st[E][S];
     int sel[E];
-    if (!resample_from<S, M, E, RES>(D, b, D.tmp, D.tkey, U, nx, smem, dred, ired, st, sel)) {
+    if (!resample_from<S, M, E, RES>(D, b, D.tmp, D.tkey, U, nx, smem, dred, ired, &mbar, st, sel)) {
         if (D.sel) {
 #pragma unroll
             for (int e = 0; e < E; ++e) D.sel[base + e] = -1;
@@ -941,8 +1059,10 @@ __global__ void __launch_bounds__(M / E) k_test_resample(const float* w_in, cons
         const double tot = scan_f64<M, E>(w, cum, dred);
         const float u0 = u[b];
         const double step = tot / (double)M;
+        double pos[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) sel[e] = upper_count<M>(cum, ((double)u0 + (double)(E * tid + e)) * step);
+        for (int e = 0; e < E; ++e) pos[e] = ((double)u0 + (double)(E * tid + e)) * step;
+        upper_counts<M, E>(cum, pos, sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(smem);
 #pragma unroll
@@ -975,7 +1095,7 @@ __global__ void k_test_model(ModelParams mp, const pf_step_input* in, int n, flo
                              float* ll)
 {
     __shared__ typename Mdl::Consts cst;
-    if (threadIdx.x == 0) Mdl::prepare(cst, *in, mp);
+    if (threadIdx.x < 32) Mdl::prepare(cst, *in, mp, threadIdx.x);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;

@@ -59,11 +59,17 @@ __global__ void k_srv_expand(const Pending* __restrict__ pend, const pf_step_inp
     for (int w = threadIdx.x; w < (int)(sizeof(pf_step_input) / 4); w += blockDim.x) dst[w] = src[w];
 }
 
+// Block i copies pending update i's estimate to out[i]; block n copies the
+// kernels' status word into out[n] (so one D2H copy brings both back).
 __global__ void k_srv_gather(const Pending* __restrict__ pend, int n, const pf_estimate* __restrict__ est_tab,
-                             pf_estimate* __restrict__ out)
+                             pf_estimate* __restrict__ out, const int32_t* __restrict__ status)
 {
     const int i = blockIdx.x;
-    if (i >= n) return;
+    if (i == n) {
+        if (threadIdx.x == 0) *reinterpret_cast<int32_t*>(out + n) = *status;
+        return;
+    }
+    if (i > n) return;
     const uint32_t* src = reinterpret_cast<const uint32_t*>(est_tab + pend[i].slot);
     uint32_t* dst = reinterpret_cast<uint32_t*>(out + i);
     for (int w = threadIdx.x; w < (int)(sizeof(pf_estimate) / 4); w += blockDim.x) dst[w] = src[w];
@@ -152,6 +158,7 @@ struct pf_server {
     Pending* d_pend = nullptr;
     pf_step_input* d_in = nullptr;
     pf_estimate* d_out = nullptr;
+    int32_t* d_status = nullptr;  // PF_STATUS_* bits set by the kernels
     // pinned staging
     Pending* h_pend = nullptr;
     pf_step_input* h_in = nullptr;
@@ -173,7 +180,7 @@ static void srv_release(pf_server* s)
     for (int m = 0; m < 3; ++m)
         if (s->d_map[m]) cudaFreeAsync(s->d_map[m], s->stream);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* dev[] = {s->d_desc, s->d_slot_in, s->d_est_tab, s->d_pend, s->d_in, s->d_out};
+    void* dev[] = {s->d_desc, s->d_slot_in, s->d_est_tab, s->d_pend, s->d_in, s->d_out, s->d_status};
     for (void* p : dev)
         if (p) cudaFree(p);
     void* host[] = {s->h_pend, s->h_in, s->h_out};
@@ -255,10 +262,12 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     STRY(cudaMalloc(&s->d_est_tab, sizeof(pf_estimate) * max_filters));
     STRY(cudaMalloc(&s->d_pend, sizeof(Pending) * max_filters));
     STRY(cudaMalloc(&s->d_in, sizeof(pf_step_input) * max_filters));
-    STRY(cudaMalloc(&s->d_out, sizeof(pf_estimate) * max_filters));
+    STRY(cudaMalloc(&s->d_out, sizeof(pf_estimate) * (max_filters + 1)));
+    STRY(cudaMalloc(&s->d_status, sizeof(int32_t)));
+    STRY(cudaMemset(s->d_status, 0, sizeof(int32_t)));
     STRY(cudaMallocHost(&s->h_pend, sizeof(Pending) * max_filters));
     STRY(cudaMallocHost(&s->h_in, sizeof(pf_step_input) * max_filters));
-    STRY(cudaMallocHost(&s->h_out, sizeof(pf_estimate) * max_filters));
+    STRY(cudaMallocHost(&s->h_out, sizeof(pf_estimate) * (max_filters + 1)));
 #undef STRY
     {
         const pf_status ms = ensure_map(s, 1 << 20);  // 8 MB per model: a few growths at most afterwards
@@ -396,6 +405,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     D.ru = reinterpret_cast<float*>(base + L.ru);
     D.gpart = reinterpret_cast<double*>(base + L.gpart);
     D.est_ctr = reinterpret_cast<int32_t*>(base + L.est_ctr);
+    D.status = s->d_status;
     const int slot = s->free_slots.back();
     D.est = s->d_est_tab + slot;
     D.N = N;
@@ -552,9 +562,9 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     }
     for (int m = 0; m < 3; ++m)
         if (used[m]) CU(cudaStreamWaitEvent(st, s->join[m], 0));
-    k_srv_gather<<<n, 64, 0, st>>>(s->d_pend, n, s->d_est_tab, s->d_out);
+    k_srv_gather<<<n + 1, 64, 0, st>>>(s->d_pend, n, s->d_est_tab, s->d_out, s->d_status);
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(pf_estimate) * n, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(s->h_out, s->d_out, sizeof(pf_estimate) * n + sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CU(cudaEventRecord(s->done, st));
     s->busy = true;
     s->launches++;
@@ -580,6 +590,9 @@ extern "C" pf_status pf_server_poll(pf_server* s, int32_t wait, pf_server_result
     }
     const int nb = (int)s->batch_slots.size();
     if (cap < nb) return fail(PF_ERR_INVALID, "result buffer holds %d, the batch has %d", cap, nb);
+    if (*reinterpret_cast<const int32_t*>(s->h_out + nb) & PF_STATUS_WAIT_TIMEOUT)
+        return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
+                                    "propagated particles)");
     for (int i = 0; i < nb; ++i) {
         Slot& sl = s->slots[s->batch_slots[i]];
         sl.in_flight = false;

@@ -43,7 +43,9 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     __shared__ double dred[33];
     __shared__ int ired[34];
     __shared__ float s_lmax;
-    const FilterDesc& D = descs[0];
+    __shared__ uint64_t mbar;
+    __shared__ FilterDesc sdesc;
+    const FilterDesc& D = load_desc(sdesc, descs);
     const int b = blockIdx.x;
     const int tid = threadIdx.x;
     const int64_t T = D.T;
@@ -55,7 +57,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     const float* prev_tmp = par ? D.tmp : X.tmp2;
     const float* prev_key = par ? D.tkey : X.tkey2;
     float* ru = D.ru + (int64_t)b * D.ru_stride;
-    if (tid == 0) Mdl::prepare(cst, *input_of(in, 0), D.mp);
+    if (tid < 32) Mdl::prepare(cst, *input_of(in, 0), D.mp, tid);
 
     // ---- R
     float st[E][S];
@@ -63,7 +65,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     if (!init) {
         int sel[E];
         resampled = resample_from<S, M, E, RES>(D, b, prev_tmp, prev_key, ru, exchange_count(D), smem, dred,
-                                                ired, st, sel);
+                                                ired, &mbar, st, sel);
         if (D.sel) {
 #pragma unroll
             for (int e = 0; e < E; ++e) D.sel[base + e] = resampled ? sel[e] : -1;
@@ -162,7 +164,9 @@ __global__ void __launch_bounds__(M / E) k_resample_only_cta(const FilterDesc* _
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double dred[33];
     __shared__ int ired[34];
-    const FilterDesc& D = descs[0];
+    __shared__ uint64_t mbar;
+    __shared__ FilterDesc sdesc;
+    const FilterDesc& D = load_desc(sdesc, descs);
     if (*X.need_init) return;  // `state` already holds the particles
     const int b = blockIdx.x;
     const int64_t base = (int64_t)b * M + E * threadIdx.x;
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(M / E) k_resample_only_cta(const FilterDesc* _
     float st[E][S];
     int sel[E];
     const bool resampled =
-        resample_from<S, M, E, RES>(D, b, t_tmp, t_key, ru, exchange_count(D), smem, dred, ired, st, sel);
+        resample_from<S, M, E, RES>(D, b, t_tmp, t_key, ru, exchange_count(D), smem, dred, ired, &mbar, st, sel);
     if (D.sel) {
 #pragma unroll
         for (int e = 0; e < E; ++e) D.sel[base + e] = resampled ? sel[e] : -1;

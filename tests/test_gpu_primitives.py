@@ -99,6 +99,24 @@ def test_resamplers_vs_oracle_other_sizes(gpu, O, m, ppt):
     assert np.array_equal(gpu.resample(2, w, uv, m, ppt), O.resample(2, w, uv, m, ppt))
 
 
+@pytest.mark.parametrize("m,ppt", [(64, 2), (256, 8), (512, 4), (512, 16), (1024, 4)])
+def test_systematic_search_jumps(gpu, O, m, ppt):
+    """Systematic selection where a thread's consecutive positions cross many
+    cumulative-sum entries (spikes among zeros, geometric and heavy-tailed
+    weights) or none (all weight on one particle)."""
+    rng = np.random.default_rng(7 * m + ppt)
+    w = np.zeros((7, m), np.float32)
+    w[0, rng.choice(m, 3, replace=False)] = [1.0, 5.0, 0.5]
+    w[1] = 0.5 ** np.arange(m, dtype=np.float64)
+    w[2, m // 2] = 1.0
+    w[3] = 1.0
+    w[4] = rng.exponential(1, m) ** 8
+    w[5, -1] = 1e-30
+    w[6, ::17] = rng.random(len(w[6, ::17]))
+    us = rng.random(7).astype(np.float32)
+    assert np.array_equal(gpu.resample(1, w.ravel(), us, m, ppt), O.resample(1, w.ravel(), us, m, ppt))
+
+
 @pytest.mark.parametrize("tag", ["1_8_32_3", "2_2048_512_2", "2_1024_256_1", "2_12_64_4", "3_16_64_5"])
 def test_exchange_routing_bit_exact(gpu, golden, tag):
     mode, N, m, t = map(int, tag.split("_"))
