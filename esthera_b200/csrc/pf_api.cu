@@ -688,7 +688,9 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
         // with an exchange period every CTA of the resampling kernel reads the
         // step counter, so it advances in a launch of its own after the kernel
         const bool late = ctr_inc && c.exchange_period > 1;
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, 1));
+        // launched as a programmatic dependent of the sampling kernel (its CTAs
+        // start during the sampling kernel's last wave and wait there)
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, 3));
         CU(mark("exchange_resample"));
         if (late) CU(launch_counter_inc(ctr_inc, st));
     } else {

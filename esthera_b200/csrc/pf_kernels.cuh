@@ -71,6 +71,14 @@ __device__ __forceinline__ const FilterDesc& load_desc(FilterDesc& sd, const Fil
     return sd;
 }
 
+// Programmatic dependent launch (split pipeline): the sampling kernel lets the
+// resampling kernel's CTAs launch once all of its own CTAs are running, and
+// those wait in wait_prerequisites() -- after their prologue -- until the
+// sampling kernel has completed and its writes are visible.  Both are no-ops
+// for kernels launched without the programmatic attribute.
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void wait_prerequisites() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // Register budgets of the split pipeline's kernels, as resident warps per SM
 // asked of the compiler: __launch_bounds__(threads, ceil(warps * 32 / threads))
 // caps the registers at 65536 / (that many threads).  Small states (the
@@ -259,6 +267,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     __shared__ FilterDesc sdesc;
     int f, b;
     cta_target(cta_map, f, b);
+    allow_dependents();
     const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     const int64_t T = D.T;
@@ -717,6 +726,7 @@ __device__ __forceinline__ void mbar_init_expect(uint64_t* mbar, unsigned bytes)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n"
                  "fence.mbarrier_init.release.cluster;\n"
                  "fence.proxy.async.shared::cta;\n"
+                 "fence.proxy.async.global;\n"
                  "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(mbar)),
                  "r"(bytes)
                  : "memory");
@@ -986,6 +996,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
     __shared__ uint64_t mbar;
     const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
+    wait_prerequisites();
     estimate_groups<S>(D, b, in, step_ctr);
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;

@@ -42,7 +42,20 @@ cudaError_t Launch<Mdl>::sample_sort(int M, int E, bool fr, int grid, cudaStream
         constexpr size_t sm = k2_smem<Mdl::S, m, e, RES>();                \
         cudaError_t r = allow_smem(fn, sm);                                \
         if (r != cudaSuccess) return r;                                    \
-        fn<<<grid, m / e, sm, st>>>(d, map, in, ctr, virt);                \
+        if (virt & 2) { /* programmatic dependent of the sampling kernel */ \
+            cudaLaunchConfig_t lc = {};                                    \
+            lc.gridDim = dim3(grid);                                       \
+            lc.blockDim = dim3(m / e);                                     \
+            lc.dynamicSmemBytes = sm;                                      \
+            lc.stream = st;                                                \
+            cudaLaunchAttribute at[1];                                     \
+            at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization; \
+            at[0].val.programmaticStreamSerializationAllowed = 1;          \
+            lc.attrs = at;                                                 \
+            lc.numAttrs = 1;                                               \
+            return cudaLaunchKernelEx(&lc, fn, d, map, in, ctr, virt & 1); \
+        }                                                                  \
+        fn<<<grid, m / e, sm, st>>>(d, map, in, ctr, virt & 1);            \
         return cudaGetLastError();                                         \
     }
 #define PF_K2_CASE_0(m, e) PF_K2_CASE(m, e, 0)
