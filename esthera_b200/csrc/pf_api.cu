@@ -86,6 +86,21 @@ bool pfhost::model_info(int model, ModelInfo* mi)
     return false;
 }
 
+bool pfhost::dependent_launch_pays(int grid, int M, int E, int S, int device)
+{
+    static int sms[64] = {};  // SM count per device, read once
+    if (device < 0 || device >= 64) return false;
+    if (sms[device] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        sms[device] = n;
+    }
+    return grid > sms[device] * pf_min_blocks(M / E, pf_k1_warps(S));
+}
+
 extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, int32_t* C, int32_t* Z)
 {
     ModelInfo mi;
@@ -688,9 +703,10 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
         // with an exchange period every CTA of the resampling kernel reads the
         // step counter, so it advances in a launch of its own after the kernel
         const bool late = ctr_inc && c.exchange_period > 1;
-        // launched as a programmatic dependent of the sampling kernel (its CTAs
-        // start during the sampling kernel's last wave and wait there)
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, 3));
+        // a programmatic dependent of the sampling kernel when that pays (its
+        // CTAs start during the sampling kernel's last wave and wait there)
+        const int virt = dependent_launch_pays(N, M, E, f->mi.S, c.device) ? 3 : 1;
+        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, virt));
         CU(mark("exchange_resample"));
         if (late) CU(launch_counter_inc(ctr_inc, st));
     } else {

@@ -175,7 +175,9 @@ static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRe
 {
     const int M = B->M, E = B->E;
     CU(B->ops.sample_sort(M, E, true, B->NS, B->stream, desc, B->map, in));
-    CU(B->ops.exchange_resample(M, E, B->cfg.resampler, B->NS, B->stream, desc, B->map, in, nullptr, 1));
+    // a programmatic dependent of the sampling kernel when that pays (starts in its last wave, waits for the grid)
+    const int virt = dependent_launch_pays((int)B->NS, M, E, B->mi.S, B->cfg.device) ? 3 : 1;
+    CU(B->ops.exchange_resample(M, E, B->cfg.resampler, B->NS, B->stream, desc, B->map, in, nullptr, virt));
     if (ctr_inc) CU(launch_counter_inc(ctr_inc, B->stream));
     return PF_OK;
 }

@@ -29,6 +29,13 @@ struct ModelInfo {
     size_t psize;
 };
 bool model_info(int model, ModelInfo* mi);
+
+// Whether to launch the resampling kernel as a programmatic dependent of the
+// sampling kernel: measured to pay when the sampling grid runs in more than
+// one wave (its CTAs start in the sampling kernel's last wave: 2^20 unicycle
+// particles, 67.0 -> 62.2 us per step) and to cost when it fits in one (2^18
+// DH-arm particles, 49.8 -> 58.3 us).
+bool dependent_launch_pays(int grid, int M, int E, int S, int device);
 const float* init_state_of(int model, const ModelParams& mp);
 uint32_t angle_mask_of(int model);
 int angle_count_of(int model);

@@ -799,8 +799,11 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
     const bool xch = E * tid + E - 1 >= M - nx;  // this thread owns slots in the exchange range
-    const bool bulk = ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
-                        (uintptr_t)(T * 4)) & 15) == 0;
+    // Bulk copies for small states (1 + S rows per sub-filter); the arm's 13
+    // rows ran slower as bulk copies issued by one thread than as per-thread
+    // cp.async (resampling kernel 34.4 vs 26.0 us at 2^18 particles).
+    const bool bulk = S <= 3 && ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
+                                  (uintptr_t)(T * 4)) & 15) == 0;
     if (bulk) {
         // the sub-filter's sorted keys and state rows by bulk copies (one
         // thread issues them), the exchanged slots patched by their owners

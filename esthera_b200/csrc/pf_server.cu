@@ -555,7 +555,10 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
         const ModelOps ops = model_ops(m);
         InputRef ir{s->d_slot_in, 1, nullptr, 0, 0};
         CU(ops.sample_sort(M, E, true, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir));
-        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir, nullptr, 1));
+        ModelInfo mi;
+        model_info(m, &mi);
+        const int virt = dependent_launch_pays((int)ctas[m], M, E, mi.S, s->device) ? 3 : 1;
+        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir, nullptr, virt));
         CU(cudaEventRecord(s->join[m], ms));
         used[m] = true;
         first += cnt;
