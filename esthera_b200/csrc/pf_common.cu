@@ -198,7 +198,7 @@ static cudaError_t test_resample_res(int M, int E, int nsub, const float* w, con
 {
 #define PF_TR(m, e)                                                                          \
     if (M == m && E == e) {                                                                  \
-        constexpr size_t sm = RES == PF_RESAMPLE_SYSTEMATIC ? (size_t)m * 8                  \
+        constexpr size_t sm = RES == PF_RESAMPLE_SYSTEMATIC ? (size_t)m * 12                 \
                             : (RES == PF_RESAMPLE_REFERENCE ? (size_t)m * 4 : (size_t)m * 16); \
         k_test_resample<m, e, RES><<<nsub, m / e, sm, st>>>(w, u, sel, prob, alias);         \
         return cudaGetLastError();                                                           \

@@ -361,41 +361,43 @@ __device__ __forceinline__ int upper_count(const double* cum, double x)
     return lo < M ? lo : M - 1;
 }
 
-// upper_count for E increasing positions x[0] <= x[1] <= ... (a thread's
-// consecutive systematic positions): a full binary search for x[0], then from
-// the previous count forward -- at most 4 single steps (the usual advance is
-// about one entry per position), else a binary search of the rest.  Same
-// results as upper_count on each position (cum is non-decreasing).
+// Systematic selection from the inclusive sums cum[0..M) by interval
+// boundaries: input j is selected by the outputs i with
+// cum[j-1] <= pos(i) < cum[j], pos(i) = (u0 + i) * step (cum[-1] = -inf; the
+// last input also takes every output with pos(i) >= cum[M-1]).  Each thread
+// finds, for its E inputs j = E*tid+e, the first output at or above cum[j-1]
+// (an estimate from t / step, corrected with the exact pos(i) comparisons),
+// writes its inputs' runs of outputs to sidx[0..M), and reads back its own E
+// outputs.  pos(i) and the comparisons are those of upper_count(cum, pos(i)),
+// so every output selects the same input (pos is non-decreasing in i).
+// Synchronises the CTA.
 template <int M, int E>
-__device__ __forceinline__ void upper_counts(const double* cum, const double (&x)[E], int (&out)[E])
+__device__ __forceinline__ void systematic_select(const double* cum, float u0f, double step, int* sidx,
+                                                  int (&sel)[E])
 {
-    int lo = 0, hi = M;
+    const int tid = threadIdx.x;
+    const double u0 = (double)u0f;
+    const double inv = step > 0.0 ? 1.0 / step : 0.0;
+    auto pos = [&](int i) { return (u0 + (double)i) * step; };
+    auto first_at_or_above = [&](double t) {  // first i in [0, M] with pos(i) >= t
+        const double est = ceil(t * inv - u0);
+        int i = est >= 0.0 ? (est <= (double)M ? (int)est : M) : 0;
+        while (i > 0 && pos(i - 1) >= t) --i;
+        while (i < M && pos(i) < t) ++i;
+        return i;
+    };
+    const int j0 = E * tid;
+    int lo = j0 == 0 ? 0 : first_at_or_above(cum[j0 - 1]);
 #pragma unroll
-    for (int it = 0; it < 11; ++it) {
-        if (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (cum[mid] <= x[0]) lo = mid + 1;
-            else hi = mid;
-        }
+    for (int e = 0; e < E; ++e) {
+        const int j = j0 + e;
+        const int hi = j == M - 1 ? M : first_at_or_above(cum[j]);
+        for (int i = lo; i < hi; ++i) sidx[i] = j;
+        lo = hi > lo ? hi : lo;
     }
-    out[0] = lo < M ? lo : M - 1;
+    __syncthreads();
 #pragma unroll
-    for (int e = 1; e < E; ++e) {
-        int n = 0;
-        while (n < 4 && lo < M && cum[lo] <= x[e]) {
-            ++lo;
-            ++n;
-        }
-        if (n == 4 && lo < M && cum[lo] <= x[e]) {
-            hi = M;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (cum[mid] <= x[e]) lo = mid + 1;
-                else hi = mid;
-            }
-        }
-        out[e] = lo < M ? lo : M - 1;
-    }
+    for (int e = 0; e < E; ++e) sel[e] = sidx[E * tid + e];
 }
 
 // FP32 Blelloch exclusive scan of M values in place (prefix_sum,

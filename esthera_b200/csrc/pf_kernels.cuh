@@ -948,12 +948,8 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(scratch);
         const double tot = scan_f64<M, E>(w, cum, dred);
-        const float u0 = ur[0] - 1.0f;
-        const double step = tot / (double)M;
-        double pos[E];
-#pragma unroll
-        for (int e = 0; e < E; ++e) pos[e] = ((double)u0 + (double)(E * tid + e)) * step;
-        upper_counts<M, E>(cum, pos, sel);
+        // the keys were read into w before the scan's barriers: kb holds the output runs
+        systematic_select<M, E>(cum, ur[0] - 1.0f, tot / (double)M, reinterpret_cast<int*>(kb), sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(scratch);
 #pragma unroll
@@ -1071,12 +1067,7 @@ __global__ void __launch_bounds__(M / E) k_test_resample(const float* w_in, cons
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(smem);
         const double tot = scan_f64<M, E>(w, cum, dred);
-        const float u0 = u[b];
-        const double step = tot / (double)M;
-        double pos[E];
-#pragma unroll
-        for (int e = 0; e < E; ++e) pos[e] = ((double)u0 + (double)(E * tid + e)) * step;
-        upper_counts<M, E>(cum, pos, sel);
+        systematic_select<M, E>(cum, u[b], tot / (double)M, reinterpret_cast<int*>(cum + M), sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(smem);
 #pragma unroll
