@@ -799,35 +799,35 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
     float* tile = kb + M;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(tile + (size_t)S * M);
     const bool xch = E * tid + E - 1 >= M - nx;  // this thread owns slots in the exchange range
-    // Bulk copies for small states (1 + S rows per sub-filter); the arm's 13
-    // rows ran slower as bulk copies issued by one thread than as per-thread
-    // cp.async (resampling kernel 34.4 vs 26.0 us at 2^18 particles).
-    const bool bulk = S <= 3 && ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
-                                  (uintptr_t)(T * 4)) & 15) == 0;
-    if (bulk) {
-        // the sub-filter's sorted keys and state rows by bulk copies (one
-        // thread issues them), the exchanged slots patched by their owners
-        // once the rows landed
+    if constexpr (S <= 3) {
+        // Small states: the sub-filter's sorted keys and state rows by bulk
+        // copies (one thread issues them), the exchanged slots patched by
+        // their owners once the rows landed.  (The arm's 13 rows ran slower as
+        // bulk copies issued by one thread than as per-thread cp.async:
+        // resampling kernel 34.4 vs 26.0 us at 2^18 particles.)
+        const bool bulk = ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
+                            (uintptr_t)(T * 4)) & 15) == 0;
+        if (!bulk) {  // rows not 16-byte aligned: not this library's allocations
+            if (tid == 0 && D.status) atomicOr(D.status, PF_STATUS_WAIT_TIMEOUT);
+            return false;
+        }
         if (tid == 0) {
             mbar_init_expect(mbar, (unsigned)((1 + S) * M * 4));
             bulk_g2s(kb, src_key + (int64_t)b * M, M * 4, mbar);
 #pragma unroll
             for (int v = 0; v < S; ++v) bulk_g2s(tile + v * M, src_tmp + v * T + (int64_t)b * M, M * 4, mbar);
         }
-        constexpr int XS = S <= 3 ? S : 1;
-        float xk[E], xs[E][XS];
-        if constexpr (S <= 3) {
-            // small states: the neighbours' values into registers while the rows are in flight
-            if (xch) {
+        // the neighbours' values into registers while the rows are in flight
+        float xk[E], xs[E][S];
+        if (xch) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const int x = M - 1 - (E * tid + e);
-                    if (x < nx) {
-                        const int64_t g = exchange_source(D, b, x);
-                        xk[e] = src_key[g];
+            for (int e = 0; e < E; ++e) {
+                const int x = M - 1 - (E * tid + e);
+                if (x < nx) {
+                    const int64_t g = exchange_source(D, b, x);
+                    xk[e] = src_key[g];
 #pragma unroll
-                        for (int v = 0; v < XS; ++v) xs[e][v] = src_tmp[v * T + g];
-                    }
+                    for (int v = 0; v < S; ++v) xs[e][v] = src_tmp[v * T + g];
                 }
             }
         }
@@ -844,44 +844,12 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
             for (int e = 0; e < E; ++e) {
                 const int x = M - 1 - (E * tid + e);
                 if (x < nx) {
-                    if constexpr (S <= 3) {
-                        kb[E * tid + e] = xk[e];
+                    kb[E * tid + e] = xk[e];
 #pragma unroll
-                        for (int v = 0; v < XS; ++v) tile[v * M + E * tid + e] = xs[e][v];
-                    } else {
-                        const int64_t g = exchange_source(D, b, x);
-                        kb[E * tid + e] = src_key[g];
-#pragma unroll
-                        for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = src_tmp[v * T + g];
-                    }
+                    for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = xs[e][v];
                 }
             }
         }
-    } else if constexpr (S <= 3) {
-        // small states: through registers
-        float okey[E], ost[S][E];
-        ldv<E>(src_key + base, okey);
-#pragma unroll
-        for (int v = 0; v < S; ++v) ldv<E>(src_tmp + v * T + base, ost[v]);
-        if (xch) {
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const int x = M - 1 - (E * tid + e);
-                if (x < nx) {
-                    const int64_t g = exchange_source(D, b, x);
-                    okey[e] = src_key[g];
-#pragma unroll
-                    for (int v = 0; v < S; ++v) ost[v][e] = src_tmp[v * T + g];
-                }
-            }
-        }
-        if (dec_u - 1.0f > D.freq) return false;
-#pragma unroll
-        for (int e = 0; e < E; ++e) kb[E * tid + e] = okey[e];
-#pragma unroll
-        for (int v = 0; v < S; ++v)
-#pragma unroll
-            for (int e = 0; e < E; ++e) tile[v * M + E * tid + e] = ost[v][e];
     } else {
         // large states: straight into shared memory (cp.async), the
         // exchanged slots overwritten by their owner once its copies landed
