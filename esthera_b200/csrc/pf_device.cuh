@@ -566,6 +566,50 @@ __device__ void vose_build(const float (&w)[E], float* prob, unsigned* alias, un
                     const unsigned aa = sen - sb, bb = (unsigned)M - sen;
                     const unsigned na = aa < bb ? aa : bb;
                     if (na == 0 || na > 32) break;
+                    if (bb == 1) {
+                        // One large entry left: every further round pairs it with the
+                        // next small one until its probability drops to <= 1 (it then
+                        // joins the small list and the pairing ends) or the smalls run
+                        // out.  Lane 0 runs those rounds back to back: the same pairs,
+                        // arithmetic and list updates as one round at a time.
+                        if (lane == 0) {
+                            const unsigned L = sl[sen];
+                            float pl = prob[L];
+                            bool to_small = false;
+                            while (sb < sen && rr < M) {
+                                unsigned sm[4];
+                                float ps[4];
+                                const unsigned left = sen - sb;
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    sm[q] = (unsigned)q < left ? sl[sb + q] : 0u;
+                                    ps[q] = (unsigned)q < left ? prob[sm[q]] : 0.0f;
+                                }
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    if (!to_small && (unsigned)q < left && rr < M) {
+                                        alias[sm[q]] = L;
+                                        pl = (pl + ps[q]) - 1.0f;
+                                        ++sb;
+                                        ++rr;
+                                        to_small = pl <= 1.0f;
+                                    }
+                                }
+                                if (to_small) break;
+                            }
+                            prob[L] = pl;
+                            if (to_small) {
+                                ++sen;  // sl[sen] already holds L: it becomes the last small entry
+                                ++lr;
+                            }
+                        }
+                        sb = __shfl_sync(kFull, sb, 0);
+                        sen = __shfl_sync(kFull, sen, 0);
+                        lr = __shfl_sync(kFull, lr, 0);
+                        rr = __shfl_sync(kFull, rr, 0);
+                        __syncwarp();
+                        break;
+                    }
                     lr += na;
                     const bool act = (unsigned)lane < na;
                     unsigned li = 0;
