@@ -120,6 +120,7 @@ def _declare(L):
         "pf_run_device": (C.c_int, [P, P, P, C.c_int32, C.c_int32]),
         "pf_run_device_continue": (C.c_int, [P, C.c_int32]),
         "pf_step_submit": (C.c_int, [P, P]),
+        "pfk_bounded_wait_test": (C.c_int, [C.c_int32, P]),
         "pf_step_collect": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
         "pf_synchronize": (C.c_int, [P]),
         "pf_stream": (P, [P]),
@@ -650,6 +651,13 @@ def boxmuller(data, n=None):
         a = np.concatenate([a, np.zeros(2 * ((n + 1) // 2) - len(a), np.float32)])
     check(lib().pfk_boxmuller(_fptr(a), n))
     return a
+
+
+def bounded_wait_test(limit=2000):
+    """Run the bounded mbarrier wait on a phase nothing completes; returns the kernel's status (1: ran out)."""
+    st = C.c_int32(-1)
+    check(lib().pfk_bounded_wait_test(int(limit), C.byref(st)))
+    return st.value
 
 
 def bitonic_sort(keys, m, ppt=0):

@@ -1050,6 +1050,18 @@ extern "C" pf_status pfk_mtgp_generate(int32_t G, uint32_t seed, uint32_t mask, 
     return PF_OK;
 }
 
+extern "C" pf_status pfk_bounded_wait_test(int32_t limit, int32_t* status)
+{
+    if (!status || limit < 1 || limit > (1 << 20)) return fail(PF_ERR_INVALID, "bad argument");
+    TRYS(require_gpu(0));
+    DevBuf d;
+    TRYS(dev_buf(d, 4));
+    CU(cudaMemset(d.p, 0xff, 4));
+    CU(launch_test_bounded_wait(limit, (int32_t*)d.p, 0));
+    CU(cudaMemcpy(status, d.p, 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
 extern "C" pf_status pfk_boxmuller(float* data, int64_t n)
 {
     if (!data || n < 0) return fail(PF_ERR_INVALID, "bad argument");

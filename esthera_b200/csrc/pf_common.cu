@@ -288,6 +288,24 @@ cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaS
     return cudaGetLastError();
 }
 
+// The bounded mbarrier wait of the resampling kernels on a phase that nothing
+// completes (initialised for one arrival that never comes): the wait gives up
+// after `limit` polls and the kernel reports PF_STATUS_WAIT_TIMEOUT in *status.
+__global__ void k_test_bounded_wait(int limit, int32_t* status)
+{
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar)) : "memory");
+    __syncthreads();
+    const bool ok = mbar_wait(&mbar, 0, limit);
+    if (threadIdx.x == 0) *status = ok ? 0 : PF_STATUS_WAIT_TIMEOUT;
+}
+
+cudaError_t launch_test_bounded_wait(int limit, int32_t* status, cudaStream_t st)
+{
+    k_test_bounded_wait<<<1, 32, 0, st>>>(limit, status);
+    return cudaGetLastError();
+}
+
 // A run's device step counter, advanced (or set) by a launch of its own once
 // every kernel of the step that reads it is enqueued before it.
 __global__ void k_counter_update(int32_t* ctr, int32_t set, int32_t value)

@@ -76,6 +76,7 @@ cudaError_t launch_mtgp_init(uint32_t* states, int n, int g0, uint32_t seed, cud
 cudaError_t launch_a2a_merge(int nfilters, const FilterDesc* d, cudaStream_t st);
 cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStream_t st);
 cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st);
+cudaError_t launch_test_bounded_wait(int limit, int32_t* status, cudaStream_t st);
 cudaError_t launch_counter_inc(int32_t* ctr, cudaStream_t st);
 cudaError_t launch_counter_set(int32_t* ctr, int32_t value, cudaStream_t st);
 

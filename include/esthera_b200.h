@@ -385,6 +385,14 @@ pf_status pf_serve_load(const pf_config* filter_cfg, const pf_load_config* load,
  * Replaces mtgp32_uint32_kernel / mtgp32_single_kernel (mtgp32-cuda.cu:180-306). */
 pf_status pfk_mtgp_generate(int32_t G, uint32_t seed, uint32_t mask, int32_t kind,
                             int64_t per_stream, int32_t calls, uint32_t* out);
+/* Failure detection without a fault (no counterpart in the reference): one
+ * CTA waits, at most `limit` polls (1..2^20), on an mbarrier phase that
+ * nothing completes -- the bounded wait the resampling kernels use for their
+ * bulk copies -- and *status receives the kernel's report: 1 (the wait ran out;
+ * the kernels set the same bit in a filter's status word, which pf_step /
+ * pf_synchronize return as PF_ERR_TIMEOUT), 0 had it completed.  The context
+ * stays usable. */
+pf_status pfk_bounded_wait_test(int32_t limit, int32_t* status);
 /* In-place Box-Muller over pairs (2i, 2i+1), 2i < n (boxmuller, pf_generic_soa.cu:481-500).
  * data must hold 2*ceil(n/2) floats. */
 pf_status pfk_boxmuller(float* data, int64_t n);

@@ -63,6 +63,11 @@ def test_config_validation(E, kw, msg):
     assert msg in str(ei.value)
 
 
+def test_bounded_wait_argument_checks(E):
+    with pytest.raises(E.PFError):
+        E.bounded_wait_test(0)
+
+
 def test_no_cpu_fallback(E):
     if E.device_count() > 0:
         pytest.skip("a GPU is present")

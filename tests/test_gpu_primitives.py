@@ -186,3 +186,12 @@ def test_estimate_entry_point_vs_fp64(gpu, log_weights):
     ln = (keys.max() + np.log(W)) if log_weights else np.log(W)
     assert abs(e["log_norm"] - ln) < 1e-5 * abs(ln) + 1e-5
     assert e["best_subfilter"] == 5 and np.array_equal(e["best"][:3], st[:, 5 * m + 17])
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(gpu):
+    """A kernel's bounded wait on an mbarrier phase that nothing completes gives
+    up, reports the timeout bit, and the context stays usable afterwards."""
+    assert gpu.bounded_wait_test(2000) == 1
+    keys = np.arange(512, dtype=np.float32)[::-1].copy()
+    k, i = gpu.bitonic_sort(keys[::-1].copy(), 512, 4)
+    assert np.array_equal(k, keys) and np.array_equal(i, np.arange(512)[::-1])
