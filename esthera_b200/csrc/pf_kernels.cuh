@@ -534,13 +534,50 @@ __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, in
                                                int32_t step_no)
 {
     __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
+    constexpr int NVMAX = 2 + 2 * S;
+    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
+    // the winner's state first: its load overlaps the sums
+    const int bv = lane - PF_MAX_STATE;
+    const float best_v = (bv >= 0 && bv < S) ? __ldcg(best_src + bv * D.T + (int64_t)best * D.M) : 0.0f;
+    const bool batched = S <= 3 && ng <= 64;
+    if (batched) {
+        // small states: every group row of the lane (groups lane, lane + 32)
+        // in one batch of loads; the same sums, in the same order, as the
+        // general loop below
+        double acc[NVMAX];
+#pragma unroll
+        for (int j = 0; j < NVMAX; ++j) acc[j] = 0.0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int q = lane + 32 * r;
+            if (q < ng) {
+                const double* gq = D.gpart + (int64_t)q * kPartStride;
+                double v[NVMAX];
+#pragma unroll
+                for (int j = 0; j < NVMAX; ++j) v[j] = j < NV ? __ldcg(gq + j) : 0.0;
+                const double sq = D.log_weights ? exp(v[0] - gm) : 1.0;
+#pragma unroll
+                for (int j = 1; j < NVMAX; ++j)
+                    if (j < NV) acc[j] += sq * v[j];
+            }
+        }
+#pragma unroll
+        for (int j = 1; j < NVMAX; ++j) {
+            if (j < NV) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(kFull, acc[j], o);
+                if (lane == 0) s_acc[j] = acc[j];
+            }
+        }
+    }
     double sqv[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int q = lane + 32 * r;
-        sqv[r] = q < ng ? (D.log_weights ? exp(__ldcg(D.gpart + (int64_t)q * kPartStride) - gm) : 1.0) : 0.0;
+        sqv[r] = (!batched && q < ng) ? (D.log_weights ? exp(__ldcg(D.gpart + (int64_t)q * kPartStride) - gm) : 1.0)
+                                      : 0.0;
     }
-    for (int j0 = 1; j0 < NV; j0 += 4) {
+    for (int j0 = 1; j0 < NV && !batched; j0 += 4) {
         double a4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
@@ -567,7 +604,6 @@ __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, in
         }
     }
     __syncwarp();
-    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
     const double W = s_acc[1];
     if (lane < PF_MAX_STATE) {
         const int v = lane;
@@ -582,8 +618,7 @@ __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, in
         }
         E.mean[v] = m;
     } else {
-        const int v = lane - PF_MAX_STATE;
-        E.best[v] = v < S ? __ldcg(best_src + v * D.T + (int64_t)best * D.M) : 0.0f;
+        E.best[bv] = best_v;
     }
     if (lane == 0) {
         const double lg = D.log_weights ? gm : 0.0;
@@ -607,7 +642,13 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
     const int sb = b + lane;
     const bool valid = sb < D.N;
     const double* pp = D.part + (int64_t)(valid ? sb : b) * kPartStride;
-    double gl = valid ? pp[0] : -INFINITY;
+    // small states: the lane's whole partial row in one batch of loads (one
+    // round trip); large states read each value where it is used
+    constexpr int NROW = S <= 3 ? NVMAX : 1;
+    double row[NROW];
+#pragma unroll
+    for (int j = 0; j < NROW; ++j) row[j] = (valid && j < NV) ? pp[j] : 0.0;
+    double gl = valid ? (S <= 3 ? row[0] : pp[0]) : -INFINITY;
     float wk = valid ? D.winner[sb] : -INFINITY;
     int wi = valid ? sb : 0x7fffffff;
 #pragma unroll
@@ -620,12 +661,12 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
             wi = oi;
         }
     }
-    const double sc = valid ? (D.log_weights ? exp(pp[0] - gl) : 1.0) : 0.0;
+    const double sc = valid ? (D.log_weights ? exp((S <= 3 ? row[0] : pp[0]) - gl) : 1.0) : 0.0;
     double* go = D.gpart + (int64_t)g * kPartStride;
 #pragma unroll
     for (int j = 1; j < NVMAX; ++j) {
         if (j < NV) {
-            double v = valid ? sc * pp[j] : 0.0;
+            double v = valid ? sc * (S <= 3 ? row[j < NROW ? j : 0] : pp[j]) : 0.0;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
             if (lane == 0) go[j] = v;
@@ -646,6 +687,7 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
     double gm = -INFINITY;
     float bk = -INFINITY;
     int bi = 0x7fffffff;
+#pragma unroll 2
     for (int q = lane; q < ng; q += 32) {
         const double* gq = D.gpart + (int64_t)q * kPartStride;
         gm = fmax(gm, __ldcg(gq));
