@@ -7,6 +7,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_set>
+#include <atomic>
 #include <vector>
 
 #include "pf_host.cuh"
@@ -88,17 +89,17 @@ bool pfhost::model_info(int model, ModelInfo* mi)
 
 bool pfhost::dependent_launch_pays(int grid, int M, int E, int S, int device)
 {
-    static int sms[64] = {};  // SM count per device, read once
+    static std::atomic<int> sms[64] = {};  // SM count per device, read once (any thread)
     if (device < 0 || device >= 64) return false;
-    if (sms[device] == 0) {
-        int n = 0;
+    int n = sms[device].load(std::memory_order_relaxed);
+    if (n == 0) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
-        sms[device] = n;
+        sms[device].store(n, std::memory_order_relaxed);
     }
-    return grid > sms[device] * pf_min_blocks(M / E, pf_k1_warps(S));
+    return grid > n * pf_min_blocks(M / E, pf_k1_warps(S));
 }
 
 extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, int32_t* C, int32_t* Z)
@@ -883,7 +884,7 @@ extern "C" pf_status pf_step_submit(pf_filter* f, const pf_step_input* in)
         f->q_next = f->steps_done;
         f->q_active = 1;
     }
-    const int slot = (int)(f->q_next % PF_QUEUE_DEPTH);
+    const int slot = (int)((uint32_t)f->q_next % PF_QUEUE_DEPTH);  // as the device maps its counter
     f->h_q_in[slot] = *in;
     CU(cudaMemcpyAsync(f->d_q_in + slot, f->h_q_in + slot, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->q_up));
     CU(cudaEventRecord(f->q_ev_up[slot], f->q_up));
@@ -908,7 +909,7 @@ extern "C" pf_status pf_step_collect(pf_filter* f, pf_estimate* out, int32_t max
     CU(cudaSetDevice(f->cfg.device));
     while (*count < max && f->q_pending > 0) {
         const int32_t k = f->q_next - f->q_pending;  // oldest pending step
-        const int slot = (int)(k % PF_QUEUE_DEPTH);
+        const int slot = (int)((uint32_t)k % PF_QUEUE_DEPTH);
         if (wait) {
             CU(cudaEventSynchronize(f->q_ev_got[slot]));
         } else {

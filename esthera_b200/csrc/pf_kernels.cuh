@@ -118,7 +118,8 @@ __device__ __forceinline__ int32_t run_step(const InputRef& in) { return in.ctr 
 
 __device__ __forceinline__ int64_t step_index(const InputRef& in)
 {
-    return in.ctr ? (int64_t)(*in.ctr % (in.cap > 0 ? in.cap : 1)) : 0;
+    // unsigned: a counter that wrapped past 2^31 steps still maps into [0, cap)
+    return in.ctr ? (int64_t)((uint32_t)*in.ctr % (uint32_t)(in.cap > 0 ? in.cap : 1)) : 0;
 }
 
 

@@ -184,6 +184,31 @@ def test_submit_collect_equals_step(gpu, pipe, period):
     assert all(np.array_equal(x["mean"], y["mean"]) and x["step"] == y["step"] for x, y in zip(a, b))
 
 
+def test_submit_collect_across_counter_wrap(gpu):
+    """The pipelined queue indexes its rings with the device step counter; a
+    filter restored with a step count just below 2^31 keeps stepping correctly
+    past the wrap (same estimates as synchronous steps from the same state)."""
+    E = gpu
+    p, inputs, _ = uni_setup(steps=12)
+    cfg = dict(particles_per_subfilter=128, num_subfilters=32, num_transfer=1, exchange=2)
+    fa = E.ParticleFilter(UNI, p, **cfg)
+    for k in range(2):
+        fa.step(inputs[k])
+    snap = fa.snapshot()
+    snap[-4:] = np.array([2 ** 31 - 3], np.int32).view(np.uint8)  # the step count, stored last
+    fb = E.ParticleFilter(UNI, p, **cfg)
+    fa.restore(snap)
+    fb.restore(snap)
+    a = [fa.step(inputs[k]) for k in range(2, 10)]
+    for k in range(2, 10):
+        fb.submit(inputs[k])
+    b = fb.collect(8)
+    assert len(b) == 8
+    for x, y in zip(a, b):
+        assert np.array_equal(x["mean"], y["mean"]) and x["best_key"] == y["best_key"]
+    assert np.array_equal(fa.particles(), fb.particles())
+
+
 def test_snapshot_restore(gpu):
     E = gpu
     p, inputs, _ = uni_setup(steps=10)
