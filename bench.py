@@ -24,7 +24,9 @@ roofline: the dominant kernel's algorithmic bytes (the sampling kernel reads
         it) over its CUDA-event time, against the measured HBM copy
         bandwidth; `step` gives the whole step (24 B per particle-step).
         traffic: the kernel's DRAM bytes per launch from the committed ncu
-        summary.
+        summary; issue: the same kernel against the instruction-issue
+        roofline (its ncu warp-instruction count at 4 issues per cycle per
+        SM at the sampled clock), the bound it actually meets.
 
 Multi-GPU (torchrun): each rank runs its own filter (weak scaling, replicas,
 no data-path collective); time = max over ranks.
@@ -487,6 +489,16 @@ def main():
             prof = json.loads(tp.read_text()).get("%s %s ppt%d" % (args.workload, args.pipeline,
                                                                    info["particles_per_thread"]), {})
             traffic = prof.get(dom, {}).get("dram_bytes_per_launch")
+        # the issue roofline the kernels are actually bound by: warp instructions
+        # per launch (ncu, profiles/) over 4 issues per cycle per SM at the
+        # sampled SM clock
+        issue = None
+        winst = prof.get(dom, {}).get("warp_instructions_per_launch")
+        if winst and clocks and clocks.get("sm_mhz"):
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            min_ms = winst / (4.0 * sms * clocks["sm_mhz"] * 1e6) * 1e3
+            issue = {"warp_instructions_per_launch": winst, "min_ms_at_full_issue": min_ms,
+                     "frac": min_ms / phases[dom], "sms": sms, "sm_mhz": clocks["sm_mhz"]}
         if W["angles"]:  # joint angles, wrapped
             d = est["mean"][:, list(W["angles"])] - truth[:total_steps, list(W["angles"])]
             d = np.remainder(d + np.pi, 2 * np.pi) - np.pi
@@ -508,7 +520,7 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "kernel": dom, "kernel_ms": phases[dom], "share": phases[dom] / sum(phases.values()),
                          "alg_bytes_per_launch": kernel_alg * particles,
-                         "ncu": prof.get(dom, {}).get("summary"),
+                         "ncu": prof.get(dom, {}).get("summary"), "issue": issue,
                          "step": {"achieved": step_achieved, "frac": step_achieved / peak,
                                   "alg_bytes_per_particle_step": alg, "phase_ms": phases}},
             "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 128,
