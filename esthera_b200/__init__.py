@@ -22,7 +22,7 @@ LIB_PATH = Path(os.environ["ESTHERA_B200_LIB"]) if os.environ.get("ESTHERA_B200_
 # enums (include/esthera_b200.h)
 PF_OK, PF_ERR_INVALID, PF_ERR_CUDA, PF_ERR_NOMEM, PF_ERR_UNSUPPORTED, PF_ERR_IO = 0, 1, 2, 3, 4, 5
 PF_ERR_ADMISSION, PF_ERR_TIMEOUT, PF_ERR_NOT_FOUND, PF_ERR_BUSY = 6, 7, 8, 9
-MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM = 0, 1, 2
+MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON = 0, 1, 2, 3
 EXCHANGE_NONE, EXCHANGE_RING, EXCHANGE_TORUS, EXCHANGE_ALL2ALL = 0, 1, 2, 3
 RESAMPLE_REFERENCE, RESAMPLE_SYSTEMATIC, RESAMPLE_VOSE = 0, 1, 2
 RNG_SUBFILTER, RNG_REFLAYOUT = 0, 1
@@ -67,6 +67,11 @@ class RefArmParams(C.Structure):
     _fields_ = [("dt", C.c_float), ("init_state", C.c_float * 9)]
 
 
+class BeaconParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("noise", C.c_float * 3), ("sigma_range", C.c_float),
+                ("num_beacons", C.c_int32), ("beacons", (C.c_float * 3) * 16), ("init_state", C.c_float * 3)]
+
+
 STEP_INPUT_DTYPE = np.dtype([("dt", np.float32), ("control", np.float32, MAX_CONTROL),
                              ("meas", np.float32, MAX_MEAS), ("pad", np.float32, 7)])
 ESTIMATE_DTYPE = np.dtype([("mean", np.float64, MAX_STATE), ("log_norm", np.float64),
@@ -75,7 +80,8 @@ ESTIMATE_DTYPE = np.dtype([("mean", np.float64, MAX_STATE), ("log_norm", np.floa
 assert STEP_INPUT_DTYPE.itemsize == C.sizeof(StepInput) == 128
 assert ESTIMATE_DTYPE.itemsize == C.sizeof(Estimate)
 
-PARAMS_TYPE = {MODEL_UNICYCLE: UnicycleParams, MODEL_DHARM: DhArmParams, MODEL_REFARM: RefArmParams}
+PARAMS_TYPE = {MODEL_UNICYCLE: UnicycleParams, MODEL_DHARM: DhArmParams, MODEL_REFARM: RefArmParams,
+               MODEL_BEACON: BeaconParams}
 
 
 class PFError(RuntimeError):
@@ -174,6 +180,9 @@ def _declare(L):
         "pf_read_trace_line": (C.c_int, [P, C.c_int, C.POINTER(StepInput), fp]),
         "pf_refarm_estimate_error": (C.c_float, [fp, fp]),
         "pf_particle_filter": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_char_p, fp]),
+        "pf_beacon_default_params": (C.c_int, [C.POINTER(BeaconParams)]),
+        "pf_beacon_estimate_error": (C.c_float, [fp, fp]),
+        "pf_beacon_particle_filter": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p, fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -248,6 +257,13 @@ def refarm_params(dt=1.0):
     for i in range(5):
         p.init_state[i] = 0.75 * np.pi
     p.init_state[5] = 7.0
+    return p
+
+
+def beacon_params():
+    """The reference unicycle program's constants (pf_beacon_default_params)."""
+    p = BeaconParams()
+    check(lib().pf_beacon_default_params(C.byref(p)))
     return p
 
 
@@ -634,6 +650,16 @@ def particle_filter(num_particles, num_blocks, num_transfer, resampling_freq, in
     e = C.c_float()
     check(lib().pf_particle_filter(num_particles, num_blocks, num_transfer, resampling_freq,
                                    str(input_file).encode(), C.byref(e)))
+    return e.value
+
+
+def beacon_particle_filter(num_particles, num_blocks, num_transfer, input_file):
+    """Drop-in for the reference unicycle program's loop (src/models/unicycle/
+    particle_filter.cu:596-1160) over a unicycle trace file; returns the mean
+    position error of the best particle."""
+    e = C.c_float()
+    check(lib().pf_beacon_particle_filter(num_particles, num_blocks, num_transfer, str(input_file).encode(),
+                                          C.byref(e)))
     return e.value
 
 

@@ -83,6 +83,7 @@ bool pfhost::model_info(int model, ModelInfo* mi)
     case PF_MODEL_UNICYCLE: *mi = {Unicycle::S, Unicycle::K, 2, 16, sizeof(pf_unicycle_params)}; return true;
     case PF_MODEL_DHARM: *mi = {DhArm::S, DhArm::K, 0, 6, sizeof(pf_dharm_params)}; return true;
     case PF_MODEL_REFARM: *mi = {RefArm::S, RefArm::K, 5, 7, sizeof(pf_refarm_params)}; return true;
+    case PF_MODEL_BEACON: *mi = {Beacon::S, Beacon::K, 2, 16, sizeof(pf_beacon_params)}; return true;
     }
     return false;
 }
@@ -118,6 +119,7 @@ const float* pfhost::init_state_of(int model, const ModelParams& mp)
     switch (model) {
     case PF_MODEL_UNICYCLE: return mp.uni.init_state;
     case PF_MODEL_DHARM: return mp.arm.init_state;
+    case PF_MODEL_BEACON: return mp.bcn.init_state;
     default: return mp.ref.init_state;
     }
 }
@@ -125,10 +127,15 @@ const float* pfhost::init_state_of(int model, const ModelParams& mp)
 
 uint32_t pfhost::angle_mask_of(int model)
 {
-    return model == PF_MODEL_UNICYCLE ? 0x4u : (model == PF_MODEL_DHARM ? 0x3fu : 0x1fu);
+    if (model == PF_MODEL_UNICYCLE || model == PF_MODEL_BEACON) return 0x4u;
+    return model == PF_MODEL_DHARM ? 0x3fu : 0x1fu;
 }
 
-int pfhost::angle_count_of(int model) { return model == PF_MODEL_UNICYCLE ? 1 : (model == PF_MODEL_DHARM ? 6 : 5); }
+int pfhost::angle_count_of(int model)
+{
+    if (model == PF_MODEL_UNICYCLE || model == PF_MODEL_BEACON) return 1;
+    return model == PF_MODEL_DHARM ? 6 : 5;
+}
 
 template <class Mdl>
 static ModelOps ops_of()
@@ -142,6 +149,7 @@ ModelOps pfhost::model_ops(int model)
 {
     if (model == PF_MODEL_UNICYCLE) return ops_of<Unicycle>();
     if (model == PF_MODEL_DHARM) return ops_of<DhArm>();
+    if (model == PF_MODEL_BEACON) return ops_of<Beacon>();
     return ops_of<RefArm>();
 }
 
@@ -448,6 +456,10 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     } else if (model == PF_MODEL_DHARM) {
         const pf_dharm_params* p = (const pf_dharm_params*)params;
         if (!(p->sigma_pos > 0) || !(p->sigma_ang > 0)) return fail(PF_ERR_INVALID, "sigmas must be > 0");
+    } else if (model == PF_MODEL_BEACON) {
+        const pf_beacon_params* p = (const pf_beacon_params*)params;
+        if (p->num_beacons < 1 || p->num_beacons > 16) return fail(PF_ERR_INVALID, "1..16 beacons");
+        if (!(p->sigma_range > 0)) return fail(PF_ERR_INVALID, "sigma_range must be > 0");
     }
     s = require_gpu(cfg->device);
     if (s != PF_OK) return s;

@@ -269,6 +269,12 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
                 release(B);
                 return fail(PF_ERR_INVALID, "filter %d: 1..8 landmarks and positive sigmas", f);
             }
+        } else if (model == PF_MODEL_BEACON) {
+            const pf_beacon_params& p = B->mp[f].bcn;
+            if (p.num_beacons < 1 || p.num_beacons > 16 || !(p.sigma_range > 0)) {
+                release(B);
+                return fail(PF_ERR_INVALID, "filter %d: 1..16 beacons and a positive sigma", f);
+            }
         }
     }
     B->nbm = 2 * (((int64_t)mi.K * M + 1) / 2);

@@ -720,6 +720,7 @@ union ModelParams {
     pf_unicycle_params uni;
     pf_dharm_params arm;
     pf_refarm_params ref;
+    pf_beacon_params bcn;
 };
 
 __device__ __forceinline__ float wrap_pi(float a) { return fmaf(-kTwoPi, floorf((a + kPi) * kInvTwoPi), a); }
@@ -976,6 +977,90 @@ struct RefArm {
         value = fmaf((cx - c.z[5]) * (cx - c.z[5]), 0.1f, value);
         value = fmaf((cy - c.z[6]) * (cy - c.z[6]), 0.1f, value);
         return -value;
+    }
+};
+
+// The reference's unicycle program (src/models/unicycle/particle_filter.cu:
+// 314-359): noisy velocity and turn rate, arc motion, heading noise gamma,
+// weight from the ranges to fixed 3-D beacons.  The arc is evaluated through
+//   sin(th + a) - sin th =  2 sin(a/2) cos(th + a/2)
+//   cos(th + a) - cos th = -2 sin(a/2) sin(th + a/2),   a = omega dt
+// (the same motion, without the cancellation of the difference form when
+// a is small, and finite as omega -> 0).  The heading is wrapped to [-pi, pi)
+// (the ranges do not depend on it).  Log weight: lnorm - h sum_i e_i^2 with
+// h = 1 / (2 sigma_range^2) (1 for the reference's exp(-sum e^2)) and
+// lnorm = log(1e5) - (L/2) log(2 pi), the reference's normalisation.
+struct Beacon {
+    static constexpr int S = 3, K = 3, NA = 1;
+    __host__ __device__ static constexpr int angle_var(int) { return 2; }
+    struct Consts {
+        float dt, hdt, v, w, nv, nw, ng, h, lnorm;
+        int L;
+        float bx[16], by[16], bz2[16], z[16];
+    };
+    // lane 16: scalars; lanes 0..15: beacon `lane`
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
+    {
+        const pf_beacon_params& p = mp.bcn;
+        const int L = p.num_beacons < 1 ? 1 : (p.num_beacons > 16 ? 16 : p.num_beacons);
+        if (lane == 16) {
+            const float dt = in.dt > 0.0f ? in.dt : p.dt;
+            c.dt = dt;
+            c.hdt = 0.5f * dt;
+            c.v = in.control[0];
+            c.w = in.control[1];
+            c.nv = p.noise[0];
+            c.nw = p.noise[1];
+            c.ng = p.noise[2];
+            c.h = (float)(0.5 / ((double)p.sigma_range * (double)p.sigma_range));
+            c.lnorm = (float)(log(1e5) - (double)(L / 2) * log(2.0 * 3.14159265358979323846));
+            c.L = L;
+        } else if (lane < 16) {
+            const int j = lane;
+            c.bx[j] = p.beacons[j][0];
+            c.by[j] = p.beacons[j][1];
+            c.bz2[j] = p.beacons[j][2] * p.beacons[j][2];
+            c.z[j] = j < L ? in.meas[j] : 0.0f;
+        }
+    }
+    // sin(u) / u: the series to u^4 below |u| = 2^-6 (remainder under u^6/5040,
+    // below 3e-15), the library sine above it.
+    __device__ static __forceinline__ float sinc(float u)
+    {
+        const float u2 = u * u;
+        if (fabsf(u) < 0.015625f) return fmaf(u2, fmaf(u2, 1.0f / 120.0f, -1.0f / 6.0f), 1.0f);
+        return sinf(u) / u;
+    }
+    __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
+                                                 float* cs)
+    {
+        const float v = fmaf(c.nv, n[0], c.v);
+        const float w = fmaf(c.nw, n[1], c.w);
+        const float g = c.ng * n[2];
+        const float ha = w * c.hdt;  // a / 2
+        const float k = v * c.dt * sinc(ha);  // v / w * 2 sin(a/2)
+        float sm, cm;
+        __sincosf(s[2] + ha, &sm, &cm);
+        const float nx = fmaf(k, cm, s[0]);
+        const float ny = fmaf(k, sm, s[1]);
+        const float nt = wrap_pi(fmaf(g, c.dt, fmaf(w, c.dt, s[2])));
+        s[0] = nx;
+        s[1] = ny;
+        s[2] = nt;
+        float s2, c2;
+        __sincosf(nt, &s2, &c2);
+        sn[0] = s2;
+        cs[0] = c2;
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j < c.L) {
+                const float dx = nx - c.bx[j], dy = ny - c.by[j];
+                const float e = pf_sqrt(fmaf(dx, dx, fmaf(dy, dy, c.bz2[j]))) - c.z[j];
+                acc = fmaf(e, e, acc);
+            }
+        }
+        return fmaf(-c.h, acc, c.lnorm);
     }
 };
 

@@ -135,25 +135,25 @@ struct pf_server {
     int64_t budget = 0, used = 0;
     int max_filters = 0;
     int E = 2;
-    int64_t nbm[3] = {}, draws[3] = {};
+    int64_t nbm[PF_NUM_MODELS] = {}, draws[PF_NUM_MODELS] = {};
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
     cudaEvent_t done = nullptr;
     // each model's kernels run on their own stream, forked from and joined
     // back into `stream`, so the models' grids of a batch overlap
-    cudaStream_t side[3] = {};
-    cudaEvent_t fork = nullptr, join[3] = {};
+    cudaStream_t side[PF_NUM_MODELS] = {};
+    cudaEvent_t fork = nullptr, join[PF_NUM_MODELS] = {};
     std::vector<Slot> slots;
     std::vector<int> free_slots;
     // slots with a queued update and none in flight, per model, in the order
     // they became ready (entries of closed slots are dropped at the launch)
-    std::vector<int> ready[3];
+    std::vector<int> ready[PF_NUM_MODELS];
     int64_t n_open = 0, resident_T = 0, resident_sub = 0, queued = 0;
     // device tables
     FilterDesc* d_desc = nullptr;
     pf_step_input* d_slot_in = nullptr;
     pf_estimate* d_est_tab = nullptr;
-    int2* d_map[3] = {};
+    int2* d_map[PF_NUM_MODELS] = {};
     int64_t map_cap = 0;
     Pending* d_pend = nullptr;
     pf_step_input* d_in = nullptr;
@@ -177,7 +177,7 @@ static void srv_release(pf_server* s)
     for (auto& sl : s->slots)
         if (sl.mem) cudaFreeAsync(sl.mem, s->stream);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    for (int m = 0; m < 3; ++m)
+    for (int m = 0; m < PF_NUM_MODELS; ++m)
         if (s->d_map[m]) cudaFreeAsync(s->d_map[m], s->stream);
     if (s->stream) cudaStreamSynchronize(s->stream);
     void* dev[] = {s->d_desc, s->d_slot_in, s->d_est_tab, s->d_pend, s->d_in, s->d_out, s->d_status};
@@ -188,7 +188,7 @@ static void srv_release(pf_server* s)
         if (p) cudaFreeHost(p);
     if (s->done) cudaEventDestroy(s->done);
     if (s->fork) cudaEventDestroy(s->fork);
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         if (s->join[m]) cudaEventDestroy(s->join[m]);
         if (s->side[m]) cudaStreamDestroy(s->side[m]);
     }
@@ -228,7 +228,7 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     s->budget = hbm_budget;
     s->max_filters = max_filters;
     s->E = E;
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         ModelInfo mi;
         model_info(m, &mi);
         s->nbm[m] = 2 * (((int64_t)mi.K * M + 1) / 2);
@@ -248,7 +248,7 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     STRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     STRY(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
     STRY(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         STRY(cudaStreamCreateWithFlags(&s->side[m], cudaStreamNonBlocking));
         STRY(cudaEventCreateWithFlags(&s->join[m], cudaEventDisableTiming));
     }
@@ -335,7 +335,7 @@ static pf_status ensure_map(pf_server* s, int64_t need)
 {
     if (need <= s->map_cap) return PF_OK;
     const int64_t cap = std::max<int64_t>(need, 4 * s->map_cap);
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         if (s->d_map[m]) CU(cudaFreeAsync(s->d_map[m], s->stream));
         s->d_map[m] = nullptr;
         CU(cudaMallocAsync(reinterpret_cast<void**>(&s->d_map[m]), sizeof(int2) * cap, s->pool, s->stream));
@@ -376,6 +376,9 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
             return fail(PF_ERR_INVALID, "1..8 landmarks and positive sigmas");
     } else if (model == PF_MODEL_DHARM) {
         if (!(mp.arm.sigma_pos > 0) || !(mp.arm.sigma_ang > 0)) return fail(PF_ERR_INVALID, "sigmas must be > 0");
+    } else if (model == PF_MODEL_BEACON) {
+        if (mp.bcn.num_beacons < 1 || mp.bcn.num_beacons > 16 || !(mp.bcn.sigma_range > 0))
+            return fail(PF_ERR_INVALID, "1..16 beacons and a positive sigma");
     }
     const int64_t ru_stride = s->draws[model] - s->nbm[model];
     const Layout L = layout_of(mi.S, M, N, ru_stride);
@@ -503,11 +506,11 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     if (s->busy) return PF_OK;  // one batch in flight at a time
     CU(cudaSetDevice(s->device));
     int n = 0;
-    int64_t ctas[3] = {0, 0, 0};
+    int64_t ctas[PF_NUM_MODELS] = {};
     s->batch_slots.clear();
     s->batch_tags.clear();
     // group the batch by model so each model's kernels see one contiguous CTA map
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         const int first = n;
         int64_t leads = 0;
         for (const int i : s->ready[m]) {
@@ -541,9 +544,9 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     // one expand launch per model group (each writes its own map), each group
     // on its model's stream after everything queued on `stream` so far
     CU(cudaEventRecord(s->fork, st));
-    bool used[3] = {false, false, false};
+    bool used[PF_NUM_MODELS] = {};
     int first = 0;
-    for (int m = 0; m < 3; ++m) {
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
         int cnt = 0;
         while (first + cnt < n && s->slots[s->h_pend[first + cnt].slot].model == m) ++cnt;
         if (cnt == 0) continue;
@@ -563,7 +566,7 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
         used[m] = true;
         first += cnt;
     }
-    for (int m = 0; m < 3; ++m)
+    for (int m = 0; m < PF_NUM_MODELS; ++m)
         if (used[m]) CU(cudaStreamWaitEvent(st, s->join[m], 0));
     k_srv_gather<<<n + 1, 64, 0, st>>>(s->d_pend, n, s->d_est_tab, s->d_out, s->d_status);
     CU(cudaGetLastError());

@@ -1,6 +1,7 @@
 /*
  * pf_traces.c -- seeded synthetic ground truth and measurements for the
- * unicycle and Denavit-Hartenberg arm models (host C).
+ * unicycle, Denavit-Hartenberg arm and beacon (range-only unicycle) models
+ * (host C).
  *
  * No public dataset is involved: every trace is generated from a seed.  The
  * random source is SplitMix64 (Steele, Lea, Flood 2014) with Box-Muller
@@ -77,6 +78,34 @@ pf_status pf_dharm_default_params(uint32_t seed, pf_dharm_params* p)
         p->init_state[i] = (float)(-M_PI / 2 + M_PI * sm64_unif(&r));
         p->init_state[6 + i] = (float)(-0.5 + sm64_unif(&r));
     }
+    return PF_OK;
+}
+
+/* The reference unicycle program's constants: the fixed beacon positions and
+ * noise levels of src/models/unicycle/particle_filter.cu:60-76, the start pose
+ * of :708-716, dt = 1 (its trace generator, generate_input.py:31-36), and
+ * sigma_range = sqrt(1/2), which makes the log weight -sum e^2 as in its
+ * importance_weight (:340-359). */
+pf_status pf_beacon_default_params(pf_beacon_params* p)
+{
+    static const float bx[10] = {12, 12, 13, 14, 16, 16, 18, 20, 20, 20};
+    static const float by[10] = {12, 37, 25, 18, 12, 37, 30, 12, 25, 37};
+    if (!p) return PF_ERR_INVALID;
+    memset(p, 0, sizeof(*p));
+    p->dt = 1.0f;
+    p->noise[0] = 0.5f;
+    p->noise[1] = 0.1f;
+    p->noise[2] = 0.01f;
+    p->sigma_range = (float)sqrt(0.5);
+    p->num_beacons = 10;
+    for (int j = 0; j < 10; ++j) {
+        p->beacons[j][0] = bx[j];
+        p->beacons[j][1] = by[j];
+        p->beacons[j][2] = 3.0f;
+    }
+    p->init_state[0] = 20.0f;
+    p->init_state[1] = 40.0f;
+    p->init_state[2] = (float)(-M_PI / 2);
     return PF_OK;
 }
 
@@ -167,6 +196,37 @@ pf_status pf_make_trace(pf_model_id model, const void* params, uint32_t seed, in
                 truth[12 * k + i] = (float)q[i];
                 truth[12 * k + 6 + i] = (float)qd[i];
             }
+        }
+        return PF_OK;
+    }
+    if (model == PF_MODEL_BEACON) {
+        /* The reference's unicycle trace generator (generate_input.py:37-56):
+         * v = |N(0.3, 0.1)|, omega = N(0, 0.3), an exact arc of length v dt,
+         * ranges to the beacons with N(0, sigma_range) noise (the generator's
+         * sigma is 1; here the filter's own sigma is used). */
+        const pf_beacon_params* P = (const pf_beacon_params*)params;
+        const int L = P->num_beacons;
+        if (L < 1 || L > 16) return PF_ERR_INVALID;
+        double x = P->init_state[0], y = P->init_state[1], th = P->init_state[2];
+        const double dt = P->dt;
+        for (int k = 0; k < steps; ++k) {
+            const double v = fabs(0.3 + 0.1 * sm64_gauss(&r)), w = 0.3 * sm64_gauss(&r);
+            const double h = 0.5 * w * dt;
+            const double sc = fabs(h) < 1e-8 ? 1.0 : sin(h) / h;
+            x += v * dt * sc * cos(th + h);
+            y += v * dt * sc * sin(th + h);
+            th = wrap(th + w * dt);
+            pf_step_input* in = &inputs[k];
+            in->dt = (float)dt;
+            in->control[0] = (float)v;
+            in->control[1] = (float)w;
+            for (int j = 0; j < L; ++j) {
+                const double dx = x - P->beacons[j][0], dy = y - P->beacons[j][1], dz = P->beacons[j][2];
+                in->meas[j] = (float)(sqrt(dx * dx + dy * dy + dz * dz) + P->sigma_range * sm64_gauss(&r));
+            }
+            truth[3 * k + 0] = (float)x;
+            truth[3 * k + 1] = (float)y;
+            truth[3 * k + 2] = (float)th;
         }
         return PF_OK;
     }

@@ -47,8 +47,10 @@ typedef enum {
 typedef enum {
     PF_MODEL_UNICYCLE = 0, /* (x, y, theta), range/bearing to landmarks */
     PF_MODEL_DHARM = 1,    /* 6-joint Denavit-Hartenberg arm, q[6] + qdot[6] */
-    PF_MODEL_REFARM = 2    /* the reference's 5-angle camera arm on a cart */
+    PF_MODEL_REFARM = 2,   /* the reference's 5-angle camera arm on a cart */
+    PF_MODEL_BEACON = 3    /* the reference's unicycle tracked by range-only beacons (x, y, theta) */
 } pf_model_id;
+#define PF_NUM_MODELS 4
 
 typedef enum {
     PF_EXCHANGE_NONE = 0,
@@ -116,6 +118,7 @@ typedef struct {
  *   unicycle: control {v, omega};        meas {range[L], bearing[L]}
  *   dharm:    control {};                 meas {px, py, pz, yaw, pitch, roll}
  *   refarm:   control {joint rates[5]};   meas {angles[5], x, y}
+ *   beacon:   control {v, omega};         meas {range[L]}
  * dt <= 0 uses the model's dt. */
 typedef struct {
     float dt;
@@ -157,6 +160,24 @@ typedef struct {
     float dt;
     float init_state[9];         /* angles[5], x, y, vX, vY */
 } pf_refarm_params;
+
+/* The reference's unicycle program (src/models/unicycle/particle_filter.cu:
+ * 314-359): v += noise[0] n0, omega += noise[1] n1, gamma = noise[2] n2;
+ * x += v/omega (sin(theta + omega dt) - sin theta),
+ * y -= v/omega (cos(theta + omega dt) - cos theta), theta += (omega + gamma) dt;
+ * weight = norm exp(-sum_i (|p - s_i| - z_i)^2 / (2 sigma_range^2)) with p = (x, y, 0)
+ * and the reference's norm = 1e5 / (2 pi)^(L/2) (L/2 an integer division).
+ * pf_beacon_default_params gives the reference's constants: 10 beacons, noise
+ * (0.5, 0.1, 0.01), sigma_range = sqrt(1/2) (its exp(-sum e^2)), dt = 1, start
+ * (20, 40, -pi/2). */
+typedef struct {
+    float dt;
+    float noise[3];              /* std of the velocity, turn-rate and heading (gamma) noise */
+    float sigma_range;
+    int32_t num_beacons;         /* 1..16 */
+    float beacons[16][3];        /* beacon positions (x, y, z) */
+    float init_state[3];         /* x, y, theta */
+} pf_beacon_params;
 
 typedef struct pf_filter pf_filter;
 
@@ -441,22 +462,36 @@ pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_state, int32_
 /* Unicycle: landmarks uniform in [-10,10]^2, truth from (0,0,0), v=1, omega=0.3 sin(0.05 t). */
 pf_status pf_unicycle_default_params(uint32_t seed, int32_t num_landmarks, pf_unicycle_params* p);
 pf_status pf_dharm_default_params(uint32_t seed, pf_dharm_params* p);
+/* The reference unicycle program's constants (particle_filter.cu:60-76, 708-716). */
+pf_status pf_beacon_default_params(pf_beacon_params* p);
 /* steps x pf_step_input and steps x num_state truth floats. */
 pf_status pf_make_trace(pf_model_id model, const void* params, uint32_t seed, int32_t steps,
                         pf_step_input* inputs, float* truth);
 
 /* ---- reference-compatible driver (reference trace files, C host) ---- */
-/* Parses one line of a reference trace: robot-arm format
+/* Parses one line of a reference trace.  PF_MODEL_REFARM: robot-arm format
  * "x y angles[5] controls[5] dt actual_x actual_y actual_angles[5]"
- * (pf_model_soa.cuh:276-301).  Returns PF_OK, or PF_ERR_IO at end of file / bad line. */
+ * (pf_model_soa.cuh:276-301).  PF_MODEL_BEACON: unicycle format
+ * "ranges[10] v omega dt actual_x actual_y actual_theta"
+ * (src/models/unicycle/particle_filter.cu:756-772).  Returns PF_OK, or
+ * PF_ERR_IO at end of file / bad line. */
 pf_status pf_read_trace_line(void* file, pf_model_id model, pf_step_input* in, float* actual);
 /* The reference's estimate_error for the robot-arm model (pf_model_soa.cuh:303-316). */
 float pf_refarm_estimate_error(const float* est, const float* actual);
+/* The unicycle program's error: position distance |est.xy - actual.xy|
+ * (particle_filter.cu:1044). */
+float pf_beacon_estimate_error(const float* est, const float* actual);
 /* Drop-in for the reference driver: runs the robot-arm filter over a trace file with
  * the reference's defaults (ring exchange, multinomial resampling) and returns the
  * mean estimate error through *mean_error. */
 pf_status pf_particle_filter(int32_t num_particles, int32_t num_blocks, int32_t num_transfer,
                              float resampling_freq, const char* input_file, float* mean_error);
+/* Drop-in for the unicycle program's main loop (particle_filter.cu:596-1160):
+ * the beacon filter with the default constants over a unicycle trace file
+ * (ring exchange of num_transfer particles, multinomial resampling every
+ * step), returning the mean position error of the best particle. */
+pf_status pf_beacon_particle_filter(int32_t num_particles, int32_t num_blocks, int32_t num_transfer,
+                                    const char* input_file, float* mean_error);
 
 #ifdef __cplusplus
 }

@@ -18,7 +18,7 @@ REF_LIB = HERE / "_ref" / "libmtgp_ref.so"
 RES_REF, RES_SYSTEMATIC, RES_VOSE = 0, 1, 2
 RNG_REFLAYOUT, RNG_SUBFILTER = 0, 1
 EXCH_NONE, EXCH_RING, EXCH_TORUS, EXCH_ALL2ALL = 0, 1, 2, 3
-MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM = 0, 1, 2
+MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON = 0, 1, 2, 3
 MASK_PARAMS, MASK_CUDA_REF = 0, 0xFF800000
 
 
@@ -27,7 +27,8 @@ class OrcModel(C.Structure):
                 ("dt", C.c_double), ("sq", C.c_double * 3), ("sigma_r", C.c_double), ("sigma_b", C.c_double),
                 ("num_landmarks", C.c_int), ("lm", (C.c_double * 2) * 8),
                 ("sigma_qd", C.c_double), ("sigma_p", C.c_double), ("sigma_a", C.c_double),
-                ("a", C.c_double * 6), ("alpha", C.c_double * 6), ("d", C.c_double * 6)]
+                ("a", C.c_double * 6), ("alpha", C.c_double * 6), ("d", C.c_double * 6),
+                ("bnoise", C.c_double * 3), ("num_beacons", C.c_int), ("bc", (C.c_double * 3) * 16)]
 
 
 class OrcFilter(C.Structure):
@@ -260,6 +261,15 @@ def model_from_params(model, p):
         md.dt, md.sigma_qd, md.sigma_p, md.sigma_a = p.dt, p.sigma_qd, p.sigma_pos, p.sigma_ang
         for i in range(6):
             md.a[i], md.alpha[i], md.d[i] = p.a[i], p.alpha[i], p.d[i]
+    elif model == MODEL_BEACON:
+        md.num_state, md.num_noise = 3, 3
+        md.dt, md.sigma_r = p.dt, p.sigma_range
+        for i in range(3):
+            md.bnoise[i] = p.noise[i]
+        md.num_beacons = p.num_beacons
+        for j in range(16):
+            for k in range(3):
+                md.bc[j][k] = p.beacons[j][k]
     else:
         md.num_state, md.num_noise = 9, 9
         md.dt = p.dt

@@ -490,19 +490,56 @@ static double refarm_step(const orc_model* md, float* s, const float* n, const f
     return -value;
 }
 
+/* The reference's unicycle program (src/models/unicycle/particle_filter.cu:
+ * 314-359) in its own difference form: v and omega with additive noise,
+ * x += v/omega (sin(th + omega dt) - sin th), y -= v/omega (cos(th + omega dt)
+ * - cos th), th += (omega + gamma) dt (wrapped to [-pi, pi) as the engine
+ * does), log weight log(1e5) - (L/2) log(2 pi) - sum e^2 / (2 sigma^2) with e
+ * the range error to each 3-D beacon (L/2 an integer division). */
+static double beacon_step(const orc_model* md, float* s, const float* n, const float* c,
+                          const float* z)
+{
+    const double dt = md->dt;
+    const double v = (double)c[0] + md->bnoise[0] * n[0];
+    const double w = (double)c[1] + md->bnoise[1] * n[1];
+    const double g = md->bnoise[2] * n[2];
+    const double th = s[2];
+    double nx, ny;
+    if (fabs(w * dt) < 1e-9) { /* the arc's straight-line limit */
+        nx = s[0] + v * dt * cos(th);
+        ny = s[1] + v * dt * sin(th);
+    } else {
+        nx = s[0] + v / w * (sin(th + w * dt) - sin(th));
+        ny = s[1] - v / w * (cos(th + w * dt) - cos(th));
+    }
+    s[0] = (float)nx;
+    s[1] = (float)ny;
+    s[2] = (float)wrap_pi(th + w * dt + g * dt);
+    const double x = s[0], y = s[1];
+    const int L = md->num_beacons;
+    double acc = 0.0;
+    for (int j = 0; j < L; ++j) {
+        const double dx = x - md->bc[j][0], dy = y - md->bc[j][1], dz = md->bc[j][2];
+        const double e = sqrt(dx * dx + dy * dy + dz * dz) - z[j];
+        acc += e * e;
+    }
+    return log(1e5) - (double)(L / 2) * log(2.0 * M_PI) - acc / (2.0 * md->sigma_r * md->sigma_r);
+}
+
 double orc_model_step(const orc_model* md, float* state, const float* noise, const float* control,
                       const float* meas)
 {
     switch (md->model) {
     case ORC_MODEL_UNICYCLE: return unicycle_step(md, state, noise, control, meas);
     case ORC_MODEL_DHARM: return dharm_step(md, state, noise, control, meas);
+    case ORC_MODEL_BEACON: return beacon_step(md, state, noise, control, meas);
     default: return refarm_step(md, state, noise, control, meas);
     }
 }
 
 static int is_angle(const orc_model* md, int v)
 {
-    if (md->model == ORC_MODEL_UNICYCLE) return v == 2;
+    if (md->model == ORC_MODEL_UNICYCLE || md->model == ORC_MODEL_BEACON) return v == 2;
     if (md->model == ORC_MODEL_DHARM) return v < 6;
     return v < 5;
 }

@@ -107,6 +107,7 @@ void orc_exchange_sources(int mode, int N, int m, int t, const float* top_keys, 
 #define ORC_MODEL_UNICYCLE 0
 #define ORC_MODEL_DHARM 1
 #define ORC_MODEL_REFARM 2
+#define ORC_MODEL_BEACON 3
 
 typedef struct {
     int model;
@@ -119,12 +120,18 @@ typedef struct {
     /* DH arm */
     double sigma_qd, sigma_p, sigma_a;
     double a[6], alpha[6], d[6];
+    /* beacon (range-only unicycle): velocity / turn-rate / heading noise std,
+     * beacon positions; sigma_r is the range std */
+    double bnoise[3];
+    int num_beacons;
+    double bc[16][3];
 } orc_model;
 
 /* control / measurement as flat float arrays:
  *   unicycle: control {v, omega}; measurement {range[L], bearing[L]}
  *   dharm:    control {} ;        measurement {px,py,pz,yaw,pitch,roll}
- *   refarm:   control {angles[5]}; measurement {angles[5], x, y} */
+ *   refarm:   control {angles[5]}; measurement {angles[5], x, y}
+ *   beacon:   control {v, omega}; measurement {range[L]} */
 
 /* Propagate one particle in place (state has num_state floats, noise has
  * num_noise normals) and return its log-likelihood.  Double precision. */
