@@ -162,6 +162,9 @@ def _declare(L):
         "pf_server_poll": (C.c_int, [P, C.c_int32, P, C.c_int32, ip]),
         "pf_server_stats_get": (C.c_int, [P, C.POINTER(ServerStats)]),
         "pf_server_get_particles": (C.c_int, [P, C.c_int32, fp, fp, fp]),
+        "pf_server_snapshot_size": (C.c_int64, [P, C.c_int32]),
+        "pf_server_snapshot": (C.c_int, [P, C.c_int32, P]),
+        "pf_server_restore": (C.c_int, [P, C.c_int32, P]),
         "pf_load_default": (C.c_int, [C.POINTER(LoadConfig)]),
         "pf_serve_load": (C.c_int, [C.POINTER(PFConfig), C.POINTER(LoadConfig), C.POINTER(LoadReport)]),
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
@@ -578,6 +581,19 @@ class Server:
         k = np.zeros(n, np.float32)
         check(lib().pf_server_get_particles(self._h, fid, _fptr(a), _fptr(srt), _fptr(k)))
         return a, srt, k
+
+    def snapshot(self, fid):
+        """Filter fid's particles, streams and update count (pf_server_snapshot), as bytes."""
+        n = lib().pf_server_snapshot_size(self._h, fid)
+        if n < 0:
+            raise PFError(PF_ERR_NOT_FOUND, "no open filter %d" % fid)
+        buf = np.zeros(n, np.uint8)
+        check(lib().pf_server_snapshot(self._h, fid, buf.ctypes.data_as(C.c_void_p)))
+        return buf.tobytes()
+
+    def restore(self, fid, snap):
+        buf = np.frombuffer(snap, np.uint8).copy()
+        check(lib().pf_server_restore(self._h, fid, buf.ctypes.data_as(C.c_void_p)))
 
 
 class LoadConfig(C.Structure):

@@ -652,3 +652,77 @@ extern "C" pf_status pf_server_get_particles(pf_server* s, int32_t id, float* so
     if (keys) CU(cudaMemcpy(keys, D.tkey, 4 * (size_t)D.T, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// per-filter snapshot / restore
+// layout: int64 header[4] = {magic, model, T, N}, state S*T floats, stream
+// words N*351, int32 updates completed.
+// ---------------------------------------------------------------------------
+static const int64_t kSrvSnapMagic = 0x5046535256534e31LL;
+
+static pf_status idle_filter(const pf_server* s, int32_t id)
+{
+    if (!s) return fail(PF_ERR_INVALID, "null argument");
+    if (id < 0 || id >= s->max_filters || !s->slots[id].open) return fail(PF_ERR_NOT_FOUND, "no open filter %d", id);
+    const Slot& sl = s->slots[id];
+    if (sl.in_flight || !sl.queue.empty()) return fail(PF_ERR_BUSY, "filter %d has updates queued or in flight", id);
+    return PF_OK;
+}
+
+extern "C" int64_t pf_server_snapshot_size(const pf_server* s, int32_t id)
+{
+    if (!s || id < 0 || id >= s->max_filters || !s->slots[id].open) return -1;
+    const Slot& sl = s->slots[id];
+    ModelInfo mi;
+    model_info(sl.model, &mi);
+    return 32 + 4 * (int64_t)mi.S * sl.T + 4 * (int64_t)sl.N * kMtgpN + 4;
+}
+
+extern "C" pf_status pf_server_snapshot(pf_server* s, int32_t id, void* buf)
+{
+    pf_status st = idle_filter(s, id);
+    if (st != PF_OK) return st;
+    if (!buf) return fail(PF_ERR_INVALID, "null argument");
+    const Slot& sl = s->slots[id];
+    ModelInfo mi;
+    model_info(sl.model, &mi);
+    const Layout L = layout_of(mi.S, s->cfg.particles_per_subfilter, sl.N, s->draws[sl.model] - s->nbm[sl.model]);
+    CU(cudaSetDevice(s->device));
+    char* p = static_cast<char*>(buf);
+    const int64_t hdr[4] = {kSrvSnapMagic, sl.model, sl.T, sl.N};
+    memcpy(p, hdr, 32);
+    p += 32;
+    const size_t sb = 4 * (size_t)mi.S * sl.T, mb = 4 * (size_t)sl.N * kMtgpN;
+    CU(cudaMemcpyAsync(p, sl.mem + L.state, sb, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaMemcpyAsync(p + sb, sl.mem + L.mtgp, mb, cudaMemcpyDeviceToHost, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    memcpy(p + sb + mb, &sl.steps, 4);
+    return PF_OK;
+}
+
+extern "C" pf_status pf_server_restore(pf_server* s, int32_t id, const void* buf)
+{
+    pf_status st = idle_filter(s, id);
+    if (st != PF_OK) return st;
+    if (!buf) return fail(PF_ERR_INVALID, "null argument");
+    Slot& sl = s->slots[id];
+    const char* p = static_cast<const char*>(buf);
+    int64_t hdr[4];
+    memcpy(hdr, p, 32);
+    if (hdr[0] != kSrvSnapMagic || hdr[1] != sl.model || hdr[2] != sl.T || hdr[3] != sl.N)
+        return fail(PF_ERR_INVALID, "snapshot does not match filter %d (model, particle count)", id);
+    p += 32;
+    ModelInfo mi;
+    model_info(sl.model, &mi);
+    const Layout L = layout_of(mi.S, s->cfg.particles_per_subfilter, sl.N, s->draws[sl.model] - s->nbm[sl.model]);
+    CU(cudaSetDevice(s->device));
+    const size_t sb = 4 * (size_t)mi.S * sl.T, mb = 4 * (size_t)sl.N * kMtgpN;
+    // pageable source: each copy is staged before the call returns, and runs
+    // in stream order before any later batch of this filter
+    CU(cudaMemcpyAsync(sl.mem + L.state, p, sb, cudaMemcpyHostToDevice, s->stream));
+    CU(cudaMemcpyAsync(sl.mem + L.mtgp, p + sb, mb, cudaMemcpyHostToDevice, s->stream));
+    int32_t steps = 0;
+    memcpy(&steps, p + sb + mb, 4);
+    sl.steps = steps;
+    return PF_OK;
+}

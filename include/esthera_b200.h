@@ -365,6 +365,17 @@ pf_status pf_server_poll(pf_server* s, int32_t wait, pf_server_result* out, int3
 pf_status pf_server_stats_get(pf_server* s, pf_server_stats* st);
 /* Current particles, sorted copy and sorted keys of filter id (host; any may be NULL). */
 pf_status pf_server_get_particles(pf_server* s, int32_t id, float* soa, float* sorted_soa, float* keys);
+/* Per-filter snapshot / restore (no counterpart in the reference), e.g. to move
+ * a filter to another server or GPU: the snapshot holds the filter's model,
+ * particle count, particles, MTGP32 stream words and update count.  Both need
+ * the filter idle (no update queued or in flight: PF_ERR_BUSY otherwise).
+ * Restore targets an open filter of the same model and particle count (opened
+ * with the same parameters for the same results) and replaces its particles,
+ * streams and update count; its next updates then give the results the
+ * snapshotted filter would have given. */
+int64_t pf_server_snapshot_size(const pf_server* s, int32_t id);
+pf_status pf_server_snapshot(pf_server* s, int32_t id, void* host_buf);
+pf_status pf_server_restore(pf_server* s, int32_t id, const void* host_buf);
 
 /* ---- the served tracking load (request loop over pf_server_*, host C) ----
  * Poisson arrivals at `rate` per second for `duration_s`; each request is a

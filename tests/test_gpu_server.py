@@ -158,3 +158,47 @@ def test_server_normalisation_vs_fp64(gpu):
         mx = kk.max()
         ln = mx + np.log(np.sum(np.exp(kk - mx)))
         assert abs(r[0]["estimate"]["log_norm"] - ln) <= 1e-6 * max(1.0, abs(ln))
+
+
+@pytest.mark.gpu
+def test_server_snapshot_restore_moves_a_filter(gpu):
+    """A filter snapshotted after 3 updates and restored into a filter of another
+    server (same model, parameters and count, different seed and slot) gives
+    the source's next results bit for bit; busy and mismatched filters are refused."""
+    E = gpu
+    p, inputs, _ = trace(E, UNI, 77, 7)
+    src = E.Server(1 << 30, 4, **CFG)
+    a = src.open(UNI, p, 2048, 77)
+    for k in range(3):
+        src.update(a, inputs[k], tag=k)
+        src.launch()
+        src.poll()
+    snap = src.snapshot(a)
+    src.update(a, inputs[3], tag=3)
+    with pytest.raises(E.PFError) as ei:
+        src.snapshot(a)  # an update queued
+    assert ei.value.status == E.PF_ERR_BUSY
+    want = []
+    for k in range(3, 7):
+        if k > 3:
+            src.update(a, inputs[k], tag=k)
+        src.launch()
+        want.append(src.poll()[0])
+    dst = E.Server(1 << 30, 4, **CFG)
+    dst.open(ARM, E.dharm_params(3), 1024, 5)  # another slot in use first
+    b = dst.open(UNI, p, 2048, 991)
+    small = dst.open(UNI, p, 1024, 991)
+    with pytest.raises(E.PFError) as ei:
+        dst.restore(small, snap)
+    assert ei.value.status == E.PF_ERR_INVALID
+    dst.restore(b, snap)
+    for k in range(3, 7):
+        dst.update(b, inputs[k], tag=k)
+        dst.launch()
+        r = dst.poll()[0]
+        w = want[k - 3]
+        assert r["step"] == w["step"] == k + 1
+        assert same(r["estimate"], w["estimate"]), k
+    assert np.array_equal(dst.particles(b, 2048)[0], src.particles(a, 2048)[0])
+    src.close()
+    dst.close()
