@@ -83,3 +83,32 @@ def sampling_importance(state, normals, control, meas, dt):
     _check(lib().ref_sampling_importance(_f(st), _f(nz), _f(ctl), _f(z), float(dt), st.shape[1], _f(w)),
            "ref_sampling_importance")
     return st, w
+
+
+# ---- the reference unicycle program's kernel (oracle/build_ref_unicycle.sh) ----
+UNICYCLE_LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libref_unicycle.so"
+_ulib = None
+
+
+def unicycle_available():
+    return UNICYCLE_LIB_PATH.exists()
+
+
+def unicycle_sampling(state, normals, v, w, dt, ranges):
+    """The unicycle program's sampling_importance on n particles (one per block):
+    (state out, S x n; linear weight norm * expf(-value), n)."""
+    global _ulib
+    if _ulib is None:
+        L = C.CDLL(str(UNICYCLE_LIB_PATH))
+        fp = C.POINTER(C.c_float)
+        L.ref_unicycle_sampling.argtypes = [fp, fp, C.c_float, C.c_float, C.c_float, fp, C.c_int, fp, fp]
+        L.ref_unicycle_sampling.restype = C.c_int
+        _ulib = L
+    st = np.ascontiguousarray(state, np.float32)
+    nz = np.ascontiguousarray(normals, np.float32)
+    z = np.ascontiguousarray(ranges, np.float32)
+    n = st.shape[1]
+    so = np.zeros_like(st)
+    wt = np.zeros(n, np.float32)
+    _check(_ulib.ref_unicycle_sampling(_f(st), _f(nz), v, w, dt, _f(z), n, _f(so), _f(wt)), "ref_unicycle_sampling")
+    return so, wt

@@ -103,3 +103,42 @@ def test_refarm_model_equals_reference_kernel(gpu):
     assert ok.mean() > 0.5
     lr = np.log(w[ok].astype(np.float64))
     assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
+
+
+@pytest.mark.skipif(not R.unicycle_available(), reason="oracle/_ref/libref_unicycle.so not built "
+                                                     "(oracle/build_ref_unicycle.sh needs the reference tree)")
+@pytest.mark.parametrize("w0,dt", [(0.2, 1.0), (-0.6, 0.5), (1.5, 1.0)])
+def test_beacon_model_equals_reference_kernel(gpu, w0, dt):
+    """The engine's beacon model against the reference unicycle program's own
+    sampling_importance (sampling + importance_weight, particle_filter.cu:314-455)
+    on the same particles, normals, controls and ranges.  States: within 2e-5
+    plus the reference's own FP32 rounding of v/w (sin(th + w dt) - sin th),
+    16 |v/w| 2^-24 (its argument th + w dt rounded to FP32, |th + w dt| < 8,
+    and one ulp of each sine; the engine evaluates the arc without that
+    difference); log-likelihoods within 1e-4 relative + 5e-3 absolute of
+    log(weight)."""
+    E = gpu
+    rng = np.random.default_rng(int(100 * abs(w0)) + int(10 * dt))
+    n = 4096
+    p = E.beacon_params()
+    # a cloud around (17, 30) tight enough that the weights stay representable
+    st = np.stack([rng.normal(17, 0.5, n), rng.normal(30, 0.5, n), rng.uniform(-3.1, 3.1, n)]).astype(np.float32)
+    nz = rng.standard_normal((3, n)).astype(np.float32)
+    inp = np.zeros(1, E.STEP_INPUT_DTYPE)[0]
+    inp["dt"] = dt
+    inp["control"][:2] = [0.3, w0]
+    bx = np.array([p.beacons[j][0] for j in range(10)], np.float64)
+    by = np.array([p.beacons[j][1] for j in range(10)], np.float64)
+    inp["meas"][:10] = np.sqrt((17 - bx) ** 2 + (30 - by) ** 2 + 9) + rng.normal(0, 0.5, 10)
+    so, ll = E.model_step(E.MODEL_BEACON, p, inp, st, nz)
+    sr, wt = R.unicycle_sampling(st, nz, 0.3, w0, dt, inp["meas"][:10])
+    v = 0.3 + 0.5 * nz[0].astype(np.float64)
+    w = w0 + 0.1 * nz[1].astype(np.float64)
+    tol = 2e-5 + 16.0 * np.abs(v / w) * 2.0 ** -24
+    assert np.all(np.abs(so[0] - sr[0]) <= tol) and np.all(np.abs(so[1] - sr[1]) <= tol)
+    # the engine wraps the heading to [-pi, pi); the program does not
+    assert np.all(np.abs(np.angle(np.exp(1j * (so[2].astype(np.float64) - sr[2])))) < 2e-5)
+    ok = wt > 1e-30
+    assert ok.mean() > 0.5
+    lr = np.log(wt[ok].astype(np.float64))
+    assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
