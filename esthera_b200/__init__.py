@@ -22,7 +22,7 @@ LIB_PATH = Path(os.environ["ESTHERA_B200_LIB"]) if os.environ.get("ESTHERA_B200_
 # enums (include/esthera_b200.h)
 PF_OK, PF_ERR_INVALID, PF_ERR_CUDA, PF_ERR_NOMEM, PF_ERR_UNSUPPORTED, PF_ERR_IO = 0, 1, 2, 3, 4, 5
 PF_ERR_ADMISSION, PF_ERR_TIMEOUT, PF_ERR_NOT_FOUND, PF_ERR_BUSY = 6, 7, 8, 9
-MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON = 0, 1, 2, 3
+MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON, MODEL_CAMARM = 0, 1, 2, 3, 4
 EXCHANGE_NONE, EXCHANGE_RING, EXCHANGE_TORUS, EXCHANGE_ALL2ALL = 0, 1, 2, 3
 RESAMPLE_REFERENCE, RESAMPLE_SYSTEMATIC, RESAMPLE_VOSE = 0, 1, 2
 RNG_SUBFILTER, RNG_REFLAYOUT = 0, 1
@@ -67,6 +67,11 @@ class RefArmParams(C.Structure):
     _fields_ = [("dt", C.c_float), ("init_state", C.c_float * 9)]
 
 
+class CamArmParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("init_state", C.c_float * 9), ("fc", C.c_float * 2), ("cc", C.c_float * 2),
+                ("kc", C.c_float * 4)]
+
+
 class BeaconParams(C.Structure):
     _fields_ = [("dt", C.c_float), ("noise", C.c_float * 3), ("sigma_range", C.c_float),
                 ("num_beacons", C.c_int32), ("beacons", (C.c_float * 3) * 16), ("init_state", C.c_float * 3)]
@@ -81,7 +86,7 @@ assert STEP_INPUT_DTYPE.itemsize == C.sizeof(StepInput) == 128
 assert ESTIMATE_DTYPE.itemsize == C.sizeof(Estimate)
 
 PARAMS_TYPE = {MODEL_UNICYCLE: UnicycleParams, MODEL_DHARM: DhArmParams, MODEL_REFARM: RefArmParams,
-               MODEL_BEACON: BeaconParams}
+               MODEL_BEACON: BeaconParams, MODEL_CAMARM: CamArmParams}
 
 
 class PFError(RuntimeError):
@@ -184,6 +189,7 @@ def _declare(L):
         "pf_refarm_estimate_error": (C.c_float, [fp, fp]),
         "pf_particle_filter": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_char_p, fp]),
         "pf_beacon_default_params": (C.c_int, [C.POINTER(BeaconParams)]),
+        "pf_camarm_default_params": (C.c_int, [C.POINTER(CamArmParams)]),
         "pf_beacon_estimate_error": (C.c_float, [fp, fp]),
         "pf_beacon_particle_filter": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_char_p, fp]),
     }
@@ -267,6 +273,13 @@ def beacon_params():
     """The reference unicycle program's constants (pf_beacon_default_params)."""
     p = BeaconParams()
     check(lib().pf_beacon_default_params(C.byref(p)))
+    return p
+
+
+def camarm_params():
+    """The reference pinhole camera's calibration and the arm's start state (pf_camarm_default_params)."""
+    p = CamArmParams()
+    check(lib().pf_camarm_default_params(C.byref(p)))
     return p
 
 

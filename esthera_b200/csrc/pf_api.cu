@@ -84,6 +84,7 @@ bool pfhost::model_info(int model, ModelInfo* mi)
     case PF_MODEL_DHARM: *mi = {DhArm::S, DhArm::K, 0, 6, sizeof(pf_dharm_params)}; return true;
     case PF_MODEL_REFARM: *mi = {RefArm::S, RefArm::K, 5, 7, sizeof(pf_refarm_params)}; return true;
     case PF_MODEL_BEACON: *mi = {Beacon::S, Beacon::K, 2, 16, sizeof(pf_beacon_params)}; return true;
+    case PF_MODEL_CAMARM: *mi = {CamArm::S, CamArm::K, 5, 7, sizeof(pf_camarm_params)}; return true;
     }
     return false;
 }
@@ -120,6 +121,7 @@ const float* pfhost::init_state_of(int model, const ModelParams& mp)
     case PF_MODEL_UNICYCLE: return mp.uni.init_state;
     case PF_MODEL_DHARM: return mp.arm.init_state;
     case PF_MODEL_BEACON: return mp.bcn.init_state;
+    case PF_MODEL_CAMARM: return mp.cam.init_state;
     default: return mp.ref.init_state;
     }
 }
@@ -150,6 +152,7 @@ ModelOps pfhost::model_ops(int model)
     if (model == PF_MODEL_UNICYCLE) return ops_of<Unicycle>();
     if (model == PF_MODEL_DHARM) return ops_of<DhArm>();
     if (model == PF_MODEL_BEACON) return ops_of<Beacon>();
+    if (model == PF_MODEL_CAMARM) return ops_of<CamArm>();
     return ops_of<RefArm>();
 }
 

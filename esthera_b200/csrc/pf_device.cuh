@@ -721,6 +721,7 @@ union ModelParams {
     pf_dharm_params arm;
     pf_refarm_params ref;
     pf_beacon_params bcn;
+    pf_camarm_params cam;
 };
 
 __device__ __forceinline__ float wrap_pi(float a) { return fmaf(-kTwoPi, floorf((a + kPi) * kInvTwoPi), a); }
@@ -924,58 +925,126 @@ struct DhArm {
     }
 };
 
-// The reference's camera robot arm (sampling_iw, src/models/robotarm/cuda/
-// pf_model_soa.cuh:114-184): state angles[5], x, y, vX, vY; normals in the
-// same variable order; log weight = -(sum 0.1 e^2) (the reference returns its exp).
+// The reference's camera robot arm: the planar chain of sampling_iw
+// (src/models/robotarm/cuda/pf_model_soa.cuh:114-184): state angles[5], x, y,
+// vX, vY; normals in the same variable order.  Propagates the particle in
+// place, returns the angle part of the error value (sum 0.1 e^2) and the
+// camera coordinates (cx, cy, cz) of the cart in the last link's frame.
+struct ArmConsts {
+    float dt;
+    float cdt[5];
+    float z[7];
+};
+
+__device__ static void arm_prepare(ArmConsts& c, const pf_step_input& in, float dt_default)
+{
+    c.dt = in.dt > 0.0f ? in.dt : dt_default;
+    for (int i = 0; i < 5; ++i) c.cdt[i] = in.control[i] * c.dt;
+    for (int i = 0; i < 7; ++i) c.z[i] = in.meas[i];
+}
+
+__device__ __forceinline__ float arm_chain(const ArmConsts& c, float* s, const float* n, float* sn, float* cs,
+                                           float& cx, float& cy, float& cz)
+{
+    const float arm[5] = {0.0f, 3.0f, 3.0f, 3.0f, 3.0f};
+    const float vX = s[7], vY = s[8];
+    const float x = fmaf(n[5], 0.2f, fmaf(vX, c.dt, s[5]));
+    const float y = fmaf(n[6], 0.2f, fmaf(vY, c.dt, s[6]));
+    s[5] = x;
+    s[6] = y;
+    s[7] = fmaf(n[7], 2.0f, vX);
+    s[8] = fmaf(n[8], 2.0f, vY);
+    float value = 0.0f;
+    cx = 0.0f;
+    cy = 0.0f;
+    cz = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const float ang = fmaf(n[i], 0.2f, s[i] + c.cdt[i]);
+        s[i] = ang;
+        float sf, cf;
+        __sincosf(ang, &sf, &cf);
+        sn[i] = sf;
+        cs[i] = cf;
+        if (i == 0) {
+            cx = fmaf(x, cf, y * sf);
+            cy = fmaf(-x, sf, y * cf);
+            cz = 0.0f;
+        } else {
+            const float nb = fmaf(cy, cf, -(cz * sf)), nc = fmaf(cy, sf, cz * cf);
+            cy = nb;
+            cz = nc - arm[i];
+        }
+        const float e = ang - c.z[i];
+        value = fmaf(e * e, 0.1f, value);
+    }
+    return value;
+}
+
+// The reference's camera arm (sampling_iw, pf_model_soa.cuh:114-184): the cart
+// position in the camera frame is measured directly; log weight =
+// -(sum 0.1 e^2) (the reference returns its exp).
 struct RefArm {
     static constexpr int S = 9, K = 9, NA = 5;
     __host__ __device__ static constexpr int angle_var(int a) { return a; }
-    struct Consts {
-        float dt;
-        float cdt[5];
-        float z[7];
-    };
+    using Consts = ArmConsts;
     __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
     {
-        if (lane != 0) return;
-        c.dt = in.dt > 0.0f ? in.dt : mp.ref.dt;
-        for (int i = 0; i < 5; ++i) c.cdt[i] = in.control[i] * c.dt;
-        for (int i = 0; i < 7; ++i) c.z[i] = in.meas[i];
+        if (lane == 0) arm_prepare(c, in, mp.ref.dt);
     }
     __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
                                                  float* cs)
     {
-        const float arm[5] = {0.0f, 3.0f, 3.0f, 3.0f, 3.0f};
-        const float vX = s[7], vY = s[8];
-        const float x = fmaf(n[5], 0.2f, fmaf(vX, c.dt, s[5]));
-        const float y = fmaf(n[6], 0.2f, fmaf(vY, c.dt, s[6]));
-        s[5] = x;
-        s[6] = y;
-        s[7] = fmaf(n[7], 2.0f, vX);
-        s[8] = fmaf(n[8], 2.0f, vY);
-        float value = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-            const float ang = fmaf(n[i], 0.2f, s[i] + c.cdt[i]);
-            s[i] = ang;
-            float sf, cf;
-            __sincosf(ang, &sf, &cf);
-            sn[i] = sf;
-            cs[i] = cf;
-            if (i == 0) {
-                cx = fmaf(x, cf, y * sf);
-                cy = fmaf(-x, sf, y * cf);
-                cz = 0.0f;
-            } else {
-                const float nb = fmaf(cy, cf, -(cz * sf)), nc = fmaf(cy, sf, cz * cf);
-                cy = nb;
-                cz = nc - arm[i];
-            }
-            const float e = ang - c.z[i];
-            value = fmaf(e * e, 0.1f, value);
-        }
+        float cx, cy, cz;
+        float value = arm_chain(c, s, n, sn, cs, cx, cy, cz);
         value = fmaf((cx - c.z[5]) * (cx - c.z[5]), 0.1f, value);
         value = fmaf((cy - c.z[6]) * (cy - c.z[6]), 0.1f, value);
+        return -value;
+    }
+};
+
+// The reference's pinhole-camera variant of the arm (sampling_iw,
+// src/models/robotarm/cuda/pf_model_soa_packed_code.cuh:61-145): the same
+// chain, then the cart's camera coordinates are projected, x_n = cx / cz,
+// y_n = cy / cz, distorted (radial kc1, kc2; tangential kc3, kc4) and mapped
+// to pixels (xp = fc_x xd + cc_x, yp = fc_y yd + cc_y); the measured x, y
+// are pixels.  Log weight = -(sum 0.1 e^2).
+struct CamArm {
+    static constexpr int S = 9, K = 9, NA = 5;
+    __host__ __device__ static constexpr int angle_var(int a) { return a; }
+    struct Consts {
+        ArmConsts a;
+        float fx, fy, ux, uy, k1, k2, k3, k4;
+    };
+    __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
+    {
+        if (lane != 0) return;
+        const pf_camarm_params& p = mp.cam;
+        arm_prepare(c.a, in, p.dt);
+        c.fx = p.fc[0];
+        c.fy = p.fc[1];
+        c.ux = p.cc[0];
+        c.uy = p.cc[1];
+        c.k1 = p.kc[0];
+        c.k2 = p.kc[1];
+        c.k3 = p.kc[2];
+        c.k4 = p.kc[3];
+    }
+    __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
+                                                 float* cs)
+    {
+        float cx, cy, cz;
+        float value = arm_chain(c.a, s, n, sn, cs, cx, cy, cz);
+        const float xn = cx / cz, yn = cy / cz;
+        const float xx = xn * xn, yy = yn * yn, xy = xn * yn;
+        const float r2 = xx + yy;
+        const float dxx = fmaf(2.0f * c.k3, xy, c.k4 * fmaf(3.0f, xx, yy));
+        const float dxy = fmaf(c.k3, fmaf(3.0f, yy, xx), 2.0f * c.k4 * xy);
+        const float rad = fmaf(c.k2 * r2, r2, fmaf(c.k1, r2, 1.0f));
+        const float xp = fmaf(c.fx, fmaf(rad, xn, dxx), c.ux);
+        const float yp = fmaf(c.fy, fmaf(rad, yn, dxy), c.uy);
+        value = fmaf((xp - c.a.z[5]) * (xp - c.a.z[5]), 0.1f, value);
+        value = fmaf((yp - c.a.z[6]) * (yp - c.a.z[6]), 0.1f, value);
         return -value;
     }
 };

@@ -1,0 +1,6 @@
+// Kernel instantiations: the fused sample+weight+sort kernel for the reference's pinhole-camera arm (lens distortion).
+#define PF_PART_K1
+#include "pf_launch_impl.cuh"
+namespace pfdev {
+template cudaError_t Launch<CamArm>::sample_sort(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
+}  // namespace pfdev

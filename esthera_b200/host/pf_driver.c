@@ -32,7 +32,7 @@ pf_status pf_read_trace_line(void* file, pf_model_id model, pf_step_input* out, 
         memcpy(actual_out, a, sizeof(a));
         return PF_OK;
     }
-    if (model != PF_MODEL_REFARM) return PF_ERR_UNSUPPORTED;
+    if (model != PF_MODEL_REFARM && model != PF_MODEL_CAMARM) return PF_ERR_UNSUPPORTED;
     pf_step_input in;
     float actual[9];
     memset(&in, 0, sizeof(in));

@@ -109,6 +109,27 @@ pf_status pf_beacon_default_params(pf_beacon_params* p)
     return PF_OK;
 }
 
+/* The reference pinhole camera's calibration
+ * (src/models/robotarm/cuda/pf_model_soa_packed_code.cuh:33-42) and the
+ * robot-arm start state (angles 3/4 pi, x = 7). */
+pf_status pf_camarm_default_params(pf_camarm_params* p)
+{
+    if (!p) return PF_ERR_INVALID;
+    memset(p, 0, sizeof(*p));
+    p->dt = 1.0f;
+    for (int i = 0; i < 5; ++i) p->init_state[i] = (float)(0.75 * M_PI);
+    p->init_state[5] = 7.0f;
+    p->fc[0] = 408.65831f;
+    p->fc[1] = 409.69059f;
+    p->cc[0] = 166.32611f;
+    p->cc[1] = 108.93539f;
+    p->kc[0] = -0.21561f;
+    p->kc[1] = 1.60704f;
+    p->kc[2] = -0.01291f;
+    p->kc[3] = 0.00007f;
+    return PF_OK;
+}
+
 /* Forward kinematics of the standard DH chain: position p[3] and ZYX yaw/pitch/roll. */
 static void dh_fk(const pf_dharm_params* P, const double* q, double* out6)
 {

@@ -48,9 +48,10 @@ typedef enum {
     PF_MODEL_UNICYCLE = 0, /* (x, y, theta), range/bearing to landmarks */
     PF_MODEL_DHARM = 1,    /* 6-joint Denavit-Hartenberg arm, q[6] + qdot[6] */
     PF_MODEL_REFARM = 2,   /* the reference's 5-angle camera arm on a cart */
-    PF_MODEL_BEACON = 3    /* the reference's unicycle tracked by range-only beacons (x, y, theta) */
+    PF_MODEL_BEACON = 3,   /* the reference's unicycle tracked by range-only beacons (x, y, theta) */
+    PF_MODEL_CAMARM = 4    /* the reference's camera arm seen through a pinhole camera with lens distortion */
 } pf_model_id;
-#define PF_NUM_MODELS 4
+#define PF_NUM_MODELS 5
 
 typedef enum {
     PF_EXCHANGE_NONE = 0,
@@ -119,6 +120,7 @@ typedef struct {
  *   dharm:    control {};                 meas {px, py, pz, yaw, pitch, roll}
  *   refarm:   control {joint rates[5]};   meas {angles[5], x, y}
  *   beacon:   control {v, omega};         meas {range[L]}
+ *   camarm:   control {joint rates[5]};   meas {angles[5], pixel x, pixel y}
  * dt <= 0 uses the model's dt. */
 typedef struct {
     float dt;
@@ -178,6 +180,23 @@ typedef struct {
     float beacons[16][3];        /* beacon positions (x, y, z) */
     float init_state[3];         /* x, y, theta */
 } pf_beacon_params;
+
+/* The reference's pinhole-camera variant of the arm
+ * (src/models/robotarm/cuda/pf_model_soa_packed_code.cuh:61-145): the
+ * refarm chain, then the cart's camera coordinates (cx, cy, cz) are
+ * projected, xn = cx/cz, yn = cy/cz, r2 = xn^2 + yn^2, distorted
+ * xd = (1 + kc1 r2 + kc2 r2^2) xn + 2 kc3 xn yn + kc4 (3 xn^2 + yn^2),
+ * yd = (1 + kc1 r2 + kc2 r2^2) yn + kc3 (3 yn^2 + xn^2) + 2 kc4 xn yn, and
+ * mapped to pixels (fc_x xd + cc_x, fc_y yd + cc_y).  Log weight
+ * -(sum 0.1 e^2).  pf_camarm_default_params gives the reference's
+ * calibration (:33-42), dt = 1 and the refarm start state. */
+typedef struct {
+    float dt;
+    float init_state[9];         /* angles[5], x, y, vX, vY */
+    float fc[2];                 /* focal lengths (pixels) */
+    float cc[2];                 /* principal point (pixels) */
+    float kc[4];                 /* radial kc1, kc2; tangential kc3, kc4 */
+} pf_camarm_params;
 
 typedef struct pf_filter pf_filter;
 
@@ -475,14 +494,17 @@ pf_status pf_unicycle_default_params(uint32_t seed, int32_t num_landmarks, pf_un
 pf_status pf_dharm_default_params(uint32_t seed, pf_dharm_params* p);
 /* The reference unicycle program's constants (particle_filter.cu:60-76, 708-716). */
 pf_status pf_beacon_default_params(pf_beacon_params* p);
+/* The reference's camera calibration (pf_model_soa_packed_code.cuh:33-42). */
+pf_status pf_camarm_default_params(pf_camarm_params* p);
 /* steps x pf_step_input and steps x num_state truth floats. */
 pf_status pf_make_trace(pf_model_id model, const void* params, uint32_t seed, int32_t steps,
                         pf_step_input* inputs, float* truth);
 
 /* ---- reference-compatible driver (reference trace files, C host) ---- */
-/* Parses one line of a reference trace.  PF_MODEL_REFARM: robot-arm format
- * "x y angles[5] controls[5] dt actual_x actual_y actual_angles[5]"
- * (pf_model_soa.cuh:276-301).  PF_MODEL_BEACON: unicycle format
+/* Parses one line of a reference trace.  PF_MODEL_REFARM and PF_MODEL_CAMARM:
+ * robot-arm format "x y angles[5] controls[5] dt actual_x actual_y
+ * actual_angles[5]" (pf_model_soa.cuh:276-301; pf_model_soa_packed_code.c:57-82,
+ * where x y are pixels).  PF_MODEL_BEACON: unicycle format
  * "ranges[10] v omega dt actual_x actual_y actual_theta"
  * (src/models/unicycle/particle_filter.cu:756-772).  Returns PF_OK, or
  * PF_ERR_IO at end of file / bad line. */

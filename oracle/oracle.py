@@ -18,7 +18,7 @@ REF_LIB = HERE / "_ref" / "libmtgp_ref.so"
 RES_REF, RES_SYSTEMATIC, RES_VOSE = 0, 1, 2
 RNG_REFLAYOUT, RNG_SUBFILTER = 0, 1
 EXCH_NONE, EXCH_RING, EXCH_TORUS, EXCH_ALL2ALL = 0, 1, 2, 3
-MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON = 0, 1, 2, 3
+MODEL_UNICYCLE, MODEL_DHARM, MODEL_REFARM, MODEL_BEACON, MODEL_CAMARM = 0, 1, 2, 3, 4
 MASK_PARAMS, MASK_CUDA_REF = 0, 0xFF800000
 
 
@@ -28,7 +28,8 @@ class OrcModel(C.Structure):
                 ("num_landmarks", C.c_int), ("lm", (C.c_double * 2) * 8),
                 ("sigma_qd", C.c_double), ("sigma_p", C.c_double), ("sigma_a", C.c_double),
                 ("a", C.c_double * 6), ("alpha", C.c_double * 6), ("d", C.c_double * 6),
-                ("bnoise", C.c_double * 3), ("num_beacons", C.c_int), ("bc", (C.c_double * 3) * 16)]
+                ("bnoise", C.c_double * 3), ("num_beacons", C.c_int), ("bc", (C.c_double * 3) * 16),
+                ("fc", C.c_double * 2), ("cc", C.c_double * 2), ("kc", C.c_double * 4)]
 
 
 class OrcFilter(C.Structure):
@@ -270,6 +271,13 @@ def model_from_params(model, p):
         for j in range(16):
             for k in range(3):
                 md.bc[j][k] = p.beacons[j][k]
+    elif model == MODEL_CAMARM:
+        md.num_state, md.num_noise = 9, 9
+        md.dt = p.dt
+        for i in range(2):
+            md.fc[i], md.cc[i] = p.fc[i], p.cc[i]
+        for i in range(4):
+            md.kc[i] = p.kc[i]
     else:
         md.num_state, md.num_noise = 9, 9
         md.dt = p.dt

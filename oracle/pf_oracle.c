@@ -453,10 +453,12 @@ static double dharm_step(const orc_model* md, float* s, const float* n, const fl
 /* The reference's robot-arm model (sampling_iw, src/models/robotarm/cuda/
  * pf_model_soa.cuh:114-184): 5 joint angles + cart (x, y, vX, vY), planar
  * camera chain, likelihood exp(-sum 0.1 e^2).  Returns log of that weight. */
-static double refarm_step(const orc_model* md, float* s, const float* n, const float* c,
-                          const float* z)
+/* The arm chain shared by the reference's arm and its pinhole-camera variant:
+ * propagates the particle in place, returns the angle part of the error
+ * value and the cart's camera coordinates in cam[3]. */
+static double arm_chain(const orc_model* md, float* s, const float* n, const float* c, const float* z,
+                        double* cam)
 {
-    (void)md;
     const double dt = md->dt;
     const double arm[5] = {0, 3, 3, 3, 3};
     double vx = s[7], vy = s[8];
@@ -485,8 +487,39 @@ static double refarm_step(const orc_model* md, float* s, const float* n, const f
         double e = a - z[i];
         value += e * e * 0.1;
     }
-    value += (cx - z[5]) * (cx - z[5]) * 0.1;
-    value += (cy - z[6]) * (cy - z[6]) * 0.1;
+    cam[0] = cx;
+    cam[1] = cy;
+    cam[2] = cz;
+    return value;
+}
+
+/* The reference's pinhole-camera arm (sampling_iw, src/models/robotarm/cuda/
+ * pf_model_soa_packed_code.cuh:61-145): the arm chain, the cart's camera
+ * coordinates projected (x/z, y/z), distorted (radial kc1, kc2; tangential
+ * kc3, kc4) and mapped to pixels; log of the weight exp(-sum 0.1 e^2). */
+static double camarm_step(const orc_model* md, float* s, const float* n, const float* c,
+                          const float* z)
+{
+    double cam[3];
+    double value = arm_chain(md, s, n, c, z, cam);
+    const double xn = cam[0] / cam[2], yn = cam[1] / cam[2];
+    const double r2 = xn * xn + yn * yn;
+    const double rad = 1.0 + md->kc[0] * r2 + md->kc[1] * r2 * r2;
+    const double xd = rad * xn + 2.0 * md->kc[2] * xn * yn + md->kc[3] * (3.0 * xn * xn + yn * yn);
+    const double yd = rad * yn + md->kc[2] * (3.0 * yn * yn + xn * xn) + 2.0 * md->kc[3] * xn * yn;
+    const double xp = md->fc[0] * xd + md->cc[0], yp = md->fc[1] * yd + md->cc[1];
+    value += (xp - z[5]) * (xp - z[5]) * 0.1;
+    value += (yp - z[6]) * (yp - z[6]) * 0.1;
+    return -value;
+}
+
+static double refarm_step(const orc_model* md, float* s, const float* n, const float* c,
+                          const float* z)
+{
+    double cam[3];
+    double value = arm_chain(md, s, n, c, z, cam);
+    value += (cam[0] - z[5]) * (cam[0] - z[5]) * 0.1;
+    value += (cam[1] - z[6]) * (cam[1] - z[6]) * 0.1;
     return -value;
 }
 
@@ -533,6 +566,7 @@ double orc_model_step(const orc_model* md, float* state, const float* noise, con
     case ORC_MODEL_UNICYCLE: return unicycle_step(md, state, noise, control, meas);
     case ORC_MODEL_DHARM: return dharm_step(md, state, noise, control, meas);
     case ORC_MODEL_BEACON: return beacon_step(md, state, noise, control, meas);
+    case ORC_MODEL_CAMARM: return camarm_step(md, state, noise, control, meas);
     default: return refarm_step(md, state, noise, control, meas);
     }
 }

@@ -108,6 +108,7 @@ void orc_exchange_sources(int mode, int N, int m, int t, const float* top_keys, 
 #define ORC_MODEL_DHARM 1
 #define ORC_MODEL_REFARM 2
 #define ORC_MODEL_BEACON 3
+#define ORC_MODEL_CAMARM 4
 
 typedef struct {
     int model;
@@ -125,13 +126,16 @@ typedef struct {
     double bnoise[3];
     int num_beacons;
     double bc[16][3];
+    /* camera arm: focal lengths, principal point, distortion kc1..kc4 */
+    double fc[2], cc[2], kc[4];
 } orc_model;
 
 /* control / measurement as flat float arrays:
  *   unicycle: control {v, omega}; measurement {range[L], bearing[L]}
  *   dharm:    control {} ;        measurement {px,py,pz,yaw,pitch,roll}
  *   refarm:   control {angles[5]}; measurement {angles[5], x, y}
- *   beacon:   control {v, omega}; measurement {range[L]} */
+ *   beacon:   control {v, omega}; measurement {range[L]}
+ *   camarm:   control {angles[5]}; measurement {angles[5], pixel x, pixel y} */
 
 /* Propagate one particle in place (state has num_state floats, noise has
  * num_noise normals) and return its log-likelihood.  Double precision. */

@@ -112,3 +112,33 @@ def unicycle_sampling(state, normals, v, w, dt, ranges):
     wt = np.zeros(n, np.float32)
     _check(_ulib.ref_unicycle_sampling(_f(st), _f(nz), v, w, dt, _f(z), n, _f(so), _f(wt)), "ref_unicycle_sampling")
     return so, wt
+
+
+# ---- the reference's pinhole-camera arm model (oracle/build_ref_camarm.sh) ----
+CAMARM_LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libref_camarm.so"
+_clib = None
+
+
+def camarm_available():
+    return CAMARM_LIB_PATH.exists()
+
+
+def camarm_sampling(state, normals, controls, meas, dt):
+    """The reference's pinhole-camera sampling_iw on n particles (n a multiple of
+    256): (state out, 9 x n; linear weight __expf(-value), n)."""
+    global _clib
+    if _clib is None:
+        L = C.CDLL(str(CAMARM_LIB_PATH))
+        fp = C.POINTER(C.c_float)
+        L.ref_camarm_sampling.argtypes = [fp, fp, fp, fp, C.c_float, C.c_int, fp, fp]
+        L.ref_camarm_sampling.restype = C.c_int
+        _clib = L
+    st = np.ascontiguousarray(state, np.float32)
+    nz = np.ascontiguousarray(normals, np.float32)
+    c = np.ascontiguousarray(controls[:5], np.float32)
+    z = np.ascontiguousarray(meas[:7], np.float32)
+    n = st.shape[1]
+    so = np.zeros_like(st)
+    wt = np.zeros(n, np.float32)
+    _check(_clib.ref_camarm_sampling(_f(st), _f(nz), _f(c), _f(z), dt, n, _f(so), _f(wt)), "ref_camarm_sampling")
+    return so, wt

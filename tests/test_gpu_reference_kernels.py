@@ -142,3 +142,31 @@ def test_beacon_model_equals_reference_kernel(gpu, w0, dt):
     assert ok.mean() > 0.5
     lr = np.log(wt[ok].astype(np.float64))
     assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
+
+
+@pytest.mark.skipif(not R.camarm_available(), reason="oracle/_ref/libref_camarm.so not built "
+                                                   "(oracle/build_ref_camarm.sh needs the reference tree)")
+@pytest.mark.parametrize("ang", [1.2, 2.0])
+def test_camarm_model_equals_reference_kernel(gpu, O, ang):
+    """The engine's camera-arm model against the reference's own pinhole-camera
+    sampling_iw (pf_model_soa_packed_code.cuh:61-145) on the same particles,
+    normals, controls and pixel measurements: states within 2e-5,
+    log-likelihoods within 1e-4 relative + 5e-3 absolute of log(weight)."""
+    import test_camarm as T
+    E = gpu
+    p = E.camarm_params()
+    rng = np.random.default_rng(int(ang * 100))
+    n = 4096
+    st = T.cloud(rng, n, ang)
+    nz = (0.1 * rng.standard_normal((9, n))).astype(np.float32)
+    inp = np.zeros(1, E.STEP_INPUT_DTYPE)[0]
+    inp["dt"] = 1.0
+    inp["control"][:5] = rng.normal(0, 0.02, 5)
+    inp["meas"][:7] = T.measurement(O, p, ang)
+    so, ll = E.model_step(E.MODEL_CAMARM, p, inp, st, nz)
+    sr, wt = R.camarm_sampling(st, nz, inp["control"], inp["meas"], 1.0)
+    assert np.allclose(so, sr, atol=2e-5, rtol=0)
+    ok = wt > 1e-30
+    assert ok.mean() > 0.5
+    lr = np.log(wt[ok].astype(np.float64))
+    assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
