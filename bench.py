@@ -9,7 +9,9 @@ seed 2, 1000 steps.  Inputs (controls and range/bearing measurements to 4
 landmarks) are synthetic, generated from the seed.  A "step" is one full
 filter step over all 2^20 particles.
 --workload arm: the 6-joint DH arm, 2^18 particles = 1024 x 256 on a 32 x 32
-torus, t = 1, seed 3.  --workload batched / served: the batched uneven
+torus, t = 1, seed 3.  --workload beacon: the reference unicycle program's
+range-only model (10 beacons) at the plain workload's shape and seed.
+--workload batched / served: the batched uneven
 filters and the served tracking load (their own JSON lines).
 
 value:  device-timed (CUDA events on the filter's stream), inputs resident
@@ -56,6 +58,8 @@ WORKLOADS = {
                   desc="unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2"),
     "arm": dict(model=1, m=256, nsub=1024, t=1, seed=3, alg=96, angles=(0, 1, 2, 3, 4, 5),
                 desc="6-joint DH arm 2^18 particles = 1024 sub-filters x 256, torus 32x32, t=1"),
+    "beacon": dict(model=3, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(),
+                   desc="10-beacon range-only unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2"),
 }
 CONFIGS = {
     "systematic": 1,
@@ -121,6 +125,8 @@ def visible_gpu_index(local_rank):
 
 
 def model_params(E, W):
+    if W["model"] == 3:
+        return E.beacon_params()
     return E.unicycle_params(W["seed"]) if W["model"] == 0 else E.dharm_params(W["seed"])
 
 
@@ -316,7 +322,7 @@ def main():
     ap.add_argument("--phase-steps", type=int, default=100, help="steps of the per-kernel timing pass")
     ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
-    ap.add_argument("--workload", default="plain", choices=["plain", "arm", "batched", "served"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "arm", "beacon", "batched", "served"])
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--batch-filters", type=int, default=4096)
