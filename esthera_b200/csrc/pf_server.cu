@@ -289,14 +289,23 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
         cudaGetLastError();
         pf_unicycle_params up;
         pf_dharm_params ap;
+        pf_refarm_params rp;
+        pf_beacon_params bp;
+        pf_camarm_params cp;
         pf_unicycle_default_params(1, 4, &up);
         pf_dharm_default_params(1, &ap);
-        const void* params[2] = {&up, &ap};
-        const size_t sizes[2] = {sizeof(up), sizeof(ap)};
+        pf_camarm_default_params(&cp);
+        pf_beacon_default_params(&bp);
+        memset(&rp, 0, sizeof(rp));
+        rp.dt = cp.dt;
+        memcpy(rp.init_state, cp.init_state, sizeof(rp.init_state));
+        const void* params[PF_NUM_MODELS] = {&up, &ap, &rp, &bp, &cp};
+        const size_t sizes[PF_NUM_MODELS] = {sizeof(up), sizeof(ap), sizeof(rp), sizeof(bp), sizeof(cp)};
+        static_assert(PF_MODEL_REFARM == 2 && PF_MODEL_BEACON == 3 && PF_MODEL_CAMARM == 4, "warm-up table order");
         pf_step_input in;
         memset(&in, 0, sizeof(in));
         pf_server_result res;
-        for (int m = 0; m < 2; ++m) {
+        for (int m = 0; m < PF_NUM_MODELS; ++m) {
             int32_t id = -1, n = 0;
             pf_status w = pf_server_open(s, (pf_model_id)m, params[m], sizes[m], M, 1u, &id);
             if (w == PF_ERR_ADMISSION) continue;  // a budget below one filter: nothing to warm

@@ -16,13 +16,14 @@ import pytest
 CAM = 4
 
 
-def cloud(rng, n, ang=1.2):
-    """Particles around angles `ang`, cart (7, 0): the camera sees the cart in front (cz > 0)."""
+def cloud(rng, n, ang=1.2, spread=0.05):
+    """Particles around angles `ang`, cart (7, 0), cart speed ~ spread: the
+    camera sees the cart at a finite depth (cz away from 0)."""
     st = np.zeros((9, n), np.float32)
-    st[:5] = ang + 0.05 * rng.standard_normal((5, n))
-    st[5] = 7 + 0.1 * rng.standard_normal(n)
-    st[6] = 0.1 * rng.standard_normal(n)
-    st[7:] = 0.05 * rng.standard_normal((2, n))
+    st[:5] = ang + spread * rng.standard_normal((5, n))
+    st[5] = 7 + 2 * spread * rng.standard_normal(n)
+    st[6] = 2 * spread * rng.standard_normal(n)
+    st[7:] = spread * rng.standard_normal((2, n))
     return st
 
 
