@@ -158,3 +158,36 @@ def test_camarm_pipelines_agree(gpu, O, res):
         assert np.array_equal(u["best"], w["best"]) and u["best_subfilter"] == w["best_subfilter"], k
         assert np.allclose(u["mean"], w["mean"], rtol=1e-12, atol=1e-12), k
     assert np.array_equal(a.particles(), b.particles())
+
+
+@pytest.mark.gpu
+def test_camarm_batch_and_server_equal_single_filters(gpu, O):
+    """Camera-arm filters in a batch and in the server reproduce pf_filter bit for bit."""
+    E = gpu
+    p = E.camarm_params()
+    for i in range(5):
+        p.init_state[i] = 2.0
+    rec = np.zeros(4, E.STEP_INPUT_DTYPE)
+    rec["dt"] = 1.0
+    rec["meas"][:, :7] = measurement(O, p, 2.0)
+    counts = [512, 256]
+    cfg = dict(num_transfer=1, exchange=1, resampler=1, particles_per_thread=4)
+    B = E.FilterBatch(CAM, [p, p], counts, particles_per_subfilter=256, **cfg)
+    best = [B.step(np.stack([rec[k], rec[k]])) for k in range(4)]
+    for f, n in enumerate(counts):
+        s = E.ParticleFilter(CAM, p, pipeline=E.PIPELINE_SPLIT, particles_per_subfilter=256, num_subfilters=n // 256,
+                             stream_offset=B.filter_info(f)["stream_offset"], **cfg)
+        for k in range(4):
+            e = s.step(rec[k])
+            assert np.array_equal(best[k][f]["mean"], e["mean"]) and best[k][f]["log_norm"] == e["log_norm"], (f, k)
+    srv = E.Server(1 << 30, 4, particles_per_subfilter=256, particles_per_thread=4, num_transfer=1, exchange=1)
+    fid = srv.open(CAM, p, 512, 9)
+    s = E.ParticleFilter(CAM, p, pipeline=E.PIPELINE_SPLIT, particles_per_subfilter=256, num_subfilters=2, seed=9,
+                         particles_per_thread=4, num_transfer=1, exchange=1)
+    for k in range(4):
+        srv.update(fid, rec[k], tag=k)
+        srv.launch()
+        r = srv.poll()[0]["estimate"]
+        e = s.step(rec[k])
+        assert np.array_equal(r["mean"], e["mean"]) and r["log_norm"] == e["log_norm"], k
+    srv.close()
