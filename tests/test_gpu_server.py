@@ -202,3 +202,50 @@ def test_server_snapshot_restore_moves_a_filter(gpu):
     assert np.array_equal(dst.particles(b, 2048)[0], src.particles(a, 2048)[0])
     src.close()
     dst.close()
+
+
+@pytest.mark.gpu
+def test_server_cancel_queued_updates(gpu):
+    """A request cancelled on the host: closing a filter drops its queued
+    updates (no result comes back for them), is refused while one of its
+    updates is on the GPU, leaves the other filters' results unchanged, and
+    its slot serves a new filter from a clean state."""
+    E = gpu
+    p, inputs, _ = trace(E, UNI, 61, 4)
+    q, qin, _ = trace(E, UNI, 62, 4)
+    alone, _ = run_alone(E, UNI, q, 1024, 62, qin)
+    srv = E.Server(1 << 30, 4, **CFG)
+    a = srv.open(UNI, p, 2048, 61)
+    b = srv.open(UNI, q, 1024, 62)
+    srv.update(a, inputs[0], tag=0)
+    srv.update(b, qin[0], tag=100)
+    assert srv.launch() == 2
+    with pytest.raises(E.PFError) as ei:
+        srv.close_filter(a)  # its update is on the GPU
+    assert ei.value.status == E.PF_ERR_BUSY
+    got_b = {}
+    for r in srv.poll():
+        if r["filter"] == b:
+            got_b[int(r["tag"]) - 100] = r["estimate"]
+    for k in (1, 2, 3):
+        srv.update(a, inputs[k], tag=k)
+    assert srv.stats()["queued_updates"] == 3
+    srv.close_filter(a)  # cancels its three queued updates
+    assert srv.stats()["queued_updates"] == 0 and srv.stats()["open_filters"] == 1
+    for k in (1, 2, 3):
+        srv.update(b, qin[k], tag=100 + k)
+        assert srv.launch() == 1
+        rs = srv.poll()
+        assert len(rs) == 1 and rs[0]["filter"] == b
+        got_b[k] = rs[0]["estimate"]
+    for k in range(4):
+        assert same(got_b[k], alone[k]), k
+    # the freed slot serves a new filter from its initial state
+    c = srv.open(UNI, p, 2048, 61)
+    srv.update(c, inputs[0], tag=7)
+    srv.launch()
+    rc = srv.poll()[0]
+    assert rc["filter"] == c and rc["step"] == 1
+    first, _ = run_alone(E, UNI, p, 2048, 61, inputs[:1])
+    assert same(rc["estimate"], first[0])
+    srv.close()
