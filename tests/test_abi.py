@@ -137,3 +137,26 @@ def test_read_trace_line_reference_format(E, tmp_path):
 
 def test_cli_binary_built():
     assert (ROOT / "esthera_b200" / "pf_cli").exists()
+
+
+def test_driver_trace_errors_on_the_host(E, tmp_path):
+    """Malformed or missing traces fail with PF_ERR_IO before any GPU work (no
+    exit(), unlike the reference's drivers); an unknown model's trace is
+    PF_ERR_UNSUPPORTED."""
+    assert E.lib().pf_particle_filter(64, 2, 1, 1.0, str(tmp_path / "absent").encode(), None) == E.PF_ERR_IO
+    assert E.lib().pf_beacon_particle_filter(64, 2, 1, str(tmp_path / "absent").encode(), None) == E.PF_ERR_IO
+    fn = tmp_path / "bad"
+    fn.write_text("0.5 1.5 2.0 2.1 oops 2.3 2.4\n")
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    inp = E.StepInput()
+    act = np.zeros(16, np.float32)
+    fp = libc.fopen(str(fn).encode(), b"r")
+    for model, want in [(E.MODEL_REFARM, E.PF_ERR_IO), (E.MODEL_UNICYCLE, E.PF_ERR_UNSUPPORTED)]:
+        got = E.lib().pf_read_trace_line(fp, model, C.byref(inp), act.ctypes.data_as(C.POINTER(C.c_float)))
+        assert got == want, (model, got)
+    libc.fclose(fp)
+    assert E.lib().pf_read_trace_line(None, E.MODEL_REFARM, C.byref(inp),
+                                      act.ctypes.data_as(C.POINTER(C.c_float))) == E.PF_ERR_INVALID
