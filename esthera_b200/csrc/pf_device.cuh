@@ -1131,6 +1131,47 @@ struct Beacon {
         }
         return fmaf(-c.h, acc, c.lnorm);
     }
+    // E particles at once: step()'s per-particle arithmetic in the same order
+    // (bit-identical results), the beacon loop outside the particle loop so
+    // each beacon's constants are read once per thread and the E range
+    // chains interleave.  noise(e, v) gives particle e's v-th normal.
+    template <int E, class Noise>
+    __device__ static __forceinline__ void step_batch(const Consts& c, float (&s)[E][S], Noise noise,
+                                                      float (&sn)[E][NA], float (&cs)[E][NA], float (&ll)[E])
+    {
+        float acc[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const float v = fmaf(c.nv, noise(e, 0), c.v);
+            const float w = fmaf(c.nw, noise(e, 1), c.w);
+            const float g = c.ng * noise(e, 2);
+            const float ha = w * c.hdt;
+            const float k = v * c.dt * sinc(ha);
+            float sm, cm;
+            __sincosf(s[e][2] + ha, &sm, &cm);
+            const float nx = fmaf(k, cm, s[e][0]);
+            const float ny = fmaf(k, sm, s[e][1]);
+            const float nt = wrap_pi(fmaf(g, c.dt, fmaf(w, c.dt, s[e][2])));
+            s[e][0] = nx;
+            s[e][1] = ny;
+            s[e][2] = nt;
+            __sincosf(nt, &sn[e][0], &cs[e][0]);
+            acc[e] = 0.0f;
+        }
+        const int L = c.L;
+#pragma unroll 1
+        for (int j = 0; j < L; ++j) {
+            const float bx = c.bx[j], by = c.by[j], bz2 = c.bz2[j], z = c.z[j];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const float dx = s[e][0] - bx, dy = s[e][1] - by;
+                const float r = pf_sqrt(fmaf(dx, dx, fmaf(dy, dy, bz2))) - z;
+                acc[e] = fmaf(r, r, acc[e]);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) ll[e] = fmaf(-c.h, acc[e], c.lnorm);
+    }
 };
 
 template <class Mdl>
