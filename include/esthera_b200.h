@@ -506,8 +506,9 @@ pf_status pf_make_trace(pf_model_id model, const void* params, uint32_t seed, in
  * actual_angles[5]" (pf_model_soa.cuh:276-301; pf_model_soa_packed_code.c:57-82,
  * where x y are pixels).  PF_MODEL_BEACON: unicycle format
  * "ranges[10] v omega dt actual_x actual_y actual_theta"
- * (src/models/unicycle/particle_filter.cu:756-772).  Returns PF_OK, or
- * PF_ERR_IO at end of file / bad line. */
+ * (src/models/unicycle/particle_filter.cu:756-772).  Returns PF_OK,
+ * PF_ERR_IO at end of file / bad line, PF_ERR_UNSUPPORTED for the models
+ * without a reference trace format (unicycle, DH arm). */
 pf_status pf_read_trace_line(void* file, pf_model_id model, pf_step_input* in, float* actual);
 /* The reference's estimate_error for the robot-arm model (pf_model_soa.cuh:303-316). */
 float pf_refarm_estimate_error(const float* est, const float* actual);
