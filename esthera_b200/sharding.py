@@ -135,3 +135,66 @@ def halo_exchange(dist, shard, to_up, to_down):
     for r in dist.batch_isend_irecv(ops):
         r.wait()
     return from_up, from_down
+
+
+# ---------------------------------------------------------------------------
+# Moving served filters between ranks (elasticity).  A filter is snapshotted
+# on its rank (pf_server_snapshot: int64 header {magic, model, particles,
+# sub-filters}, then particles, MTGP32 stream words and the update count),
+# sent, opened on the destination with the same model, parameters and count,
+# and restored there (pf_server_restore); its next updates give the results
+# it would have given at home.
+# ---------------------------------------------------------------------------
+SNAPSHOT_MAGIC = 0x5046535256534E31
+
+
+def snapshot_header(buf):
+    """(model, particles, sub-filters) from a pf_server_snapshot buffer; raises
+    ValueError when the buffer is not one."""
+    h = np.frombuffer(bytes(buf[:32]), dtype=np.int64)
+    if len(h) != 4 or int(h[0]) != SNAPSHOT_MAGIC:
+        raise ValueError("not a served-filter snapshot")
+    return int(h[1]), int(h[2]), int(h[3])
+
+
+def plan_moves(loads):
+    """Rebalance served filters over ranks by particle count.  loads[r] is rank
+    r's list of (filter id, particles).  Greedy: while moving some filter from
+    the most loaded rank to the least loaded one lowers the larger of the two
+    loads, move the largest such filter.  Returns [(src, dst, filter id)]."""
+    per = [dict(l) for l in loads]
+    moves = []
+    while len(per) > 1:
+        tot = [sum(p.values()) for p in per]
+        hi = max(range(len(per)), key=lambda r: (tot[r], -r))
+        lo = min(range(len(per)), key=lambda r: (tot[r], r))
+        best = None
+        for fid, n in sorted(per[hi].items(), key=lambda kv: (-kv[1], kv[0])):
+            if max(tot[hi] - n, tot[lo] + n) < tot[hi]:
+                best = (fid, n)
+                break
+        if best is None:
+            break
+        fid, n = best
+        del per[hi][fid]
+        per[lo][fid] = n
+        moves.append((hi, lo, fid))
+    return moves
+
+
+def send_filter(dist, snap, dst):
+    """Send one snapshot (bytes) to rank dst: its length, then its bytes."""
+    import torch
+    payload = torch.from_numpy(np.frombuffer(bytes(snap), dtype=np.uint8).copy())
+    dist.send(torch.tensor([payload.numel()], dtype=torch.int64), dst, tag=3)
+    dist.send(payload, dst, tag=4)
+
+
+def recv_filter(dist, src):
+    """Receive one snapshot sent by send_filter from rank src (bytes)."""
+    import torch
+    n = torch.zeros(1, dtype=torch.int64)
+    dist.recv(n, src, tag=3)
+    payload = torch.empty(int(n.item()), dtype=torch.uint8)
+    dist.recv(payload, src, tag=4)
+    return payload.numpy().tobytes()

@@ -80,3 +80,79 @@ def test_single_rank_shard_is_whole_torus(O):
     assert np.array_equal(got_s, want_state) and np.array_equal(got_k, want_keys)
     with pytest.raises(ValueError):
         TorusShard(2048, 512, 2, 3, 0)  # 64 rows over 3 ranks
+
+
+def _fake_snapshot(model, particles, m, seed):
+    """A buffer in pf_server_snapshot's layout (header + random body)."""
+    from esthera_b200.sharding import SNAPSHOT_MAGIC
+    body = np.random.default_rng(seed).integers(0, 256, 3 * 4 * particles + 351 * 4 * (particles // m) + 4,
+                                                dtype=np.uint8)
+    hdr = np.array([SNAPSHOT_MAGIC, model, particles, particles // m], np.int64)
+    return hdr.tobytes() + body.tobytes()
+
+
+def test_plan_moves_balances_particles():
+    from esthera_b200.sharding import plan_moves
+    loads = [[(1, 4096), (2, 2048), (3, 1024), (4, 1024)], [(5, 256)], []]
+    moves = plan_moves(loads)
+    per = [dict(l) for l in loads]
+    for src, dst, fid in moves:
+        per[dst][fid] = per[src].pop(fid)
+    tot = [sum(p.values()) for p in per]
+    assert max(tot) == 4096 and sum(tot) == 8448  # the largest filter bounds the maximum
+    assert all(len(set(p)) == len(p) for p in per)
+    assert plan_moves([[(1, 100)], [(2, 90)]]) == []  # no move lowers the maximum
+    assert plan_moves([[(1, 10), (2, 10)]]) == []      # one rank
+
+
+def test_snapshot_header():
+    from esthera_b200.sharding import snapshot_header
+    snap = _fake_snapshot(3, 4096, 512, 1)
+    assert snapshot_header(snap) == (3, 4096, 8)
+    with pytest.raises(ValueError):
+        snapshot_header(b"\0" * 64)
+
+
+def _mover(rank, world, port, q):
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+        from esthera_b200.sharding import plan_moves, recv_filter, send_filter, snapshot_header
+        filters = {10: (0, 2048), 11: (3, 4096), 12: (1, 1024), 13: (4, 512)}  # id: (model, particles)
+        loads = [[(f, n) for f, (_, n) in filters.items()], []]
+        moves = plan_moves(loads)
+        ok = bool(moves)
+        for src, dst, fid in moves:
+            model, n = filters[fid]
+            want = _fake_snapshot(model, n, 256, fid)
+            if rank == src:
+                send_filter(dist, want, dst)
+            elif rank == dst:
+                got = recv_filter(dist, src)
+                ok = ok and got == want and snapshot_header(got) == (model, n, n // 256)
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, ok))
+    except Exception as e:  # report, never hang the parent
+        q.put((rank, repr(e)))
+
+
+def test_move_filters_between_ranks():
+    """Rebalancing plan + snapshot transport over 2 gloo ranks: every moved
+    filter's snapshot arrives byte for byte with its header intact."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mover, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert all(v is True for v in res.values()), res
