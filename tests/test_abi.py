@@ -160,3 +160,15 @@ def test_driver_trace_errors_on_the_host(E, tmp_path):
     libc.fclose(fp)
     assert E.lib().pf_read_trace_line(None, E.MODEL_REFARM, C.byref(inp),
                                       act.ctypes.data_as(C.POINTER(C.c_float))) == E.PF_ERR_INVALID
+
+
+def test_cli_rejects_unknown_model_and_missing_trace(tmp_path):
+    import subprocess
+    cli = ROOT / "esthera_b200" / "pf_cli"
+    r = subprocess.run([str(cli), "-M", "bogus", str(tmp_path / "t")], capture_output=True, text=True)
+    assert r.returncode == 1 and "unknown model" in r.stderr
+    r = subprocess.run([str(cli), "-M", "unicycle"], capture_output=True, text=True)
+    assert r.returncode == 1 and "no input file" in r.stderr
+    r = subprocess.run([str(cli), "-M", "unicycle", "-m", "64", "-N", "2", str(tmp_path / "absent")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "error" in r.stderr  # PF_ERR_IO before any GPU work
