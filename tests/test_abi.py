@@ -42,6 +42,31 @@ def test_model_info(E):
     assert E.model_info(E.MODEL_UNICYCLE) == (3, 3, 2, 16)
     assert E.model_info(E.MODEL_DHARM) == (12, 6, 0, 6)
     assert E.model_info(E.MODEL_REFARM) == (9, 9, 5, 7)
+    assert E.model_info(E.MODEL_BEACON) == (3, 3, 2, 16)
+    assert E.model_info(E.MODEL_CAMARM) == (9, 9, 5, 7)
+    with pytest.raises(E.PFError):
+        E.model_info(5)
+
+
+def test_model_params_validated_on_the_host(E):
+    """Bad model parameters are refused before any GPU work (on a GPU-less
+    host the valid ones then fail with PF_ERR_CUDA: no CPU path)."""
+    b = E.beacon_params()
+    for field, val in [("num_beacons", 0), ("num_beacons", 17), ("sigma_range", 0.0)]:
+        q = E.BeaconParams.from_buffer_copy(b)
+        setattr(q, field, val)
+        with pytest.raises(E.PFError) as ei:
+            E.ParticleFilter(E.MODEL_BEACON, q, num_subfilters=8)
+        assert ei.value.status == E.PF_ERR_INVALID, field
+    # a params struct of the wrong model is refused by its size
+    with pytest.raises(E.PFError) as ei:
+        E.ParticleFilter(E.MODEL_CAMARM, b, num_subfilters=8)
+    assert ei.value.status == E.PF_ERR_INVALID
+    if E.device_count() == 0:
+        for model, params in [(E.MODEL_BEACON, b), (E.MODEL_CAMARM, E.camarm_params())]:
+            with pytest.raises(E.PFError) as ei:
+                E.ParticleFilter(model, params, num_subfilters=8)
+            assert ei.value.status == E.PF_ERR_CUDA
 
 
 @pytest.mark.parametrize("kw,msg", [
