@@ -145,6 +145,24 @@ def test_beacon_oracle_filter_tracks(O, E):
     assert rmse < 0.5, rmse
 
 
+@pytest.mark.parametrize("log_weights", [0, 1])
+def test_beacon_oracle_program_loop(O, E, log_weights):
+    """The drop-in loop's configuration on the oracle: ring exchange, the
+    reference's multinomial resampling (FP32 Blelloch scan) every step, the
+    best particle of the best sub-filter as the estimate (linear weights as
+    the program keeps them, and log weights)."""
+    p = E.beacon_params()
+    inputs, truth = E.make_trace(BEACON, p, 6, 40)
+    f = O.Filter(O.model_from_params(BEACON, p), 256, 16, 1, O.EXCH_RING, O.RES_REF, O.RNG_SUBFILTER, 96, 4,
+                 log_weights, 1.0, 0xF000000D, 0, np.array(p.init_state[:], np.float32))
+    err = []
+    for k in range(40):
+        e, _ = f.step(inputs["control"][k], inputs["meas"][k])
+        assert 0 <= e.best_sub < 16 and np.isfinite(e.best_key)
+        err.append(np.hypot(e.best[0] - truth[k, 0], e.best[1] - truth[k, 1]))
+    assert np.mean(err) < 2.0, np.mean(err)
+
+
 # ---------------------------------------------------------------- GPU
 def _angle_close(a, b, atol):
     return np.all(np.abs(np.angle(np.exp(1j * (a.astype(np.float64) - b)))) < atol)
