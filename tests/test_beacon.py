@@ -78,6 +78,23 @@ def test_beacon_oracle_straight_line_limit(O, E):
     assert np.allclose(new[:, 0], [20 + 0.3 * np.cos(0.5), 40 + 0.3 * np.sin(0.5), 0.5], atol=2e-6)
 
 
+def test_half_angle_arc_equals_the_programs_difference_form():
+    """The device's arc, v dt sinc(w dt / 2) (cos, sin)(th + w dt / 2), is the
+    program's v/w (sin(th + w dt) - sin th, -(cos(th + w dt) - cos th)) (FP64;
+    the identities sin a - sin b = 2 cos((a+b)/2) sin((a-b)/2) and
+    cos a - cos b = -2 sin((a+b)/2) sin((a-b)/2)), and stays finite as w -> 0."""
+    rng = np.random.default_rng(8)
+    th = rng.uniform(-np.pi, np.pi, 1000)
+    v = rng.uniform(0.0, 2.0, 1000)
+    w = rng.uniform(-3.0, 3.0, 1000)
+    dt = rng.uniform(0.05, 1.0, 1000)
+    h = 0.5 * w * dt
+    k = v * dt * np.sinc(h / np.pi)  # numpy's sinc is sin(pi x) / (pi x)
+    assert np.allclose(k * np.cos(th + h), v / w * (np.sin(th + w * dt) - np.sin(th)), rtol=0, atol=1e-12)
+    assert np.allclose(k * np.sin(th + h), -v / w * (np.cos(th + w * dt) - np.cos(th)), rtol=0, atol=1e-12)
+    assert np.isclose(1.0 * 1.0 * np.sinc(0.0), 1.0)
+
+
 def write_trace(path, inputs, truth):
     """The unicycle program's trace format: ranges[10] v omega dt x y theta."""
     rows = []
