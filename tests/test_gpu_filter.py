@@ -290,7 +290,7 @@ def rmse_xy(ests, truth):
     return float(np.sqrt(np.mean(np.sum((m - truth[:, :2]) ** 2, axis=1))))
 
 
-def test_cfg0_unicycle_rmse_matches_oracle(gpu, O):
+def test_unicycle_4096_rmse_matches_oracle(gpu, O):
     """Plain unicycle filter: 4096 = 8 x 512, systematic every step, no exchange, 100 steps, seed 1."""
     E = gpu
     p, inputs, truth = uni_setup(1, 100)
@@ -306,7 +306,7 @@ def test_cfg0_unicycle_rmse_matches_oracle(gpu, O):
     assert abs(g - o) <= 0.05 * o + 0.005, (g, o)
 
 
-def test_cfg1_shape_properties(gpu):
+def test_unicycle_2p20_torus_shape_properties(gpu):
     """2^20 particles = 2048 x 512 on a 32 x 64 torus, t = 2: sortedness, routing
     bounds, systematic monotone selections, finite estimates (size-independent checks)."""
     E = gpu
@@ -327,7 +327,7 @@ def test_cfg1_shape_properties(gpu):
 
 
 @pytest.mark.parametrize("res", [1, 2])
-def test_cfg1_unicycle_tracks(gpu, res):
+def test_unicycle_torus_256x512_tracks(gpu, res):
     E = gpu
     p, inputs, truth = uni_setup(2, 200)
     f, ests = run(E, UNI, p, inputs, particles_per_subfilter=512, num_subfilters=256, num_transfer=2, exchange=2,
