@@ -30,10 +30,18 @@ roofline: the dominant kernel's algorithmic bytes (the sampling kernel reads
         roofline (its ncu warp-instruction count at 4 issues per cycle per
         SM at the sampled clock), the bound it actually meets.
 
+clocks: nvidia-smi samples (20 ms) over a window of about a second: untimed
+        steps of the same work for ~0.5 s before and after the timed ones.
+latency_ms: pf_step's per-step latency on the host (p50/p99/p999) beside the
+        device step times.
+
 Multi-GPU (torchrun): each rank runs its own filter (weak scaling, replicas,
 no data-path collective); time = max over ranks.
 --impl reference: the CPU restatement of the reference step (the reference's
-OpenCL path cannot run here) on all host cores, on a bounded sample.
+OpenCL path cannot run here) on all host cores, on the full workload shape
+(W warm-up steps, then the K timed steps in >= 3 repeats, time-bounded; the
+median repeat); its inputs come from oracle/workload.py, so that process never
+loads the engine.  The plain line's cpu_baseline is the same, bounded to 20 s.
 """
 import argparse
 import ctypes as C
@@ -51,14 +59,15 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 ALG_BYTES = 24  # unicycle, per particle-step
+MAX_ROLL = 20000  # untimed steps at most on either side of the timed ones (clock window)
 # single-filter workloads: model, sub-filter size, sub-filters, torus transfer,
 # seed, algorithmic bytes per particle-step (state read + write)
 WORKLOADS = {
-    "plain": dict(model=0, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(),
+    "plain": dict(model=0, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(), torus=(32, 64),
                   desc="unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2"),
-    "arm": dict(model=1, m=256, nsub=1024, t=1, seed=3, alg=96, angles=(0, 1, 2, 3, 4, 5),
+    "arm": dict(model=1, m=256, nsub=1024, t=1, seed=3, alg=96, angles=(0, 1, 2, 3, 4, 5), torus=(32, 32),
                 desc="6-joint DH arm 2^18 particles = 1024 sub-filters x 256, torus 32x32, t=1"),
-    "beacon": dict(model=3, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(),
+    "beacon": dict(model=3, m=512, nsub=2048, t=2, seed=2, alg=24, angles=(), torus=(32, 64),
                    desc="10-beacon range-only unicycle 2^20 particles = 2048 sub-filters x 512, torus 32x64, t=2"),
 }
 CONFIGS = {
@@ -75,44 +84,79 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def clock_sampler(gpu_index):
-    cmd = ["nvidia-smi", "-i", str(gpu_index),
-           "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-           "--format=csv,noheader,nounits", "-lms", "20"]
-    try:
-        return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-    except OSError:
-        return None
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 20 ms, read by a thread.
+    start() returns once the first sample has arrived (the sampler takes a
+    while to come up), so a window of load begun after it is covered."""
 
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-def clock_summary(proc):
-    if proc is None:
-        return None
-    proc.send_signal(signal.SIGTERM)
-    try:
-        out, _ = proc.communicate(timeout=5)
-    except subprocess.TimeoutExpired:
-        proc.kill()
-        out, _ = proc.communicate()
-    sm, smax, reasons = [], None, set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    for line in out.strip().splitlines():
-        f = [x.strip() for x in line.split(",")]
-        if len(f) < 8:
-            continue
+    def __init__(self, gpu_index):
+        self.cmd = ["nvidia-smi", "-i", str(gpu_index),
+                    "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                    "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                    "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                    "--format=csv,noheader,nounits", "-lms", "20"]
+        self.lines, self.proc, self.thread = [], None, None
+        self.t_start = self.t_stop = None
+
+    def start(self, wait_s=10.0):
+        import threading
         try:
-            sm.append(float(f[0]))
-            smax = float(f[1])
-        except ValueError:
-            continue
-        for n, v in zip(names, f[4:8]):
-            if v.lower() == "active":
-                reasons.add(n)
-    if not sm:
-        return None
-    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+
+        def read():
+            for line in self.proc.stdout:
+                self.lines.append((time.perf_counter(), line))
+
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+        t0 = time.perf_counter()
+        while not self.lines and time.perf_counter() - t0 < wait_s and self.proc.poll() is None:
+            time.sleep(0.01)
+        return self
+
+    def mark(self, start):
+        """Brackets the window whose samples are summarised (the load window)."""
+        if start:
+            self.t_start = time.perf_counter()
+        else:
+            self.t_stop = time.perf_counter()
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, reasons, power = [], None, set(), []
+        for t, line in self.lines:
+            if self.t_start is not None and not (self.t_start <= t <= (self.t_stop or t)):
+                continue
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+                power.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(self.NAMES, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "window_s": (self.t_stop - self.t_start) if self.t_start and self.t_stop else None,
+                "power_w_median": float(np.median(power)) if power else None}
 
 
 def visible_gpu_index(local_rank):
@@ -130,50 +174,92 @@ def model_params(E, W):
     return E.unicycle_params(W["seed"]) if W["model"] == 0 else E.dharm_params(W["seed"])
 
 
-def cpu_baseline(steps, resampler, threads=0, budget_s=20.0, W=None):
-    """The oracle's whole step (C, OpenMP over sub-filters) on a sample of the
-    workload: 256 sub-filters (a 16 x 16 torus) of the workload's size."""
-    W = W or WORKLOADS["plain"]
+def workload_config(W, resampler_name, extra=None):
+    """The `config` both arms report for a single-filter workload."""
+    c = {"workload": "%s, %s resampling every step, FP32 state/log-weights, FP64 normalisation+cumsum"
+                     % (W["desc"], resampler_name),
+         "particles": W["m"] * W["nsub"], "subfilters": W["nsub"], "particles_per_subfilter": W["m"],
+         "torus": W["torus"], "num_transfer": W["t"], "seed": W["seed"]}
+    c.update(extra or {})
+    return c
+
+
+def cpu_filter_run(W, resampler, warmup, steps, budget_s, repeats=3):
+    """The oracle's whole step (C, OpenMP over all host cores) on the full
+    workload (same shape, torus, t and seeded trace as the GPU arm), built
+    from oracle/workload.py so the process never loads the engine.  Runs
+    `warmup` untimed steps, then up to `steps` timed steps split into
+    `repeats` (>= 3) equal chunks, stopping early at `budget_s`; the value is
+    the median chunk throughput."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    import esthera_b200 as E
     import oracle as O
-    nsub, m = 256, W["m"]
-    p = model_params(E, W)
-    inputs, _ = E.make_trace(W["model"], p, W["seed"], steps)
+    import workload as Wk
+    m, nsub = W["m"], W["nsub"]
+    p = Wk.params(W["model"], W["seed"])
+    total = warmup + max(steps, repeats)
+    control, meas, _, _ = Wk.make_trace(W["model"], p, W["seed"], total)
     md = O.model_from_params(W["model"], p)
-    S = E.model_info(W["model"])[0]
-    f = O.Filter(md, m, nsub, W["t"], O.EXCH_TORUS, resampler, O.RNG_SUBFILTER, 96, 2, 1, 1.0, W["seed"], 0,
+    S = Wk.NUM_STATE[W["model"]]
+    f = O.Filter(md, m, nsub, W["t"], O.EXCH_TORUS, resampler, O.RNG_SUBFILTER, 96, 4, 1, 1.0, 0xF000000D, 0,
                  np.array(p.init_state[:S], np.float32))
-    f.step(inputs["control"][0], inputs["meas"][0], threads)  # warm-up
-    done, t0 = 0, time.perf_counter()
-    for k in range(1, steps):
-        f.step(inputs["control"][k], inputs["meas"][k], threads)
-        done += 1
-        if time.perf_counter() - t0 > budget_s:
+    t_w = time.perf_counter()
+    k = 0
+    for k in range(max(warmup, 1)):
+        f.step(control[k], meas[k])
+        if time.perf_counter() - t_w > budget_s / 4:
             break
-    dt = time.perf_counter() - t0
-    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    step_s = (time.perf_counter() - t_w) / (k + 1)
+    k += 1
+    timed = max(repeats, min(steps, int(budget_s / max(step_s, 1e-6))))
+    chunk = max(1, timed // repeats)
+    rates = []
+    for r in range(repeats):
+        t0 = time.perf_counter()
+        for _ in range(chunk):
+            f.step(control[k % total], meas[k % total])
+            k += 1
+        rates.append(m * nsub * chunk / (time.perf_counter() - t0))
     f.close()
-    return {"value": m * nsub * done / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-            "sample": "%d steps of %d sub-filters x %d particles (of the %s workload), torus 16x16, t=%d"
-                      % (done, nsub, m, W["desc"].split(" = ")[0], W["t"])}
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    return {"value": float(np.median(rates)), "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "repeats": [float(x) for x in rates],
+            "sample": "%d repeats x %d steps of the full workload (%s, torus %dx%d, t=%d); median of the repeats"
+                      % (repeats, chunk, W["desc"].split(" = ")[0], W["torus"][0], W["torus"][1], W["t"]),
+            "cpu": cpu_model()}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def reference_arm(args, rank, world):
+    """The reference's CPU path of the step: the oracle's C restatement (the
+    reference's own OpenCL-on-CPU path cannot run on these hosts), full
+    workload shape, all host cores; rank 0 only."""
     resampler = CONFIGS[args.resampler]
     if rank != 0:
         return 0
     W = WORKLOADS.get(args.workload, WORKLOADS["plain"])
-    base = cpu_baseline(args.warmup + args.steps + 1, resampler, 0, budget_s=60.0, W=W)
+    base = cpu_filter_run(W, resampler, args.warmup, args.steps, budget_s=150.0)
     line = {"metric": "particle-steps/s", "value": base["value"], "unit": "particle-steps/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace)",
-            "config": {"workload": "%s, %s resampling" % (W["desc"], args.resampler), "sample": base["sample"]},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace, seed %d)"
+            % W["seed"], "config": workload_config(W, args.resampler),
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "note": "the reference's OpenCL-on-CPU path is not runnable (no CPU OpenCL runtime); "
-                    "this is the C restatement of the reference step, OpenMP over sub-filters"}
+            "note": "the reference's OpenCL-on-CPU path is not runnable (no CPU OpenCL runtime); this is the "
+                    "oracle's C restatement of the reference step, OpenMP over sub-filters; inputs from "
+                    "oracle/workload.py (the engine's library is not loaded)"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -368,8 +454,10 @@ def main():
     W = WORKLOADS[args.workload]
     m, nsub, particles = W["m"], W["nsub"], W["m"] * W["nsub"]
     p = model_params(E, W)
-    total_steps = args.warmup + args.steps
-    inputs, truth = E.make_trace(W["model"], p, W["seed"], total_steps + args.e2e_steps)
+    # the trace covers warm-up, the clock window's untimed steps before and
+    # after the timed ones (at most MAX_ROLL each) and the timed steps
+    total_steps = args.warmup + args.steps + 2 * MAX_ROLL
+    inputs, truth = E.make_trace(W["model"], p, W["seed"], total_steps)
     f = E.ParticleFilter(W["model"], p, particles_per_subfilter=m, num_subfilters=nsub, num_transfer=W["t"],
                          exchange=E.EXCHANGE_TORUS, resampler=resampler, seed=W["seed"] + 1000 * rank, device=local,
                          particles_per_thread=args.ppt if args.pipeline == "split" else 0,
@@ -382,15 +470,37 @@ def main():
     torch.cuda.synchronize()
 
     # warm-up: builds the graph and runs W steps (no per-launch events in the timed graph)
-    f.run_device(d_in.data_ptr(), d_est.data_ptr(), total_steps, args.warmup)
+    t_w = time.perf_counter()
+    f.run_device(d_in.data_ptr(), d_est.data_ptr(), total_steps, 1)
     f.synchronize()
+    t_w = time.perf_counter()
+    for k in range(args.warmup - 1):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        f.run_continue(1)
+    f.synchronize()
+    per_step_s = (time.perf_counter() - t_w) / max(args.warmup - 1, 1)
+    # the clock window: untimed steps (same work, same L2 flush) for about
+    # half a second before and after the timed steps, so the nvidia-smi
+    # samples (every 20 ms) cover at least a second of this load around them
+    roll = int(min(MAX_ROLL, max(1, np.ceil(0.5 / max(per_step_s, 1e-6)))))
+
+    def untimed(n):
+        for k in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            f.run_continue(1)
+        f.synchronize()
 
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(visible_gpu_index(local)).start() if rank == 0 else None
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clk = clock_sampler(visible_gpu_index(local)) if rank == 0 else None
+    if clk:
+        clk.mark(True)
+    untimed(roll)
     step_ms, phase_ms = [], {}
     for k in range(args.steps):
         with torch.cuda.stream(stream):
@@ -401,9 +511,13 @@ def main():
         ev1.synchronize()
         step_ms.append(ev0.elapsed_time(ev1))
     torch.cuda.synchronize()
+    untimed(roll)
+    if clk:
+        clk.mark(False)
     if dist:
         dist.barrier()
-    clocks = clock_summary(clk)
+    clocks = clk.stop() if clk else None
+    steps_run = args.warmup + 2 * roll + args.steps
     total_ms = float(np.sum(step_ms))
     if dist:
         t = torch.tensor([total_ms], device="cuda")
@@ -461,12 +575,15 @@ def main():
 
     # the synchronous call, one step at a time (the step latency a caller of pf_step sees)
     f.set_initial_state(np.array(p.init_state[:E.model_info(W["model"])[0]], np.float32))
-    sync_ms = []
+    sync_ms, lat_ms = [], []
     for k in range(K):
         with torch.cuda.stream(stream):
             flush.fill_(float(k))
             ev0.record(stream)
+        stream.synchronize()  # the flush is done: the host clock below sees pf_step alone
+        t0 = time.perf_counter()
         f.step(inputs[k])
+        lat_ms.append((time.perf_counter() - t0) * 1e3)
         ev1.record(stream)
         ev1.synchronize()
         sync_ms.append(ev0.elapsed_time(ev1))
@@ -506,22 +623,20 @@ def main():
             issue = {"warp_instructions_per_launch": winst, "min_ms_at_full_issue": min_ms,
                      "frac": min_ms / phases[dom], "sms": sms, "sm_mhz": clocks["sm_mhz"]}
         if W["angles"]:  # joint angles, wrapped
-            d = est["mean"][:, list(W["angles"])] - truth[:total_steps, list(W["angles"])]
+            d = est["mean"][:steps_run, list(W["angles"])] - truth[:steps_run, list(W["angles"])]
             d = np.remainder(d + np.pi, 2 * np.pi) - np.pi
         else:  # position
-            d = est["mean"][:, :2] - truth[:total_steps, :2]
+            d = est["mean"][:steps_run, :2] - truth[:steps_run, :2]
         rmse = float(np.sqrt(np.mean(np.sum(d ** 2, axis=1))))
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded trace, seed %d)" % W["seed"],
-            "config": {"workload": "%s, %s resampling every step, FP32 state/log-weights, FP64 "
-                                   "normalisation+cumsum" % (W["desc"], args.resampler),
-                       "particles": particles, "subfilters": nsub, "particles_per_subfilter": m,
-                       "particles_per_thread": info["particles_per_thread"], "rng": "MTGP32 per sub-filter",
-                       "pipeline": {0: "fused (one kernel per step)", 1: "phased", 2: "split"}[info["pipeline"]],
-                       "l2": "flushed before every timed step (256 MB write)", "parallelism": "replicas" if world > 1
-                       else "single GPU"},
+            "config": workload_config(W, args.resampler, {
+                "particles_per_thread": info["particles_per_thread"], "rng": "MTGP32 per sub-filter",
+                "pipeline": {0: "fused (one kernel per step)", 1: "phased", 2: "split"}[info["pipeline"]],
+                "l2": "flushed before every timed step (256 MB write)",
+                "parallelism": "replicas" if world > 1 else "single GPU"}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "kernel": dom, "kernel_ms": phases[dom], "share": phases[dom] / sum(phases.values()),
@@ -537,14 +652,22 @@ def main():
                     "sync": {"value": world * particles * args.e2e_steps / (sync_total * 1e-3)
                              if args.e2e_steps > 0 else None, "ms_per_step": sync_total / max(args.e2e_steps, 1),
                              "api": "pf_step (synchronous, one step at a time)"}},
+            "latency_ms": {"what": "pf_step (synchronous, host input -> estimate on the host), one step at a "
+                                   "time from an idle GPU with L2 flushed, %d steps" % K,
+                           "p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                           "p999": float(np.percentile(lat_ms, 99.9)),
+                           "device_step": {"what": "timed steps, CUDA events around each graph launch",
+                                           "p50": float(np.percentile(step_ms, 50)),
+                                           "p99": float(np.percentile(step_ms, 99))}},
             "gpu_launches": int(args.steps * len(phases)),
             "timing": "value: CUDA events around each step's graph launch (no events inside); kernel times: "
                       "a separate %d-step pass with events between the launches" % args.phase_steps,
             "clocks": clocks,
-            "rmse": {"value": rmse, "of": "joint angles (rad)" if W["angles"] else "x, y position (m)"},
+            "rmse": {"value": rmse, "of": "joint angles (rad)" if W["angles"] else "x, y position (m)",
+                     "steps": steps_run},
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(40, resampler, 0, budget_s=15.0, W=W)
+            line["cpu_baseline"] = cpu_filter_run(W, resampler, 1, 1000, budget_s=20.0)
         print(json.dumps(line), flush=True)
     f.close()
     if dist:

@@ -132,6 +132,7 @@ def _declare(L):
         "pf_run_device_continue": (C.c_int, [P, C.c_int32]),
         "pf_step_submit": (C.c_int, [P, P]),
         "pfk_bounded_wait_test": (C.c_int, [C.c_int32, P]),
+        "pfk_bounded_wait_mixed_test": (C.c_int, [P, C.c_int32, P, P]),
         "pf_step_collect": (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
         "pf_synchronize": (C.c_int, [P]),
         "pf_stream": (P, [P]),
@@ -141,7 +142,7 @@ def _declare(L):
         "pf_get_info": (C.c_int, [P, ip, ip, ip, ip, C.POINTER(C.c_int64)]),
         "pf_snapshot_size": (C.c_int64, [P]),
         "pf_snapshot": (C.c_int, [P, P]),
-        "pf_restore": (C.c_int, [P, P]),
+        "pf_restore": (C.c_int, [P, P, C.c_size_t]),
         "pf_batch_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, C.POINTER(P)]),
         "pf_batch_destroy": (C.c_int, [P]),
         "pf_batch_set_initial_states": (C.c_int, [P, fp]),
@@ -169,7 +170,7 @@ def _declare(L):
         "pf_server_get_particles": (C.c_int, [P, C.c_int32, fp, fp, fp]),
         "pf_server_snapshot_size": (C.c_int64, [P, C.c_int32]),
         "pf_server_snapshot": (C.c_int, [P, C.c_int32, P]),
-        "pf_server_restore": (C.c_int, [P, C.c_int32, P]),
+        "pf_server_restore": (C.c_int, [P, C.c_int32, P, C.c_size_t]),
         "pf_load_default": (C.c_int, [C.POINTER(LoadConfig)]),
         "pf_serve_load": (C.c_int, [C.POINTER(PFConfig), C.POINTER(LoadConfig), C.POINTER(LoadReport)]),
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
@@ -426,7 +427,7 @@ class ParticleFilter:
 
     def restore(self, buf):
         b = np.ascontiguousarray(buf, np.uint8)
-        check(lib().pf_restore(self._h, b.ctypes.data_as(C.c_void_p)))
+        check(lib().pf_restore(self._h, b.ctypes.data_as(C.c_void_p), b.nbytes))
 
 
 class FilterBatch:
@@ -606,7 +607,7 @@ class Server:
 
     def restore(self, fid, snap):
         buf = np.frombuffer(snap, np.uint8).copy()
-        check(lib().pf_server_restore(self._h, fid, buf.ctypes.data_as(C.c_void_p)))
+        check(lib().pf_server_restore(self._h, fid, buf.ctypes.data_as(C.c_void_p), buf.nbytes))
 
 
 class LoadConfig(C.Structure):
@@ -713,6 +714,16 @@ def bounded_wait_test(limit=2000):
     st = C.c_int32(-1)
     check(lib().pfk_bounded_wait_test(int(limit), C.byref(st)))
     return st.value
+
+
+def bounded_wait_mixed_test(limits):
+    """CTA-wide bounded wait with a bulk copy in flight and per-thread poll
+    limits; returns (outcome per thread, copied flag)."""
+    lim = np.ascontiguousarray(limits, np.int32)
+    out = np.zeros(len(lim), np.int32)
+    copied = C.c_int32(-2)
+    check(lib().pfk_bounded_wait_mixed_test(_iptr(lim), len(lim), _iptr(out), C.byref(copied)))
+    return out, copied.value
 
 
 def bitonic_sort(keys, m, ppt=0):

@@ -364,6 +364,9 @@ static int32_t* status_word(pf_filter* f) { return reinterpret_cast<int32_t*>(f-
 
 static pf_status check_status(int32_t st)
 {
+    if (st & PF_STATUS_MISALIGNED)
+        return fail(PF_ERR_INVALID, "a sorted copy's rows were not 16-byte aligned (sub-filters kept their "
+                                    "propagated particles)");
     if (st & PF_STATUS_WAIT_TIMEOUT)
         return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
                                     "propagated particles)");
@@ -1003,9 +1006,12 @@ extern "C" pf_status pf_snapshot(pf_filter* f, void* buf)
     return PF_OK;
 }
 
-extern "C" pf_status pf_restore(pf_filter* f, const void* buf)
+extern "C" pf_status pf_restore(pf_filter* f, const void* buf, size_t size)
 {
     if (!f || !buf) return fail(PF_ERR_INVALID, "null argument");
+    const int64_t want = pf_snapshot_size(f);
+    if (size < 32 || (int64_t)size != want)
+        return fail(PF_ERR_INVALID, "snapshot of %zu bytes; this filter takes %lld", size, (long long)want);
     const char* p = (const char*)buf;
     int64_t hdr[4];
     memcpy(hdr, p, 32);
@@ -1075,6 +1081,30 @@ extern "C" pf_status pfk_bounded_wait_test(int32_t limit, int32_t* status)
     CU(cudaMemset(d.p, 0xff, 4));
     CU(launch_test_bounded_wait(limit, (int32_t*)d.p, 0));
     CU(cudaMemcpy(status, d.p, 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pfk_bounded_wait_mixed_test(const int32_t* limits, int32_t nthreads, int32_t* outcome,
+                                                 int32_t* copied)
+{
+    if (!limits || !outcome || !copied || nthreads < 32 || nthreads > 1024 || nthreads % 32)
+        return fail(PF_ERR_INVALID, "bad argument");
+    for (int i = 0; i < nthreads; ++i)
+        if (limits[i] < 0 || limits[i] > (1 << 20)) return fail(PF_ERR_INVALID, "poll limits must be in [0, 2^20]");
+    TRYS(require_gpu(0));
+    std::vector<uint32_t> src(kMixedWaitSrcBytes / 4);
+    for (size_t i = 0; i < src.size(); ++i) src[i] = 0x9e3779b9u * (uint32_t)(i + 1);
+    DevBuf dl, ds, dout;
+    TRYS(dev_buf(dl, (size_t)nthreads * 4));
+    TRYS(dev_buf(ds, kMixedWaitSrcBytes));
+    TRYS(dev_buf(dout, (size_t)(nthreads + 1) * 4));
+    CU(cudaMemcpy(dl.p, limits, (size_t)nthreads * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ds.p, src.data(), kMixedWaitSrcBytes, cudaMemcpyHostToDevice));
+    CU(cudaMemset(dout.p, 0x7f, (size_t)(nthreads + 1) * 4));
+    int32_t* o = static_cast<int32_t*>(dout.p);
+    CU(launch_test_bounded_wait_mixed(static_cast<const int32_t*>(dl.p), nthreads, ds.p, o, o + nthreads, 0));
+    CU(cudaMemcpy(outcome, o, (size_t)nthreads * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(copied, o + nthreads, 4, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
 

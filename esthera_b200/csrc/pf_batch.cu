@@ -165,6 +165,9 @@ static pf_status upload_batch_descs(pf_batch* B, pf_estimate* run_est, int32_t c
 
 static pf_status batch_status(int32_t st)
 {
+    if (st & PF_STATUS_MISALIGNED)
+        return fail(PF_ERR_INVALID, "a sorted copy's rows were not 16-byte aligned (sub-filters kept their "
+                                    "propagated particles)");
     if (st & PF_STATUS_WAIT_TIMEOUT)
         return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
                                     "propagated particles)");

@@ -306,6 +306,46 @@ cudaError_t launch_test_bounded_wait(int limit, int32_t* status, cudaStream_t st
     return cudaGetLastError();
 }
 
+// The CTA-wide wait of the resampling kernels (mbar_wait_cta) with a bulk copy
+// really in flight and a poll limit per thread from the host (limits[tid]; 0:
+// the thread gives up at once, so some threads run out while others see the
+// copy land).  outcome[tid] receives each thread's result (1, 0 or -1; the
+// same in every thread when the decision is CTA-wide); *copied is 1 when the
+// shared-memory words equal the source once the CTA went on (the copy landed
+// before anyone moved on), 0 when they differ, -1 when the outcome was -1.
+constexpr int kMixedWaitBytes = 32768;
+__global__ void k_test_bounded_wait_mixed(const int32_t* __restrict__ limits, const uint4* __restrict__ src,
+                                          int32_t* __restrict__ outcome, int32_t* __restrict__ copied)
+{
+    __shared__ __align__(128) uint4 buf[kMixedWaitBytes / 16];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) {
+        mbar_init_expect(&mbar, kMixedWaitBytes);
+        bulk_g2s(buf, src, kMixedWaitBytes, &mbar);
+    }
+    __syncthreads();  // the mbarrier is initialised
+    const int r = mbar_wait_cta(&mbar, 0, limits[threadIdx.x], kBulkDrainPolls);
+    outcome[threadIdx.x] = r;
+    if (r < 0) {
+        if (threadIdx.x == 0) *copied = -1;
+        return;
+    }
+    int bad = 0;
+    for (int i = threadIdx.x; i < kMixedWaitBytes / 16; i += blockDim.x) {
+        const uint4 a = buf[i], b = src[i];
+        bad |= (a.x != b.x) | (a.y != b.y) | (a.z != b.z) | (a.w != b.w);
+    }
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) *copied = bad ? 0 : 1;
+}
+
+cudaError_t launch_test_bounded_wait_mixed(const int32_t* limits, int nthreads, const void* src, int32_t* outcome,
+                                           int32_t* copied, cudaStream_t st)
+{
+    k_test_bounded_wait_mixed<<<1, nthreads, 0, st>>>(limits, static_cast<const uint4*>(src), outcome, copied);
+    return cudaGetLastError();
+}
+
 // A run's device step counter, advanced (or set) by a launch of its own once
 // every kernel of the step that reads it is enqueued before it.
 __global__ void k_counter_update(int32_t* ctr, int32_t set, int32_t value)

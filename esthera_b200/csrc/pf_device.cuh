@@ -182,7 +182,8 @@ __device__ __forceinline__ void mtgp_generate_bm(MtgpSmem& s, int n, int nbm, fl
 // coefficients in a^2, fitted for this project by least squares on 4000
 // Chebyshev nodes refined with Lawson iterations towards the minimax fit
 // (max error 1.4e-7 in FP32 Horner) -- plus octant reduction with one fast
-// division.  Max absolute error about 3e-7 rad.
+// division.  Max absolute error about 3e-7 rad.  fit_atan2.py (beside this
+// file) regenerates the fit and checks both bounds against FP64 atan2.
 __device__ __forceinline__ float pf_atan2(float y, float x)
 {
     const float ax = fabsf(x), ay = fabsf(y);

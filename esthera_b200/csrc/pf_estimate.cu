@@ -9,6 +9,8 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>
+
 #include "pf_launch.cuh"
 
 namespace pfdev {
@@ -278,7 +280,41 @@ constexpr int kNoAllocMaxSubfilters = 4096;  // 4096 * 35 doubles = 1.15 MB per 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxSubfilters * kEstStride];
 
 static std::mutex g_noalloc_mu;
-static double* g_noalloc_ptr[256];  // device address of g_noalloc_scratch, per device ordinal
+// Device address of g_noalloc_scratch per device ordinal, valid for the CUDA
+// context whose process-unique id is stored beside it: cudaDeviceReset (or a
+// caller switching to another context on the same ordinal) loads the module
+// afresh, possibly at another address, and the new context has a new id, so
+// the next call looks the address up again instead of using a stale one.
+static double* g_noalloc_ptr[256];
+static unsigned long long g_noalloc_ctx[256];
+
+// The current context's process-unique id (cuCtxGetId; ids are never reused
+// within a process), through the runtime's driver entry points so the library
+// needs no link against libcuda.  0 when no context is current.
+static unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) {
+            cudaGetLastError();
+            return 0;
+        }
+        get_current = reinterpret_cast<GetCurrent>(a);
+        get_id = reinterpret_cast<GetId>(b);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 extern "C" pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_state, int32_t num_state,
                                           int64_t num_particles, int32_t m, uint32_t angle_mask,
@@ -298,10 +334,12 @@ extern "C" pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_st
     }
     double* scratch = nullptr;
     {
-        // Once per device, with that device current: the host-side name of the
-        // array is only a stand-in, so ask the runtime for its device address.
+        // Once per device (and again after the device's context was replaced),
+        // with that device current: the host-side name of the array is only a
+        // stand-in, so ask the runtime for its device address.
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        unsigned long long ctx = current_context_id();
+        if (!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) {
@@ -309,6 +347,7 @@ extern "C" pf_status pfk_estimate_noalloc(const float* d_keys, const float* d_st
                 return pfi_fail(PF_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed");
             }
             g_noalloc_ptr[dev] = static_cast<double*>(p);
+            g_noalloc_ctx[dev] = current_context_id();  // the lookup made the context current if none was
         }
         scratch = g_noalloc_ptr[dev];
     }

@@ -53,8 +53,20 @@ struct FilterDesc {
 };
 
 // status bits: a bounded wait on a bulk copy ran out (the sub-filter kept its
+// propagated particles); a sorted copy handed to the resampling was not
+// 16-byte aligned (not this library's allocation; the sub-filter kept its
 // propagated particles)
 constexpr int PF_STATUS_WAIT_TIMEOUT = 1;
+constexpr int PF_STATUS_MISALIGNED = 2;
+
+// Outcome of resample_from: the CTA resampled; it kept its propagated
+// particles (decision uniform, ESS gate, misaligned rows, or a wait that ran
+// out after which the copies still landed); or its bulk copies may still be
+// landing in shared memory, so the CTA must not touch its dynamic shared
+// memory again.
+constexpr int PF_RS_RESAMPLED = 1;
+constexpr int PF_RS_KEPT = 0;
+constexpr int PF_RS_LOST = -1;
 
 // A CTA's filter descriptor, copied once into shared memory (all threads of
 // the CTA call this at their start).  The kernels read descriptor fields all
@@ -799,19 +811,40 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity, int l
     return false;
 }
 
+// CTA-wide bounded wait for the bulk copies counted on `mbar`.  Each thread
+// polls at most limits[0] times, then the CTA agrees (__syncthreads_and), so
+// every thread takes the same branch even when only some of them ran out.  If
+// any gave up, every thread waits again, at most limits[1] polls, for the
+// copies still in flight, so that none is writing this CTA's shared memory
+// when the CTA moves on to reuse it or exits.  Returns 1 when the copies landed
+// within the first wait, 0 when they landed only in the second (the caller
+// reports the timeout; shared memory is quiet), -1 when they may still be in
+// flight (the caller must not touch the destination again).  Every thread of
+// the CTA must call it.
+__device__ __forceinline__ int mbar_wait_cta(uint64_t* mbar, unsigned parity, int limit, int drain_limit)
+{
+    if (__syncthreads_and(mbar_wait(mbar, parity, limit))) return 1;
+    return __syncthreads_and(mbar_wait(mbar, parity, drain_limit)) ? 0 : -1;
+}
+constexpr int kBulkWaitPolls = 1 << 18;
+constexpr int kBulkDrainPolls = 1 << 18;
+
 // Resampling of sub-filter b from a sorted copy (src_tmp, src_key: this
 // filter's arrays, sorted per sub-filter) with the exchange applied virtually
 // (nx weakest slots take the neighbours' top-t, read from the same sorted
-// copy).  U: the sub-filter's uniforms (decision first).  Returns false when
-// the decision uniform exceeds resampling_freq (the sub-filter keeps its
-// propagated particles); otherwise st holds this thread's E resampled
-// particles (positions E*tid+e) and sel their source slots.  Every thread of
-// the CTA must call it (it synchronises the CTA).  Restates resampling
+// copy).  U: the sub-filter's uniforms (decision first).  Returns PF_RS_KEPT
+// when the decision uniform exceeds resampling_freq or the ESS gate holds (the
+// sub-filter keeps its propagated particles), PF_RS_RESAMPLED with st holding
+// this thread's E resampled particles (positions E*tid+e) and sel their source
+// slots, or -- with a status bit set -- PF_RS_KEPT (rows not 16-byte aligned,
+// or a wait that ran out before the copies landed) or PF_RS_LOST (the copies
+// may still be landing in smem).  The result is the same in every thread.
+// Every thread of the CTA must call it (it synchronises the CTA).  Restates resampling
 // (pf_generic_soa.cu:415-453) for PF_RESAMPLE_REFERENCE and resampling_valias
 // (resampling-valias.cl:214-300) for PF_RESAMPLE_VOSE; PF_RESAMPLE_SYSTEMATIC
 // uses the FP64 scan.
 template <int S, int M, int E, int RES>
-__device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const float* __restrict__ src_tmp,
+__device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const float* __restrict__ src_tmp,
                                               const float* __restrict__ src_key, const float* __restrict__ U,
                                               int nx, unsigned char* smem, double* dred, int* ired,
                                               uint64_t* mbar, float (&st)[E][S], int (&sel)[E])
@@ -850,9 +883,9 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
         // resampling kernel 34.4 vs 26.0 us at 2^18 particles.)
         const bool bulk = ((reinterpret_cast<uintptr_t>(src_key) | reinterpret_cast<uintptr_t>(src_tmp) |
                             (uintptr_t)(T * 4)) & 15) == 0;
-        if (!bulk) {  // rows not 16-byte aligned: not this library's allocations
-            if (tid == 0 && D.status) atomicOr(D.status, PF_STATUS_WAIT_TIMEOUT);
-            return false;
+        if (!bulk) {  // rows not 16-byte aligned: not this library's allocations (no copy issued)
+            if (tid == 0 && D.status) atomicOr(D.status, PF_STATUS_MISALIGNED);
+            return PF_RS_KEPT;
         }
         if (tid == 0) {
             mbar_init_expect(mbar, (unsigned)((1 + S) * M * 4));
@@ -875,13 +908,12 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
             }
         }
         __syncthreads();  // the mbarrier is initialised
-        bool ok = mbar_wait(mbar, 0);
-        if (!ok) {
-            ok = mbar_wait(mbar, 0);  // the copies in flight, once more
+        const int landed = mbar_wait_cta(mbar, 0, kBulkWaitPolls, kBulkDrainPolls);
+        if (landed <= 0) {
             if (tid == 0 && D.status) atomicOr(D.status, PF_STATUS_WAIT_TIMEOUT);
-            if (!ok) return false;
+            return landed < 0 ? PF_RS_LOST : PF_RS_KEPT;
         }
-        if (dec_u - 1.0f > D.freq) return false;
+        if (dec_u - 1.0f > D.freq) return PF_RS_KEPT;
         if (xch) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
@@ -900,7 +932,7 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
 #pragma unroll
         for (int v = 0; v < S; ++v) cp_async_floats<E>(tile + v * M + E * tid, src_tmp + v * T + base);
         cp_async_wait();
-        if (dec_u - 1.0f > D.freq) return false;
+        if (dec_u - 1.0f > D.freq) return PF_RS_KEPT;
         if (xch) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
@@ -954,7 +986,7 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
         }
         __syncthreads();
         // all-zero weights count as uniform (ESS = m): no resampling
-        if (!(t2 > 0.0) || t1 * t1 >= (double)D.ess_frac * (double)M * t2) return false;
+        if (!(t2 > 0.0) || t1 * t1 >= (double)D.ess_frac * (double)M * t2) return PF_RS_KEPT;
     }
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
         double* cum = reinterpret_cast<double*>(scratch);
@@ -982,7 +1014,7 @@ __device__ __forceinline__ bool resample_from(const FilterDesc& D, int b, const 
     for (int v = 0; v < S; ++v)
 #pragma unroll
         for (int e = 0; e < E; ++e) st[e][v] = tile[v * M + sel[e]];
-    return true;
+    return PF_RS_RESAMPLED;
 }
 
 template <int S, int M, int E, int RES>
@@ -1018,7 +1050,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
     }
     float st[E][S];
     int sel[E];
-    if (!resample_from<S, M, E, RES>(D, b, D.tmp, D.tkey, U, nx, smem, dred, ired, &mbar, st, sel)) {
+    if (resample_from<S, M, E, RES>(D, b, D.tmp, D.tkey, U, nx, smem, dred, ired, &mbar, st, sel) != PF_RS_RESAMPLED) {
         if (D.sel) {
 #pragma unroll
             for (int e = 0; e < E; ++e) D.sel[base + e] = -1;

@@ -77,6 +77,9 @@ cudaError_t launch_a2a_merge(int nfilters, const FilterDesc* d, cudaStream_t st)
 cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStream_t st);
 cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st);
 cudaError_t launch_test_bounded_wait(int limit, int32_t* status, cudaStream_t st);
+constexpr int kMixedWaitSrcBytes = 32768;  // the source buffer launch_test_bounded_wait_mixed copies
+cudaError_t launch_test_bounded_wait_mixed(const int32_t* limits, int nthreads, const void* src, int32_t* outcome,
+                                           int32_t* copied, cudaStream_t st);
 cudaError_t launch_counter_inc(int32_t* ctr, cudaStream_t st);
 cudaError_t launch_counter_set(int32_t* ctr, int32_t value, cudaStream_t st);
 

@@ -605,6 +605,9 @@ extern "C" pf_status pf_server_poll(pf_server* s, int32_t wait, pf_server_result
     }
     const int nb = (int)s->batch_slots.size();
     if (cap < nb) return fail(PF_ERR_INVALID, "result buffer holds %d, the batch has %d", cap, nb);
+    if (*reinterpret_cast<const int32_t*>(s->h_out + nb) & PF_STATUS_MISALIGNED)
+        return fail(PF_ERR_INVALID, "a sorted copy's rows were not 16-byte aligned (sub-filters kept their "
+                                    "propagated particles)");
     if (*reinterpret_cast<const int32_t*>(s->h_out + nb) & PF_STATUS_WAIT_TIMEOUT)
         return fail(PF_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out in a kernel (sub-filters kept their "
                                     "propagated particles)");
@@ -709,11 +712,14 @@ extern "C" pf_status pf_server_snapshot(pf_server* s, int32_t id, void* buf)
     return PF_OK;
 }
 
-extern "C" pf_status pf_server_restore(pf_server* s, int32_t id, const void* buf)
+extern "C" pf_status pf_server_restore(pf_server* s, int32_t id, const void* buf, size_t size)
 {
     pf_status st = idle_filter(s, id);
     if (st != PF_OK) return st;
     if (!buf) return fail(PF_ERR_INVALID, "null argument");
+    const int64_t want = pf_server_snapshot_size(s, id);
+    if (size < 32 || (int64_t)size != want)
+        return fail(PF_ERR_INVALID, "snapshot of %zu bytes; filter %d takes %lld", size, id, (long long)want);
     Slot& sl = s->slots[id];
     const char* p = static_cast<const char*>(buf);
     int64_t hdr[4];

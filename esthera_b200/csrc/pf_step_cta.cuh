@@ -61,17 +61,24 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
 
     // ---- R
     float st[E][S];
-    bool resampled = false;
+    int rs = PF_RS_KEPT;
     if (!init) {
         int sel[E];
-        resampled = resample_from<S, M, E, RES>(D, b, prev_tmp, prev_key, ru, exchange_count(D), smem, dred,
-                                                ired, &mbar, st, sel);
+        rs = resample_from<S, M, E, RES>(D, b, prev_tmp, prev_key, ru, exchange_count(D), smem, dred, ired, &mbar,
+                                         st, sel);
         if (D.sel) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) D.sel[base + e] = resampled ? sel[e] : -1;
+            for (int e = 0; e < E; ++e) D.sel[base + e] = rs == PF_RS_RESAMPLED ? sel[e] : -1;
         }
     }
-    if (!resampled) {
+    if (rs == PF_RS_LOST) {
+        // bulk copies may still be landing in dynamic shared memory, which G..S
+        // reuse: skip them (the status word already reports the timeout); the
+        // estimate tickets still count this CTA so the next step starts clean
+        if (tid < 32) estimate_last_done<S>(D, X, b, in, step_ctr, tid);
+        return;
+    }
+    if (rs != PF_RS_RESAMPLED) {
 #pragma unroll
         for (int v = 0; v < S; ++v) {
             float o[E];
@@ -176,8 +183,8 @@ __global__ void __launch_bounds__(M / E) k_resample_only_cta(const FilterDesc* _
     const float* ru = D.ru + (int64_t)b * D.ru_stride;
     float st[E][S];
     int sel[E];
-    const bool resampled =
-        resample_from<S, M, E, RES>(D, b, t_tmp, t_key, ru, exchange_count(D), smem, dred, ired, &mbar, st, sel);
+    const bool resampled = resample_from<S, M, E, RES>(D, b, t_tmp, t_key, ru, exchange_count(D), smem, dred, ired,
+                                                       &mbar, st, sel) == PF_RS_RESAMPLED;
     if (D.sel) {
 #pragma unroll
         for (int e = 0; e < E; ++e) D.sel[base + e] = resampled ? sel[e] : -1;

@@ -269,10 +269,12 @@ void* pf_stream(pf_filter* f);
 /* Resolved configuration: pipeline actually used, particles per thread, torus dims, device bytes. */
 pf_status pf_get_info(pf_filter* f, int32_t* pipeline, int32_t* particles_per_thread, int32_t* torus_dx,
                       int32_t* torus_dy, int64_t* device_bytes);
-/* Snapshot / restore of particles, sorted keys and MTGP stream words (host buffer of pf_snapshot_size bytes). */
+/* Snapshot / restore of particles, MTGP stream words and the step count (host buffer of
+ * pf_snapshot_size bytes; restore rejects a buffer whose size differs with PF_ERR_INVALID,
+ * before reading past it). */
 int64_t pf_snapshot_size(pf_filter* f);
 pf_status pf_snapshot(pf_filter* f, void* host_buf);
-pf_status pf_restore(pf_filter* f, const void* host_buf);
+pf_status pf_restore(pf_filter* f, const void* host_buf, size_t size);
 
 /* ---- batched filters: many independent filters of uneven sizes stepped together ----
  * The reference runs one filter per process (particle_filter, pf_generic_soa.cu:686);
@@ -391,10 +393,12 @@ pf_status pf_server_get_particles(pf_server* s, int32_t id, float* soa, float* s
  * Restore targets an open filter of the same model and particle count (opened
  * with the same parameters for the same results) and replaces its particles,
  * streams and update count; its next updates then give the results the
- * snapshotted filter would have given. */
+ * snapshotted filter would have given.  Restore takes the buffer's size and
+ * rejects one that is not pf_server_snapshot_size bytes (a truncated transfer)
+ * with PF_ERR_INVALID before reading past it. */
 int64_t pf_server_snapshot_size(const pf_server* s, int32_t id);
 pf_status pf_server_snapshot(pf_server* s, int32_t id, void* host_buf);
-pf_status pf_server_restore(pf_server* s, int32_t id, const void* host_buf);
+pf_status pf_server_restore(pf_server* s, int32_t id, const void* host_buf, size_t size);
 
 /* ---- the served tracking load (request loop over pf_server_*, host C) ----
  * Poisson arrivals at `rate` per second for `duration_s`; each request is a
@@ -444,6 +448,17 @@ pf_status pfk_mtgp_generate(int32_t G, uint32_t seed, uint32_t mask, int32_t kin
  * pf_synchronize return as PF_ERR_TIMEOUT), 0 had it completed.  The context
  * stays usable. */
 pf_status pfk_bounded_wait_test(int32_t limit, int32_t* status);
+/* The same wait made CTA-wide, with a bulk copy of 32 KB really in flight
+ * into shared memory and a poll limit per thread (limits[nthreads], 0..2^20;
+ * 0: that thread gives up at once while the others may see the copy land).
+ * The threads agree on one outcome: outcome[tid] = 1 (landed within the
+ * first wait), 0 (some thread ran out; the copy landed in the second wait, so
+ * the kernels report PF_ERR_TIMEOUT and keep their propagated particles) or
+ * -1 (the copy may still be in flight: the kernel leaves that shared memory
+ * alone).  *copied = 1 when the shared words equal the source once the block
+ * went on, 0 when not, -1 after outcome -1.  nthreads: 32..1024, a multiple
+ * of 32.  No counterpart in the reference. */
+pf_status pfk_bounded_wait_mixed_test(const int32_t* limits, int32_t nthreads, int32_t* outcome, int32_t* copied);
 /* In-place Box-Muller over pairs (2i, 2i+1), 2i < n (boxmuller, pf_generic_soa.cu:481-500).
  * data must hold 2*ceil(n/2) floats. */
 pf_status pfk_boxmuller(float* data, int64_t n);
@@ -480,7 +495,9 @@ pf_status pfk_estimate(const float* keys, const float* state, int32_t num_state,
  * sized for at most 4096 sub-filters (num_particles / m), about 1.15 MB held
  * by every GPU that loads the library.  Larger inputs return PF_ERR_INVALID.
  * The first call on a device looks up the array's device address (make that
- * call before any stream capture).  All calls share the array and every call
+ * call before any stream capture); the address is kept per device and CUDA
+ * context, so the first call after cudaDeviceReset (or from another context
+ * on the same device) looks it up again.  All calls share the array and every call
  * overwrites the entries it reads, so nothing needs clearing; calls that
  * overlap on the GPU (other streams, other threads) race on it.
  * Asynchronous on `stream` (a cudaStream_t, NULL = default stream). */

@@ -3,10 +3,12 @@
 # (src/models/robotarm/cuda/pf_model_soa_packed_code.cuh, straight from the
 # Esthera tree) behind the C-ABI of oracle/ref_camarm_harness.cu into
 # oracle/_ref/libref_camarm.so.  Test infrastructure only.  Needs the
-# reference tree (default /root/reference); outputs only into oracle/_ref/.
+# reference tree ($ESTHERA_REF, else ../reference beside the repository);
+# outputs only into oracle/_ref/.
 set -e
-REF=${ESTHERA_REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the Esthera tree: $ESTHERA_REF, else a checkout named "reference" beside the repository
+REF=${ESTHERA_REF:-$HERE/../../reference}
 SRC="$REF/src/models/robotarm/cuda"
 [ -f "$SRC/pf_model_soa_packed_code.cuh" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
 NVCC=${NVCC:-$( [ -x /usr/local/cuda/bin/nvcc ] && echo /usr/local/cuda/bin/nvcc || echo nvcc)}

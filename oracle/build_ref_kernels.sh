@@ -4,10 +4,12 @@
 # model header, straight from the Esthera tree, cuRAND build, its main()
 # renamed) behind the C-ABI of oracle/ref_kernels_harness.cu into
 # oracle/_ref/libref_kernels.so.  Test infrastructure only.  Needs the
-# reference tree (default /root/reference); outputs only into oracle/_ref/.
+# reference tree ($ESTHERA_REF, else ../reference beside the repository);
+# outputs only into oracle/_ref/.
 set -e
-REF=${ESTHERA_REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the Esthera tree: $ESTHERA_REF, else a checkout named "reference" beside the repository
+REF=${ESTHERA_REF:-$HERE/../../reference}
 SRC="$REF/src/partfilt/cuda"
 [ -f "$SRC/pf_generic_soa.cu" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
 NVCC=${NVCC:-$( [ -x /usr/local/cuda/bin/nvcc ] && echo /usr/local/cuda/bin/nvcc || echo nvcc)}

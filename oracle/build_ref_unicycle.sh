@@ -4,11 +4,12 @@
 # cuRAND build, its main() renamed, the legacy cutil.h replaced by
 # oracle/cutil_shim/cutil.h) behind the C-ABI of
 # oracle/ref_unicycle_harness.cu into oracle/_ref/libref_unicycle.so.  Test
-# infrastructure only.  Needs the reference tree (default /root/reference);
-# outputs only into oracle/_ref/.
+# infrastructure only.  Needs the reference tree ($ESTHERA_REF, else
+# ../reference beside the repository); outputs only into oracle/_ref/.
 set -e
-REF=${ESTHERA_REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the Esthera tree: $ESTHERA_REF, else a checkout named "reference" beside the repository
+REF=${ESTHERA_REF:-$HERE/../../reference}
 SRC="$REF/src/models/unicycle"
 [ -f "$SRC/particle_filter.cu" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
 NVCC=${NVCC:-$( [ -x /usr/local/cuda/bin/nvcc ] && echo /usr/local/cuda/bin/nvcc || echo nvcc)}

@@ -100,6 +100,8 @@ def _declare(L):
                                       C.c_uint32, C.c_uint32, fp]),
         "orc_filter_free": (None, [C.POINTER(OrcFilter)]),
         "orc_filter_step": (C.c_int, [C.POINTER(OrcFilter), fp, fp, C.POINTER(OrcEstimate), ip, C.c_int]),
+        "orc_filter_sample": (C.c_int, [C.POINTER(OrcFilter), fp, fp, C.POINTER(OrcEstimate), C.c_int]),
+        "orc_filter_resample": (C.c_int, [C.POINTER(OrcFilter), ip, C.c_int]),
         "orc_stream_draws": (C.c_int64, [C.c_int, C.c_int, C.c_int]),
     }
     for n, (r, a) in sig.items():
@@ -321,6 +323,29 @@ class Filter:
         sel = np.zeros(self.m * self.N, np.int32) if want_sel else None
         lib().orc_filter_step(C.byref(self.f), _f(c), _f(z), C.byref(e), None if sel is None else _i(sel), threads)
         return e, sel
+
+    def sample(self, control, meas, threads=0):
+        """First half of step(): propagate + weight, sort, estimate."""
+        e = OrcEstimate()
+        c = np.ascontiguousarray(control, np.float32)
+        z = np.ascontiguousarray(meas, np.float32)
+        lib().orc_filter_sample(C.byref(self.f), _f(c), _f(z), C.byref(e), threads)
+        return e
+
+    def resample(self, threads=0):
+        """Second half of step(): exchange + resampling from the sorted copy; the selection."""
+        sel = np.zeros(self.m * self.N, np.int32)
+        lib().orc_filter_resample(C.byref(self.f), _i(sel), threads)
+        return sel
+
+    def set_sorted(self, soa, keys):
+        """Replace the sorted copy (S x T states, T keys) between sample() and resample()."""
+        T = self.m * self.N
+        a = np.ascontiguousarray(soa, np.float32).reshape(-1)
+        k = np.ascontiguousarray(keys, np.float32).reshape(-1)
+        assert a.size == self.S * T and k.size == T
+        C.memmove(self.f.tmp, a.ctypes.data, 4 * self.S * T)
+        C.memmove(self.f.tkey, k.ctypes.data, 4 * T)
 
     def set_dt(self, dt):
         self.f.mdl.dt = dt

@@ -627,6 +627,12 @@ void orc_filter_free(orc_filter* f)
 int orc_filter_step(orc_filter* f, const float* control, const float* meas, orc_estimate* est,
                     int32_t* sel_out, int threads)
 {
+    int r = orc_filter_sample(f, control, meas, est, threads);
+    return r ? r : orc_filter_resample(f, sel_out, threads);
+}
+
+int orc_filter_sample(orc_filter* f, const float* control, const float* meas, orc_estimate* est, int threads)
+{
     const int m = f->m, N = f->N, S = f->mdl.num_state, K = f->mdl.num_noise;
     const int64_t T = f->T;
     const int64_t draws = orc_stream_draws(K, m, f->resampler);
@@ -719,6 +725,20 @@ int orc_filter_step(orc_filter* f, const float* control, const float* meas, orc_
         est->log_norm = (f->log_weights ? gmax : 0.0) + log(Ssum);
     }
     free(part);
+    return 0;
+}
+
+int orc_filter_resample(orc_filter* f, int32_t* sel_out, int threads)
+{
+    const int m = f->m, N = f->N, S = f->mdl.num_state, K = f->mdl.num_noise;
+    const int64_t T = f->T;
+    const int64_t draws = orc_stream_draws(K, m, f->resampler);
+    const int64_t nb = 2 * (((int64_t)K * m + 1) / 2);
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#else
+    threads = 1;
+#endif
     /* 4. exchange routing */
     int32_t* src = (int32_t*)malloc(sizeof(int32_t) * (size_t)T);
     float* topk = NULL;

@@ -185,6 +185,15 @@ void orc_filter_free(orc_filter* f);
  * -1 for sub-filters that skipped resampling). threads <= 0: all cores. */
 int orc_filter_step(orc_filter* f, const float* control, const float* meas,
                     orc_estimate* est, int32_t* sel, int threads);
+/* The two halves of orc_filter_step: orc_filter_sample runs steps RNG,
+ * propagate + weight, sort, winner and estimate (state propagated in place,
+ * tmp / tkey the sorted copy); orc_filter_resample runs the exchange and the
+ * resampling from tmp / tkey with this step's uniforms into state.  A test
+ * may replace tmp / tkey in between (e.g. with a device's own sorted copy) to
+ * check exchange routing and resampling given identical weights. */
+int orc_filter_sample(orc_filter* f, const float* control, const float* meas,
+                      orc_estimate* est, int threads);
+int orc_filter_resample(orc_filter* f, int32_t* sel, int threads);
 
 /* Number of uniforms one sub-filter stream consumes per step in
  * ORC_RNG_SUBFILTER mode. */

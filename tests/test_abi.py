@@ -91,6 +91,10 @@ def test_config_validation(E, kw, msg):
 def test_bounded_wait_argument_checks(E):
     with pytest.raises(E.PFError):
         E.bounded_wait_test(0)
+    for lim in (np.zeros(48, np.int32), np.zeros(2048, np.int32), np.full(64, -1, np.int32)):
+        with pytest.raises(E.PFError) as ei:
+            E.bounded_wait_mixed_test(lim)
+        assert ei.value.status == E.PF_ERR_INVALID
 
 
 def test_no_cpu_fallback(E):

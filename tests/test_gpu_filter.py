@@ -218,6 +218,9 @@ def test_snapshot_restore(gpu):
     snap = f.snapshot()
     a = [f.step(inputs[k]) for k in range(4, 8)]
     pa = f.particles()
+    with pytest.raises(E.PFError) as ei:
+        f.restore(snap[:-4])  # truncated: refused before it is read
+    assert ei.value.status == E.PF_ERR_INVALID
     f.restore(snap)
     b = [f.step(inputs[k]) for k in range(4, 8)]
     assert np.array_equal(pa, f.particles())

@@ -1,0 +1,126 @@
+"""Parity at the exact shapes the bench measures.
+
+* 2^20-particle unicycle filter: 2048 sub-filters of 512 on a 32 x 64 torus,
+  t = 2, landmarks and trajectory from seed 2; systematic and Vose resampling.
+* 2^18-particle 6-joint DH arm: 1024 sub-filters of 256 on a 32 x 32 torus,
+  t = 1, DH parameters and trajectory from seed 3; systematic resampling.
+
+Per step (three steps, the engine re-seeded from the oracle's particles before
+each, so every step is compared on equal inputs):
+  * sorted log-weights of every sub-filter within FP32 tolerance of the
+    oracle's FP64 model (1e-4 relative + 2e-3 absolute for the unicycle,
+    + 5e-3 for the arm), sorted states equal to 1e-4 wherever the FP32 and FP64
+    keys put the particle at the same sorted position (>= 97 %);
+  * exchange routing + resampling given identical weights and uniforms: the
+    oracle's exchange and resampler run on the engine's own sorted copy must
+    select the same slots for all 2^20 (2^18) particles and produce the same
+    resampled particles, bit for bit;
+  * the estimate (log normalisation, posterior mean) within tolerance.
+Over 100 free-running steps the tracking RMSE against the seeded ground
+truth equals the oracle's within 5 % + 0.005.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+UNI, ARM = 0, 1
+
+
+def _shape(E, model, res):
+    if model == UNI:
+        return dict(particles_per_subfilter=512, num_subfilters=2048, num_transfer=2, exchange=E.EXCHANGE_TORUS,
+                    resampler=res, pipeline=E.PIPELINE_SPLIT)
+    return dict(particles_per_subfilter=256, num_subfilters=1024, num_transfer=1, exchange=E.EXCHANGE_TORUS,
+                resampler=res, pipeline=E.PIPELINE_SPLIT)
+
+
+def _setup(E, model, steps):
+    if model == UNI:
+        p = E.unicycle_params(2)
+        inputs, truth = E.make_trace(UNI, p, 2, steps)
+    else:
+        p = E.dharm_params(3)
+        inputs, truth = E.make_trace(ARM, p, 3, steps)
+    return p, inputs, truth
+
+
+def _oracle(E, O, model, p, cfg, ppt):
+    md = O.model_from_params(model, p)
+    return O.Filter(md, cfg["particles_per_subfilter"], cfg["num_subfilters"], cfg["num_transfer"], O.EXCH_TORUS,
+                    cfg["resampler"], O.RNG_SUBFILTER, 96, ppt, 1, 1.0, 0xF000000D, 0,
+                    np.array(p.init_state, np.float32))
+
+
+def _angle_rows(model):
+    return [2] if model == UNI else list(range(6))
+
+
+@pytest.mark.parametrize("model,res", [(UNI, 1), (UNI, 2), (ARM, 1)])
+def test_steps_vs_oracle_at_bench_shape(gpu, O, model, res):
+    E = gpu
+    p, inputs, _ = _setup(E, model, 3)
+    cfg = _shape(E, model, res)
+    f = E.ParticleFilter(model, p, **cfg)
+    info = f.info()
+    assert info["pipeline"] == E.PIPELINE_SPLIT
+    assert info["torus"] == ((32, 64) if model == UNI else (32, 32))
+    f.record_selection(True)
+    of = _oracle(E, O, model, p, cfg, info["particles_per_thread"])
+    m, N = cfg["particles_per_subfilter"], cfg["num_subfilters"]
+    katol = 2e-3 if model == UNI else 5e-3
+    for k in range(3):
+        if k > 0:
+            f.set_particles(of.state())
+        ge = f.step(inputs[k])
+        oe = of.sample(inputs["control"][k], inputs["meas"][k])
+        gs, gk = f.sorted()
+        os_, ok = of.sorted()
+        assert ge["flags"] == 0
+        assert np.all(gk.reshape(N, m)[:, :-1] >= gk.reshape(N, m)[:, 1:])
+        assert np.all(np.abs(gk - ok) <= 1e-4 * np.abs(ok) + katol), np.max(np.abs(gk - ok))
+        d = np.abs(gs.astype(np.float64) - os_)
+        for a in _angle_rows(model):
+            d[a] = np.abs(np.angle(np.exp(1j * (gs[a].astype(np.float64) - os_[a]))))
+        same = d.max(axis=0) < 1e-4
+        assert same.mean() > 0.97, same.mean()
+        assert abs(ge["log_norm"] - oe.log_norm) < 1e-3 * abs(oe.log_norm) + 1e-3
+        S = 3 if model == UNI else 12
+        lin = [v for v in range(S) if v not in _angle_rows(model)]
+        assert np.allclose(np.array(ge["mean"])[lin], np.array(oe.mean)[:S][lin], atol=2e-3)
+        for a in _angle_rows(model):
+            assert abs(np.angle(np.exp(1j * (ge["mean"][a] - oe.mean[a])))) < 2e-3
+        # exchange + resampling given identical weights and uniforms: bit for bit
+        of.set_sorted(gs, gk)
+        osel = of.resample()
+        gsel = f.selection()
+        assert np.array_equal(gsel, osel), np.mean(gsel == osel)
+        assert np.array_equal(f.particles(), of.state())
+
+
+def _rmse(model, means, truth):
+    if model == UNI:
+        m = np.array([e[:2] for e in means])
+        return float(np.sqrt(np.mean(np.sum((m - truth[:, :2]) ** 2, axis=1))))
+    q = np.array([e[:6] for e in means])
+    err = np.angle(np.exp(1j * (q - truth[:, :6])))
+    return float(np.sqrt(np.mean(err[20:] ** 2)))
+
+
+@pytest.mark.parametrize("model,res", [(UNI, 1), (UNI, 2), (ARM, 1)])
+def test_rmse_vs_oracle_at_bench_shape(gpu, O, model, res):
+    """100 free-running steps (no re-seeding): the engine's and the oracle's
+    tracking RMSE against the seeded ground truth agree within 5 % + 0.005."""
+    E = gpu
+    steps = 100
+    p, inputs, truth = _setup(E, model, steps)
+    cfg = _shape(E, model, res)
+    f = E.ParticleFilter(model, p, **cfg)
+    of = _oracle(E, O, model, p, cfg, f.info()["particles_per_thread"])
+    g, o = [], []
+    for k in range(steps):
+        g.append(np.array(f.step(inputs[k])["mean"]))
+        o.append(np.array(of.step(inputs["control"][k], inputs["meas"][k])[0].mean))
+    rg, ro = _rmse(model, g, truth), _rmse(model, o, truth)
+    assert rg < (0.25 if model == UNI else 0.06) and ro < (0.25 if model == UNI else 0.06), (rg, ro)
+    assert abs(rg - ro) <= 0.05 * ro + 0.005, (rg, ro)

@@ -195,3 +195,22 @@ def test_bounded_wait_reports_timeout_and_context_survives(gpu):
     keys = np.arange(512, dtype=np.float32)[::-1].copy()
     k, i = gpu.bitonic_sort(keys[::-1].copy(), 512, 4)
     assert np.array_equal(k, keys) and np.array_equal(i, np.arange(512)[::-1])
+
+
+@pytest.mark.parametrize("nthreads,give_up", [(128, [5]), (256, [0, 31, 200]), (512, list(range(0, 512, 2)))])
+def test_bounded_wait_is_cta_wide_with_copies_in_flight(gpu, nthreads, give_up):
+    """Some threads' waits run out (poll limit 0, set on the host) while the
+    others see the bulk copy land: every thread must take the same branch, and
+    the copy must have landed in shared memory before the block went on."""
+    limits = np.full(nthreads, 1 << 18, np.int32)
+    limits[give_up] = 0
+    out, copied = gpu.bounded_wait_mixed_test(limits)
+    assert np.all(out == out[0]), np.unique(out)
+    assert out[0] == 0 and copied == 1
+    # no thread gives up: the first wait succeeds everywhere
+    out, copied = gpu.bounded_wait_mixed_test(np.full(nthreads, 1 << 18, np.int32))
+    assert np.all(out == 1) and copied == 1
+    # the context is still usable
+    keys = np.arange(256, dtype=np.float32)
+    k, _ = gpu.bitonic_sort(keys, 256, 4)
+    assert np.array_equal(k, keys[::-1])

@@ -14,9 +14,20 @@ import pytest
 sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
 import ref_kernels as R  # noqa: E402
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not R.available(), reason="oracle/_ref/libref_kernels.so not built "
-                                                           "(oracle/build_ref_kernels.sh needs the reference tree)")]
+pytestmark = pytest.mark.gpu
+
+
+def _require(built, lib, recipe):
+    """The reference's own kernels are the strongest parity evidence: a missing
+    library fails the test instead of skipping it (build() makes them wherever
+    the Esthera tree is present, and the built files travel with the tree)."""
+    if not built:
+        pytest.fail("oracle/_ref/%s is missing: run oracle/%s (needs the Esthera tree)" % (lib, recipe))
+
+
+@pytest.fixture(autouse=True)
+def _reference_kernels_built():
+    _require(R.available(), "libref_kernels.so", "build_ref_kernels.sh")
 
 PPT = {32: [1], 64: [2], 128: [2, 4], 256: [2, 4, 8], 512: [2, 4, 16], 1024: [2, 4]}
 
@@ -105,8 +116,6 @@ def test_refarm_model_equals_reference_kernel(gpu):
     assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
 
 
-@pytest.mark.skipif(not R.unicycle_available(), reason="oracle/_ref/libref_unicycle.so not built "
-                                                     "(oracle/build_ref_unicycle.sh needs the reference tree)")
 @pytest.mark.parametrize("w0,dt", [(0.2, 1.0), (-0.6, 0.5), (1.5, 1.0)])
 def test_beacon_model_equals_reference_kernel(gpu, w0, dt):
     """The engine's beacon model against the reference unicycle program's own
@@ -117,6 +126,7 @@ def test_beacon_model_equals_reference_kernel(gpu, w0, dt):
     and one ulp of each sine; the engine evaluates the arc without that
     difference); log-likelihoods within 1e-4 relative + 5e-3 absolute of
     log(weight)."""
+    _require(R.unicycle_available(), "libref_unicycle.so", "build_ref_unicycle.sh")
     E = gpu
     rng = np.random.default_rng(int(100 * abs(w0)) + int(10 * dt))
     n = 4096
@@ -144,14 +154,13 @@ def test_beacon_model_equals_reference_kernel(gpu, w0, dt):
     assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
 
 
-@pytest.mark.skipif(not R.camarm_available(), reason="oracle/_ref/libref_camarm.so not built "
-                                                   "(oracle/build_ref_camarm.sh needs the reference tree)")
 @pytest.mark.parametrize("ang", [1.2, 2.0])
 def test_camarm_model_equals_reference_kernel(gpu, O, ang):
     """The engine's camera-arm model against the reference's own pinhole-camera
     sampling_iw (pf_model_soa_packed_code.cuh:61-145) on the same particles,
     normals, controls and pixel measurements: states within 2e-5,
     log-likelihoods within 1e-4 relative + 5e-3 absolute of log(weight)."""
+    _require(R.camarm_available(), "libref_camarm.so", "build_ref_camarm.sh")
     import test_camarm as T
     E = gpu
     p = E.camarm_params()

@@ -191,6 +191,9 @@ def test_server_snapshot_restore_moves_a_filter(gpu):
     with pytest.raises(E.PFError) as ei:
         dst.restore(small, snap)
     assert ei.value.status == E.PF_ERR_INVALID
+    with pytest.raises(E.PFError) as ei:
+        dst.restore(b, snap[: len(snap) // 2])  # a truncated transfer is refused before it is read
+    assert ei.value.status == E.PF_ERR_INVALID
     dst.restore(b, snap)
     for k in range(3, 7):
         dst.update(b, inputs[k], tag=k)

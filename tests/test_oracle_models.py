@@ -143,3 +143,24 @@ def test_oracle_ess_gate(O, E, res):
     st, srt = gated.state().reshape(3, N, m), gated.sorted()[0].reshape(3, N, m)
     for b in np.flatnonzero(skipped):
         assert np.array_equal(np.sort(st[0, b]), np.sort(srt[0, b]))
+
+
+def test_oracle_step_equals_sample_then_resample(O, E):
+    """orc_filter_step is orc_filter_sample followed by orc_filter_resample, and
+    handing the resampler its own sorted copy back changes nothing."""
+    p = E.unicycle_params(2)
+    inputs, _ = E.make_trace(0, p, 2, 3)
+    md = O.model_from_params(0, p)
+    for res in (0, 1, 2):
+        a = O.Filter(md, 128, 16, 2, O.EXCH_TORUS, res, O.RNG_SUBFILTER, 96, 4, 1, 1.0, 0xF000000D, 0,
+                     np.zeros(3, np.float32))
+        b = O.Filter(md, 128, 16, 2, O.EXCH_TORUS, res, O.RNG_SUBFILTER, 96, 4, 1, 1.0, 0xF000000D, 0,
+                     np.zeros(3, np.float32))
+        for k in range(3):
+            ea, sa = a.step(inputs["control"][k], inputs["meas"][k], want_sel=True)
+            eb = b.sample(inputs["control"][k], inputs["meas"][k])
+            s, kk = b.sorted()
+            b.set_sorted(s, kk)
+            sb = b.resample()
+            assert np.array_equal(sa, sb) and np.array_equal(a.state(), b.state())
+            assert ea.log_norm == eb.log_norm and list(ea.mean) == list(eb.mean)

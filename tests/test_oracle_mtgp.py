@@ -48,9 +48,9 @@ def test_cuda_reference_mask_differs(O, golden):
     assert not np.array_equal(cm, golden["kat_f32_0_1"])
 
 
-def test_live_reference_library_if_built(O):
+def test_live_reference_library(O):
     if O.ref_lib() is None:
-        pytest.skip("oracle/_ref not built in this checkout")
+        pytest.fail("oracle/_ref/libmtgp_ref.so is missing: run oracle/build_ref.sh (needs the Esthera tree)")
     for set_, seed in [(3, 9), (150, 0xDEADBEEF), (199, 0)]:
         for kind in (0, 1):
             assert np.array_equal(O.mtgp_stream(set_, seed, 2000, kind=kind), O.ref_mtgp_stream(set_, seed, 2000, kind))

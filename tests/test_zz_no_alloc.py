@@ -44,6 +44,26 @@ def test_noalloc_matches_allocating_entry_point(gpu, lw):
         assert np.array_equal(got["best"][:3], ref["best"][:3]) and got["flags"] == ref["flags"] == 0
 
 
+def test_noalloc_allocates_no_device_memory(gpu):
+    """The one promise of the entry point: after a first call (which loads the
+    module and looks up its scratch address), further calls leave the device's
+    free memory unchanged."""
+    import torch
+    E = gpu
+    keys, st = _inputs(7, 512, 2048, 1)
+    dk = torch.from_numpy(keys).cuda()
+    ds = torch.from_numpy(np.ascontiguousarray(st)).cuda()
+    dout = torch.zeros(E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    E.estimate_noalloc(dk.data_ptr(), ds.data_ptr(), 3, len(keys), 512, dout.data_ptr(), 0b100, 1)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(20):
+        E.estimate_noalloc(dk.data_ptr(), ds.data_ptr(), 3, len(keys), 512, dout.data_ptr(), 0b100, 1)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_rejects_more_than_its_scratch(gpu):
     import torch
     E = gpu
