@@ -204,6 +204,32 @@ __device__ __forceinline__ float pf_atan2(float y, float x)
     return copysignf(r, y);
 }
 
+// exp(x) for the resampling's max-subtracted log-weights x <= 0, from
+// correctly rounded FP32 operations only (no SFU approximation), so that the
+// oracle's restatement (orc_expneg) gives the same bits and resampling is
+// bit-identical given identical log-weights: n = rint(x log2 e), r = x - n ln2
+// (Cody-Waite split, two fmaf), exp(x) = 2^n P(r), P of degree 6 fitted for
+// this project (least squares + Lawson iterations on [-ln2/2, ln2/2],
+// relative error 2.3e-9; fit_exp.py beside this file regenerates and checks
+// it: at most 2 ulp on [-87, 0]).  x < -87 (and -inf) gives 0, NaN stays NaN.
+__device__ __forceinline__ float pf_expneg(float x)
+{
+    const float n = rintf(x * 1.442695022e+00f);
+    float r = fmaf(n, -0.693145751953125f, x);
+    r = fmaf(n, -1.428606765e-06f, r);
+    float p = 1.384175848e-03f;
+    p = fmaf(p, r, 8.375782520e-03f);
+    p = fmaf(p, r, 4.166811332e-02f);
+    p = fmaf(p, r, 1.666641235e-01f);
+    p = fmaf(p, r, 4.999999404e-01f);
+    p = fmaf(p, r, 1.000000000e+00f);
+    p = fmaf(p, r, 1.0f);
+    const int ni = (int)n;
+    const bool ok = x >= -87.0f && ni >= -126;
+    const float scale = __int_as_float((ok ? ni + 127 : 0) << 23);
+    return x != x ? x : (ok ? p * scale : 0.0f);
+}
+
 // sqrt(d2) for d2 >= 0 through the SFU reciprocal square root (0 -> 0).
 __device__ __forceinline__ float pf_sqrt(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 

@@ -956,7 +956,7 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
         for (int e = 1; e < E; ++e) mx = fmaxf(mx, w[e]);
         mx = block_max(mx, reinterpret_cast<float*>(ired));
 #pragma unroll
-        for (int e = 0; e < E; ++e) w[e] = __expf(w[e] - mx);
+        for (int e = 0; e < E; ++e) w[e] = pf_expneg(w[e] - mx);
     }
     if (D.ess_frac > 0.0f) {
         // effective sample size (sum w)^2 / sum w^2 in FP64; a sub-filter whose

@@ -103,6 +103,7 @@ def _declare(L):
         "orc_filter_sample": (C.c_int, [C.POINTER(OrcFilter), fp, fp, C.POINTER(OrcEstimate), C.c_int]),
         "orc_filter_resample": (C.c_int, [C.POINTER(OrcFilter), ip, C.c_int]),
         "orc_stream_draws": (C.c_int64, [C.c_int, C.c_int, C.c_int]),
+        "orc_expneg": (C.c_float, [C.c_float]),
     }
     for n, (r, a) in sig.items():
         f = getattr(L, n)
@@ -374,6 +375,12 @@ class Filter:
             self.close()
         except Exception:
             pass
+
+
+def expneg(x):
+    """orc_expneg element-wise (FP32 in, FP32 out)."""
+    x = np.ascontiguousarray(x, np.float32).reshape(-1)
+    return np.array([lib().orc_expneg(C.c_float(float(v))) for v in x], np.float32)
 
 
 def stream_draws(num_noise, m, resampler):

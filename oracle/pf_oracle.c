@@ -579,6 +579,36 @@ static int is_angle(const orc_model* md, int v)
 }
 
 /* ---------------- whole filter ---------------- */
+/* exp(x) for max-subtracted log-weights x <= 0 from correctly rounded FP32
+ * operations only: n = rint(x log2 e), r = x - n ln2 (Cody-Waite, two fmaf),
+ * exp(x) = 2^n P(r) with the project's degree-6 fit of P (the engine's
+ * pf_expneg evaluates the same operations in the same order, so both give the
+ * same bits; esthera_b200/csrc/fit_exp.py fits and checks the polynomial).
+ * x < -87 (and -inf) gives 0; NaN stays NaN. */
+float orc_expneg(float x)
+{
+    const float n = rintf(x * 1.442695022e+00f);
+    float r = fmaf(n, -0.693145751953125f, x);
+    r = fmaf(n, -1.428606765e-06f, r);
+    float p = 1.384175848e-03f;
+    p = fmaf(p, r, 8.375782520e-03f);
+    p = fmaf(p, r, 4.166811332e-02f);
+    p = fmaf(p, r, 1.666641235e-01f);
+    p = fmaf(p, r, 4.999999404e-01f);
+    p = fmaf(p, r, 1.000000000e+00f);
+    p = fmaf(p, r, 1.0f);
+    if (x != x) return x;
+    if (!(x >= -87.0f)) return 0.0f;
+    const int ni = (int)n;
+    if (ni < -126) return 0.0f;
+    union {
+        uint32_t u;
+        float f;
+    } sc;
+    sc.u = (uint32_t)(ni + 127) << 23;
+    return p * sc.f;
+}
+
 int64_t orc_stream_draws(int num_noise, int m, int resampler)
 {
     int64_t nb = 2 * (((int64_t)num_noise * m + 1) / 2);
@@ -770,7 +800,7 @@ int orc_filter_resample(orc_filter* f, int32_t* sel_out, int threads)
             if (w[s] > mx) mx = w[s];
         }
         if (f->log_weights)
-            for (int s = 0; s < m; ++s) w[s] = expf(w[s] - mx);
+            for (int s = 0; s < m; ++s) w[s] = orc_expneg(w[s] - mx);
         if (f->ess_frac > 0.0f) {
             /* effective sample size in FP64; all-zero weights count as uniform */
             double s1 = 0.0, s2 = 0.0;

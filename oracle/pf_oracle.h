@@ -195,6 +195,10 @@ int orc_filter_sample(orc_filter* f, const float* control, const float* meas,
                       orc_estimate* est, int threads);
 int orc_filter_resample(orc_filter* f, int32_t* sel, int threads);
 
+/* exp of a max-subtracted log-weight (x <= 0) from correctly rounded FP32
+ * operations only, bit-identical to the engine's resampling weights. */
+float orc_expneg(float x);
+
 /* Number of uniforms one sub-filter stream consumes per step in
  * ORC_RNG_SUBFILTER mode. */
 int64_t orc_stream_draws(int num_noise, int m, int resampler);

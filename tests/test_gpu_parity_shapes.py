@@ -9,9 +9,9 @@ Per step (three steps, the engine re-seeded from the oracle's particles before
 each, so every step is compared on equal inputs):
   * sorted log-weights of every sub-filter within FP32 tolerance of the
     oracle's FP64 model (1e-4 relative + 2e-3 absolute for the unicycle,
-    + 5e-3 for the arm), sorted states equal to 1e-4 wherever the FP32 and FP64
-    keys put the particle at the same sorted position (>= 97 %);
-  * exchange routing + resampling given identical weights and uniforms: the
+    + 5e-3 for the arm); propagated states equal to 1e-4, each sub-filter's
+    particles compared in the order of a tie-free coordinate (>= 99 %);
+  * exchange routing + resampling given identical log-weights and uniforms: the
     oracle's exchange and resampler run on the engine's own sorted copy must
     select the same slots for all 2^20 (2^18) particles and produce the same
     resampled particles, bit for bit;
@@ -56,6 +56,26 @@ def _angle_rows(model):
     return [2] if model == UNI else list(range(6))
 
 
+def _same_particles(gs, os_, m, N, model):
+    """Fraction of particles equal (1e-4, angles wrapped) when each sub-filter's
+    propagated particles are put in the order of a coordinate that has no ties
+    (x for the unicycle, a joint velocity for the arm: both take fresh noise
+    every step).  Sorted positions are not compared: resampled duplicates share
+    their key exactly (the arm's joint angles advance with the velocity of the
+    previous step), and the network's placement of such ties follows near-ties
+    elsewhere in the sub-filter, where FP32 and FP64 keys may order differently."""
+    S = gs.shape[0]
+    col = 0 if model == UNI else 6
+    g = gs.reshape(S, N, m).astype(np.float64)
+    o = os_.reshape(S, N, m).astype(np.float64)
+    g = np.take_along_axis(g, np.argsort(g[col], axis=1, kind="stable")[None], axis=2)
+    o = np.take_along_axis(o, np.argsort(o[col], axis=1, kind="stable")[None], axis=2)
+    d = np.abs(g - o)
+    for a in _angle_rows(model):
+        d[a] = np.abs(np.angle(np.exp(1j * (g[a] - o[a]))))
+    return float((d.max(axis=0) < 1e-4).mean())
+
+
 @pytest.mark.parametrize("model,res", [(UNI, 1), (UNI, 2), (ARM, 1)])
 def test_steps_vs_oracle_at_bench_shape(gpu, O, model, res):
     E = gpu
@@ -79,11 +99,8 @@ def test_steps_vs_oracle_at_bench_shape(gpu, O, model, res):
         assert ge["flags"] == 0
         assert np.all(gk.reshape(N, m)[:, :-1] >= gk.reshape(N, m)[:, 1:])
         assert np.all(np.abs(gk - ok) <= 1e-4 * np.abs(ok) + katol), np.max(np.abs(gk - ok))
-        d = np.abs(gs.astype(np.float64) - os_)
-        for a in _angle_rows(model):
-            d[a] = np.abs(np.angle(np.exp(1j * (gs[a].astype(np.float64) - os_[a]))))
-        same = d.max(axis=0) < 1e-4
-        assert same.mean() > 0.97, same.mean()
+        same = _same_particles(gs, os_, m, N, model)
+        assert same > 0.99, same
         assert abs(ge["log_norm"] - oe.log_norm) < 1e-3 * abs(oe.log_norm) + 1e-3
         S = 3 if model == UNI else 12
         lin = [v for v in range(S) if v not in _angle_rows(model)]

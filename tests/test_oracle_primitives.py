@@ -170,3 +170,26 @@ def test_golden_pinned_to_reference_kernels(golden, m):
 def test_ring_golden_pinned_to_reference_kernel(golden):
     ref = np.load(Path(__file__).resolve().parent / "golden" / "ref_kernels.npz")
     assert np.array_equal(golden["exch_src_1_8_32_3"], ref["exch_src_1_8_32_3"])
+
+
+def test_oracle_expneg_accuracy(O):
+    """orc_expneg (the resampling weights' exponential, bit-identical to the
+    engine's) is within 2 ulp of exp on [-87, 0], 0 below, NaN for NaN."""
+    rng = np.random.default_rng(5)
+    x = np.concatenate([-rng.exponential(3.0, 20000), -rng.uniform(0, 87, 20000), [0.0, -1e-30, -87.0]])
+    x = x.astype(np.float32)
+    got = O.expneg(x).astype(np.float64)
+    ref = np.exp(x.astype(np.float64))
+    assert np.max(np.abs(got - ref) / np.spacing(ref.astype(np.float32))) <= 2.0
+    e = O.expneg(np.float32([-87.5, -100.0, -np.inf, np.nan]))
+    assert np.all(e[:3] == 0) and np.isnan(e[3])
+
+
+def test_exp_fit_script_checks_pass():
+    import importlib.util
+    from pathlib import Path
+    spec = importlib.util.spec_from_file_location(
+        "fit_exp", Path(__file__).resolve().parents[1] / "esthera_b200" / "csrc" / "fit_exp.py")
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    assert m.main([]) == 0
