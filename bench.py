@@ -30,8 +30,8 @@ roofline: the dominant kernel's algorithmic bytes (the sampling kernel reads
         roofline (its ncu warp-instruction count at 4 issues per cycle per
         SM at the sampled clock), the bound it actually meets.
 
-clocks: nvidia-smi samples (20 ms) over a window of about a second: untimed
-        steps of the same work for ~0.5 s before and after the timed ones.
+clocks: nvidia-smi samples (20 ms) over a window of more than a second:
+        untimed steps of the same work for ~0.8 s before and after the timed ones.
 latency_ms: pf_step's per-step latency on the host (p50/p99/p999) beside the
         device step times.
 
@@ -59,7 +59,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 ALG_BYTES = 24  # unicycle, per particle-step
-MAX_ROLL = 20000  # untimed steps at most on either side of the timed ones (clock window)
+MAX_ROLL = 40000  # untimed steps at most on either side of the timed ones (clock window)
 # single-filter workloads: model, sub-filter size, sub-filters, torus transfer,
 # seed, algorithmic bytes per particle-step (state read + write)
 WORKLOADS = {
@@ -481,9 +481,9 @@ def main():
     f.synchronize()
     per_step_s = (time.perf_counter() - t_w) / max(args.warmup - 1, 1)
     # the clock window: untimed steps (same work, same L2 flush) for about
-    # half a second before and after the timed steps, so the nvidia-smi
-    # samples (every 20 ms) cover at least a second of this load around them
-    roll = int(min(MAX_ROLL, max(1, np.ceil(0.5 / max(per_step_s, 1e-6)))))
+    # 0.8 s before and after the timed steps, so the nvidia-smi samples
+    # (every 20 ms) cover more than a second of this load around them
+    roll = int(min(MAX_ROLL, max(1, np.ceil(0.8 / max(per_step_s, 1e-6)))))
 
     def untimed(n):
         for k in range(n):

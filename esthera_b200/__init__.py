@@ -176,6 +176,7 @@ def _declare(L):
         "pfk_mtgp_generate": (C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, C.c_int64, C.c_int32, up]),
         "pfk_boxmuller": (C.c_int, [fp, C.c_int64]),
         "pfk_bitonic_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32]),
+        "pfk_rank_sort": (C.c_int, [fp, ip, C.c_int32, C.c_int32, C.c_int32, ip]),
         "pfk_resample": (C.c_int, [C.c_int32, fp, fp, C.c_int32, C.c_int32, C.c_int32, ip]),
         "pfk_vose_build": (C.c_int, [fp, C.c_int32, C.c_int32, C.c_int32, fp, up]),
         "pfk_exchange_sources": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, ip]),
@@ -724,6 +725,15 @@ def bounded_wait_mixed_test(limits):
     copied = C.c_int32(-2)
     check(lib().pfk_bounded_wait_mixed_test(_iptr(lim), len(lim), _iptr(out), C.byref(copied)))
     return out, copied.value
+
+
+def rank_sort(keys, m, ppt=0):
+    """pfk_rank_sort: (sorted keys, permutation, sub-filters that fell back to the full network)."""
+    k = np.array(keys, dtype=np.float32, copy=True)
+    idx = np.zeros(len(k), np.int32)
+    fb = C.c_int32(-1)
+    check(lib().pfk_rank_sort(_fptr(k), _iptr(idx), m, len(k) // m, ppt, C.byref(fb)))
+    return k, idx, fb.value
 
 
 def bitonic_sort(keys, m, ppt=0):

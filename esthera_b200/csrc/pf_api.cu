@@ -1134,9 +1134,30 @@ extern "C" pf_status pfk_bitonic_sort(float* keys, int32_t* idx, int32_t m, int3
     TRYS(dev_buf(dk, n * 4));
     TRYS(dev_buf(di, n * 4));
     CU(cudaMemcpy(dk.p, keys, n * 4, cudaMemcpyHostToDevice));
-    CU(launch_test_sort(m, E, nsub, (float*)dk.p, (int32_t*)di.p, 0));
+    CU(launch_test_sort(m, E, nsub, (float*)dk.p, (int32_t*)di.p, 0, nullptr, 0));
     CU(cudaMemcpy(keys, dk.p, n * 4, cudaMemcpyDeviceToHost));
     CU(cudaMemcpy(idx, di.p, n * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pfk_rank_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt,
+                                   int32_t* fallbacks)
+{
+    if (!keys || !idx || !fallbacks || nsub < 1) return fail(PF_ERR_INVALID, "bad argument");
+    const int E = pick_ppt(m, ppt);
+    if (!me_supported(m, E)) return fail(PF_ERR_UNSUPPORTED, "m=%d ppt=%d not built", m, E);
+    TRYS(require_gpu(0));
+    const size_t n = (size_t)m * nsub;
+    DevBuf dk, di, dc;
+    TRYS(dev_buf(dk, n * 4));
+    TRYS(dev_buf(di, n * 4));
+    TRYS(dev_buf(dc, 4));
+    CU(cudaMemcpy(dk.p, keys, n * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemset(dc.p, 0, 4));
+    CU(launch_test_sort(m, E, nsub, (float*)dk.p, (int32_t*)di.p, 1, (int32_t*)dc.p, 0));
+    CU(cudaMemcpy(keys, dk.p, n * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(idx, di.p, n * 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(fallbacks, dc.p, 4, cudaMemcpyDeviceToHost));
     return PF_OK;
 }
 

@@ -180,12 +180,14 @@ __global__ void k_a2a_merge_step(const FilterDesc* __restrict__ descs, StepState
 }
 
 
-cudaError_t launch_test_sort(int M, int E, int nsub, float* keys, int32_t* idx, cudaStream_t st)
+cudaError_t launch_test_sort(int M, int E, int nsub, float* keys, int32_t* idx, int rank, int32_t* fallbacks,
+                             cudaStream_t st)
 {
-#define PF_TS(m, e)                                                  \
-    if (M == m && E == e) {                                          \
-        k_test_sort<m, e><<<nsub, m / e, 0, st>>>(keys, idx);        \
-        return cudaGetLastError();                                   \
+#define PF_TS(m, e)                                                                  \
+    if (M == m && E == e) {                                                          \
+        if (rank) k_test_sort<m, e, true><<<nsub, m / e, 0, st>>>(keys, idx, fallbacks); \
+        else k_test_sort<m, e, false><<<nsub, m / e, 0, st>>>(keys, idx, fallbacks);    \
+        return cudaGetLastError();                                                   \
     }
     PF_ME_LIST(PF_TS)
 #undef PF_TS

@@ -61,6 +61,43 @@ __device__ __forceinline__ void mtgp_load(MtgpSmem& s, const uint32_t* __restric
     __syncthreads();
 }
 
+// mtgp_load with the global reads of the stream words issued first (into
+// registers, NT threads) and `work()` run while they are in flight -- the
+// sampling kernels compute the step's model constants there.  Same result as
+// mtgp_load; ends with a barrier.
+template <int NT, class Work>
+__device__ __forceinline__ void mtgp_load_overlap(MtgpSmem& s, const uint32_t* __restrict__ gstate, int set,
+                                                  uint32_t mask, Work work)
+{
+    constexpr int R = (kMtgpN + NT - 1) / NT;
+    const int tid = threadIdx.x;
+    uint32_t w[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * NT;
+        w[r] = i < kMtgpN ? __ldcs(gstate + i) : 0u;
+    }
+    const uint32_t* P = g_mtgp_params + set * 52;
+    const uint32_t tb = tid < 16 ? P[4 + tid] : 0u, tt = tid < 16 ? P[36 + tid] : 0u;
+    work();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = tid + r * NT;
+        if (i < kMtgpN) s.ring[i] = w[r];
+    }
+    if (tid < 16) {
+        s.tbl[tid] = tb;
+        s.ttb[tid] = tt;
+    }
+    if (tid == 0) {
+        s.pos = P[0];
+        s.sh1 = P[1];
+        s.sh2 = P[2];
+        s.mask = mask ? mask : P[3];
+    }
+    __syncthreads();
+}
+
 // Generate n outputs of the stream held in s.ring, in rounds of 256:
 // output k: x_{k+351} = rec(x_k, x_{k+1}, x_{k+pos}); out_k = temper(x_{k+351}, x_{k+pos-1}).
 // Within a round every read index is < base+351 <= every write index, so
@@ -123,7 +160,11 @@ __device__ __forceinline__ void box_muller(float x, float y, float& z1, float& z
 // shared loads and the normals go out as one 64-bit store to nz[k], nz[k+1]
 // (the same values as mtgp_generate followed by box_muller on nz[2q], nz[2q+1]).
 // Words k >= nbm (k < n) go to emit(k, word).  Ends with a barrier.
-template <class Emit>
+// RAW: the first nbm words are stored as they are (floats in [1,2)) and the
+// caller applies box_muller to each pair (nz[2q], nz[2q+1]) when it reads
+// them; the same normals, with the Box-Muller chains taken out of the
+// barrier-separated rounds.
+template <bool RAW = false, class Emit>
 __device__ __forceinline__ void mtgp_generate_bm(MtgpSmem& s, int n, int nbm, float* __restrict__ nz, Emit emit)
 {
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -133,6 +174,10 @@ __device__ __forceinline__ void mtgp_generate_bm(MtgpSmem& s, int n, int nbm, fl
     for (int base = 0; base < n; base += kMtgpLanes) {
         for (int l2 = tid; l2 < kMtgpLanes / 2; l2 += nt) {
             const int k = base + 2 * l2;  // even
+            // past the requested words (the last round): nothing this pair
+            // writes is read again -- the state kept is x_n .. x_{n+350}, the
+            // last of which pair (n-2, n-1) writes
+            if (k >= n) continue;
             const uint2 x01 = ld2(k), x23 = ld2(k + 2);
             uint32_t t0, y0, y1;
             if ((pos & 1u) == 0) {
@@ -166,9 +211,13 @@ __device__ __forceinline__ void mtgp_generate_bm(MtgpSmem& s, int n, int nbm, fl
             const uint32_t o0 = (r0 >> 9) ^ s.ttb[ta & 0x0f];
             const uint32_t o1 = (r1 >> 9) ^ s.ttb[tb & 0x0f];
             if (k < nbm) {
-                float z1, z2;
-                box_muller(__uint_as_float(o0), __uint_as_float(o1), z1, z2);
-                *reinterpret_cast<float2*>(nz + k) = make_float2(z1, z2);
+                if constexpr (RAW) {
+                    *reinterpret_cast<uint2*>(nz + k) = make_uint2(o0, o1);
+                } else {
+                    float z1, z2;
+                    box_muller(__uint_as_float(o0), __uint_as_float(o1), z1, z2);
+                    *reinterpret_cast<float2*>(nz + k) = make_float2(z1, z2);
+                }
             } else {
                 if (k < n) emit(k, o0);
                 if (k + 1 < n) emit(k + 1, o1);
@@ -309,6 +358,100 @@ __device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], f
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// The same descending sort when ties are rare (small-state models, whose keys
+// are continuous functions of freshly perturbed states).  With distinct keys
+// the sorted permutation is unique, so any correct sort gives the network's
+// result; this one runs the network on the keys alone (a shuffle and a min /
+// max per element and stage instead of two shuffles and four selects), then
+// recovers the permutation: each thread finds the sorted position of each of
+// its keys by a binary search over the sorted keys in shared memory and
+// writes its index there.  If any two keys compare equal (ties, +0 / -0,
+// repeated -inf) or a key is NaN, the whole CTA (every thread takes the same
+// branch) sorts the original (key, index) pairs with bitonic_sort_desc, which
+// keeps the reference network's tie order.  Same contract as
+// bitonic_sort_desc for a CTA owning one sub-filter (tid = threadIdx.x);
+// returns true when the CTA fell back to the full network.
+// ---------------------------------------------------------------------------
+template <int M, int E>
+__device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si)
+{
+    const int tid = threadIdx.x;
+    float v[E];
+    bool nan = false;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        v[e] = k[e];
+        nan |= k[e] != k[e];
+    }
+#pragma unroll
+    for (int size = 2; size <= M; size <<= 1) {
+#pragma unroll
+        for (int stride = size / 2; stride > 0; stride >>= 1) {
+            if (stride < E) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if ((e & stride) == 0) {
+                        // descending where (p & size) == 0: the larger key first
+                        const bool asc = ((E * tid + e) & size) != 0;
+                        const float hi = fmaxf(v[e], v[e + stride]), lo = fminf(v[e], v[e + stride]);
+                        v[e] = asc ? lo : hi;
+                        v[e + stride] = asc ? hi : lo;
+                    }
+                }
+            } else if (stride < 32 * E) {
+                const int lm = stride / E;
+                // p & size and the thread's side of the pair are the same for all e here
+                const bool keep_max = (((E * tid) & size) != 0) == ((tid & lm) != 0);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float o = __shfl_xor_sync(kFull, v[e], lm);
+                    v[e] = keep_max ? fmaxf(v[e], o) : fminf(v[e], o);
+                }
+            } else {
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+                __syncthreads();
+                const bool keep_max = (((E * tid) & size) != 0) == (((E * tid) & stride) != 0);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float o = sk[(E * tid + e) ^ stride];
+                    v[e] = keep_max ? fmaxf(v[e], o) : fminf(v[e], o);
+                }
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+    __syncthreads();
+    bool tie = nan;
+#pragma unroll
+    for (int e = 0; e + 1 < E; ++e) tie |= v[e] == v[e + 1];
+    if (E * tid + E < M) tie |= v[E - 1] == sk[E * tid + E];
+    if (__syncthreads_or(tie)) {
+        bitonic_sort_desc<M, E>(k, ix, sk, si);
+        return true;
+    }
+    // sorted position of each original key = the number of keys above it
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        int pos = 0;
+#pragma unroll
+        for (int step = M / 2; step > 0; step >>= 1)
+            if (sk[pos + step - 1] > k[e]) pos += step;
+        si[pos] = E * tid + e;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        k[e] = v[e];
+        ix[e] = si[E * tid + e];
+    }
+    return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -762,27 +905,31 @@ struct Unicycle {
         float lx[8], ly[8], rm[8], cb[8], sb[8];
     };
     // Exact-arc velocity model: x' = x + A cos th - B sin th, y' = y + A sin th + B cos th
-    // with A = v sin(w dt)/w, B = v (1 - cos(w dt))/w (straight-line limit as w -> 0).
+    // with A = v sin(w dt)/w, B = v (1 - cos(w dt))/w (straight-line limit as w -> 0),
+    // evaluated in FP32 through the half angle h = w dt / 2: sin(w dt) = 2 sin h cos h,
+    // 1 - cos(w dt) = 2 sin^2 h (no cancellation for small w dt).
     // lane 8: motion constants; lanes 0..7: landmark `lane`
     __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
     {
         const pf_unicycle_params& p = mp.uni;
         const int L = p.num_landmarks < 1 ? 1 : (p.num_landmarks > 8 ? 8 : p.num_landmarks);
         if (lane == 8) {
-            const double dt = in.dt > 0.0f ? in.dt : p.dt;
-            const double v = in.control[0], w = in.control[1];
-            const double wd = w * dt;
-            double A, B;
-            if (fabs(wd) < 1e-4) {
-                A = v * dt * (1.0 - wd * wd / 6.0);
-                B = v * dt * (wd / 2.0);
+            const float dt = in.dt > 0.0f ? in.dt : p.dt;
+            const float v = in.control[0], w = in.control[1];
+            const float wd = w * dt;
+            float A, B;
+            if (fabsf(wd) < 1e-4f) {
+                A = v * dt * (1.0f - wd * wd / 6.0f);
+                B = v * dt * (wd * 0.5f);
             } else {
-                A = v * sin(wd) / w;
-                B = v * (1.0 - cos(wd)) / w;
+                float sh, ch;
+                sincosf(0.5f * wd, &sh, &ch);
+                A = v * (2.0f * sh * ch) / w;
+                B = v * (2.0f * sh * sh) / w;
             }
-            c.A = (float)A;
-            c.B = (float)B;
-            c.wd = (float)wd;
+            c.A = A;
+            c.B = B;
+            c.wd = wd;
             c.sq0 = p.sigma_q[0];
             c.sq1 = p.sigma_q[1];
             c.sq2 = p.sigma_q[2];
@@ -794,9 +941,7 @@ struct Unicycle {
             c.lx[j] = p.landmarks[j][0];
             c.ly[j] = p.landmarks[j][1];
             c.rm[j] = j < L ? in.meas[j] : 0.0f;
-            const double bj = j < L ? (double)in.meas[L + j] : 0.0;
-            c.cb[j] = (float)cos(bj);
-            c.sb[j] = (float)sin(bj);
+            sincosf(j < L ? in.meas[L + j] : 0.0f, &c.sb[j], &c.cb[j]);
         }
     }
     __device__ static __forceinline__ float step(const Consts& c, float* s, const float* n, float* sn,
@@ -897,8 +1042,7 @@ struct DhArm {
             const int i = lane;
             c.a[i] = p.a[i];
             c.d[i] = p.d[i];
-            c.ca[i] = (float)cos((double)p.alpha[i]);
-            c.sa[i] = (float)sin((double)p.alpha[i]);
+            sincosf(p.alpha[i], &c.sa[i], &c.ca[i]);
             c.z[i] = in.meas[i];
         }
     }
@@ -1109,7 +1253,8 @@ struct Beacon {
             c.nw = p.noise[1];
             c.ng = p.noise[2];
             c.h = (float)(0.5 / ((double)p.sigma_range * (double)p.sigma_range));
-            c.lnorm = (float)(log(1e5) - (double)(L / 2) * log(2.0 * 3.14159265358979323846));
+            // log(1e5) - (L/2) log(2 pi), the logarithms as FP64 constants
+            c.lnorm = (float)(11.512925464970229 - (double)(L / 2) * 1.8378770664093453);
             c.L = L;
         } else if (lane < 16) {
             const int j = lane;
@@ -1232,6 +1377,30 @@ __device__ __forceinline__ void model_step_batch(const typename Mdl::Consts& c, 
             for (int v = 0; v < Mdl::K; ++v) n[v] = noise(e, v);
             ll[e] = Mdl::step(c, s[e], n, sn[e], cs[e]);
         }
+    }
+}
+
+// Models whose weights are continuous functions of a state that every step
+// perturbs in every variable the weight depends on: two particles share a key
+// only by coincidence, so their sub-filters sort with rank_sort_desc.  The
+// DH arm is not one (a resampled duplicate's joint angles advance with the
+// velocity of the previous step, before its noise, so duplicates keep equal
+// keys), nor, conservatively, are the reference's arms.
+template <class Mdl>
+struct RareTies : std::false_type {};
+template <>
+struct RareTies<Unicycle> : std::true_type {};
+template <>
+struct RareTies<Beacon> : std::true_type {};
+
+// The sampling kernels' sort of one sub-filter per CTA (see rank_sort_desc).
+template <class Mdl, int M, int E>
+__device__ __forceinline__ void sort_subfilter(float (&k)[E], int (&ix)[E], float* sk, int* si)
+{
+    if constexpr (RareTies<Mdl>::value) {
+        rank_sort_desc<M, E>(k, ix, sk, si);
+    } else {
+        bitonic_sort_desc<M, E>(k, ix, sk, si);
     }
 }
 

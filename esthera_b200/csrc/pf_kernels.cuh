@@ -199,68 +199,112 @@ __device__ __forceinline__ const pf_step_input* input_of(const InputRef& in, int
     return in.base + (int64_t)f * in.filter_stride + step_index(in);
 }
 
-// Shared-memory footprint of k_sample_sort (dynamic part).
+// Whether the sampling kernels leave Box-Muller out of the MTGP32 rounds: for
+// small states with an even number of particles per thread, each thread turns
+// the raw pairs of its own particles (e, e+1) into normals in registers right
+// before the model (independent chains, no barrier between them).
+template <class Mdl, int E>
+constexpr bool raw_normals() { return E % 2 == 0 && Mdl::K * E <= 16; }
+
+// This thread's E x K normals from the raw MTGP32 words in shared memory
+// (raw_normals): pair (v M + E tid + e, +1) -> particles e, e+1 of variable v.
+template <class Mdl, int M, int E>
+__device__ __forceinline__ void normals_from_raw(const float* nz, int tid, float (&z)[E][Mdl::K])
+{
+#pragma unroll
+    for (int v = 0; v < Mdl::K; ++v)
+#pragma unroll
+        for (int e = 0; e < E; e += 2) {
+            const float2 u = *reinterpret_cast<const float2*>(nz + v * M + E * tid + e);
+            box_muller(u.x, u.y, z[e][v], z[e + 1][v]);
+        }
+}
+
+// k_sample_sort's dynamic shared memory: the MTGP32 ring (FR), one region
+// holding in turn the normals, the state stage of the sorted gather and the
+// estimate partials' per-thread sums, then the sort keys + indices.
+template <class Mdl, int M, bool FR>
+constexpr size_t k1_stage_bytes()
+{
+    const size_t nz = FR ? (size_t)(2 * ((Mdl::K * M + 1) / 2)) * 4 : 0;
+    const size_t stage = (size_t)Mdl::S * M * 4;
+    return nz > stage ? nz : stage;
+}
 template <class Mdl, int M, bool FR>
 constexpr size_t k1_smem()
 {
-    size_t s = 0;
-    if (FR) s += sizeof(MtgpSmem);
-    size_t nz = FR ? (size_t)(2 * ((Mdl::K * M + 1) / 2)) * 4 : 0;
-    size_t stage = (size_t)Mdl::S * M * 4;
-    s += nz > stage ? nz : stage;
-    s += (size_t)M * 8;  // sort keys + indices
-    return s;
+    return (FR ? sizeof(MtgpSmem) : 0) + k1_stage_bytes<Mdl, M, FR>() + (size_t)M * 8;
 }
 
 // Estimate partials of one sub-filter from particles in any order:
 // [0] key max, [1] sum w, [2+v] sum w x_v (angles: sum w sin), [2+S+a] sum w cos.
-// One value at a time (few live registers): each thread sums its E particles
-// in order, lanes combine with the xor-shuffle tree, warps in index order.
-// sin/cos of the angular variables are taken from the (already propagated)
-// state, the values the model returned for them.
-template <class Mdl, int E>
-__device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float lmax,
-                                               const float (&okey)[E], const float (&st)[E][Mdl::S], double* red)
+// Each thread sums its E particles in FP64, in order; sn / cs are the sines
+// and cosines of the angular state variables, as the model returned them.
+// The NV x NT per-thread sums then go through shared memory (acc, ACC_BYTES
+// bytes, free for this call; chunks of values when they do not all fit): P
+// consecutive lanes per value (P the largest power of two with NV * P <= NT,
+// at most 32) each add NT / P rows in order, then an xor-shuffle tree over
+// the P lanes.  A fixed order: deterministic for a given (M, E).
+template <class Mdl, int E, int NT, size_t ACC_BYTES>
+__device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float lmax, const float (&okey)[E],
+                                               const float (&st)[E][Mdl::S],
+                                               const float (&sn)[E][Mdl::NA > 0 ? Mdl::NA : 1],
+                                               const float (&cs)[E][Mdl::NA > 0 ? Mdl::NA : 1], double* acc)
 {
     constexpr int S = Mdl::S, NA = Mdl::NA, NV = 1 + S + NA;
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int CH = (int)(ACC_BYTES / (8 * NT)) < NV ? (int)(ACC_BYTES / (8 * NT)) : NV;  // values per chunk
+    static_assert(CH >= 1, "the partials buffer holds at least one row of per-thread sums");
+    constexpr int PR = NT / CH;
+    constexpr int P = PR >= 32 ? 32 : (PR >= 16 ? 16 : (PR >= 8 ? 8 : (PR >= 4 ? 4 : (PR >= 2 ? 2 : 1))));
+    const int tid = threadIdx.x;
     double w[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) w[e] = D.log_weights ? (double)__expf(okey[e] - lmax) : (double)okey[e];
-    __syncthreads();
+    double* out = D.part + (int64_t)b * kPartStride;
 #pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        double a = 0.0;
+    for (int c0 = 0; c0 < NV; c0 += CH) {
+        __syncthreads();  // the buffer (or the previous chunk) is free
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            if (i == 0) {
-                a += w[e];
-            } else if (i <= S) {
-                const int v = i - 1;
-                float x = st[e][v];
-                if (is_angle_var<Mdl>(v)) {
-                    float c;
-                    __sincosf(st[e][v], &x, &c);
+        for (int c = 0; c < CH; ++c) {
+            const int i = c0 + c;
+            if (i < NV) {
+                double a = 0.0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    if (i == 0) {
+                        a += w[e];
+                    } else if (i <= S) {
+                        const int v = i - 1;
+                        float x = st[e][v];
+                        if constexpr (NA > 0) {
+                            if (is_angle_var<Mdl>(v)) {
+                                int ai = 0;
+#pragma unroll
+                                for (int q = 0; q < NA; ++q)
+                                    if (Mdl::angle_var(q) == v) ai = q;
+                                x = sn[e][ai];
+                            }
+                        }
+                        a += w[e] * (double)x;
+                    } else {
+                        a += w[e] * (double)cs[e][i - 1 - S];
+                    }
                 }
-                a += w[e] * (double)x;
-            } else {
-                float sn, cs;
-                __sincosf(st[e][Mdl::angle_var(i - 1 - S)], &sn, &cs);
-                a += w[e] * (double)cs;
+                acc[c * NT + tid] = a;
             }
         }
+        __syncthreads();
+        const int c = tid / P, j = tid % P;
+        double a = 0.0;
+        if (c < CH && c0 + c < NV) {
+#pragma unroll 4
+            for (int t = j; t < NT; t += P) a += acc[c * NT + t];
+        }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
-        if (lane == 0) red[wp * NV + i] = a;
+        for (int o = P / 2; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
+        if (j == 0 && c < CH && c0 + c < NV) out[1 + c0 + c] = a;
     }
-    __syncthreads();
-    double* out = D.part + (int64_t)b * kPartStride;
-    if (threadIdx.x < NV) {
-        double sum = red[threadIdx.x];
-        for (int q = 1; q < nw; ++q) sum += red[q * NV + threadIdx.x];
-        out[1 + threadIdx.x] = sum;
-    }
-    if (threadIdx.x == 0) out[0] = (double)lmax;
+    if (tid == 0) out[0] = (double)lmax;
 }
 
 // ---------------------------------------------------------------------------
@@ -275,7 +319,6 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     constexpr int NANG = NA > 0 ? NA : 1;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ typename Mdl::Consts cst;
-    __shared__ double red[(NT / 32) * (1 + S + NANG)];
     __shared__ float s_lmax;
     __shared__ FilterDesc sdesc;
     int f, b;
@@ -292,23 +335,25 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         ms = reinterpret_cast<MtgpSmem*>(p);
         p += sizeof(MtgpSmem);
     }
-    float* nz = reinterpret_cast<float*>(p);     // normals (FR), later the state stage
+    float* nz = reinterpret_cast<float*>(p);     // normals (FR), later the state stage, then the partials
     float* stage = nz;
-    {
-        size_t a = FR ? (size_t)(2 * ((K * M + 1) / 2)) * 4 : 0, c = (size_t)S * M * 4;
-        p += a > c ? a : c;
-    }
+    p += k1_stage_bytes<Mdl, M, FR>();
     float* sk = reinterpret_cast<float*>(p);
     int* si = reinterpret_cast<int*>(p + (size_t)M * 4);
 
-    if (tid < 32) Mdl::prepare(cst, *input_of(in, f), D.mp, tid);
     if constexpr (FR) {
         uint32_t* gst = D.mtgp + (int64_t)b * kMtgpN;
-        mtgp_load(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, true);
+        // the step's model constants (one warp) while the stream words are in flight
+        mtgp_load_overlap<NT>(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, [&] {
+            if (tid < 32) Mdl::prepare(cst, *input_of(in, f), D.mp, tid);
+        });
         const int nbm = D.nbm;
         float* ru = D.ru + (int64_t)b * D.ru_stride;
-        mtgp_generate_bm(*ms, D.draws, nbm, nz, [&](int k, uint32_t o) { ru[k - nbm] = __uint_as_float(o); });
+        mtgp_generate_bm<raw_normals<Mdl, E>()>(*ms, D.draws, nbm, nz,
+                                                [&](int k, uint32_t o) { ru[k - nbm] = __uint_as_float(o); });
         mtgp_store(*ms, gst, D.draws);
+    } else {
+        if (tid < 32) Mdl::prepare(cst, *input_of(in, f), D.mp, tid);
     }
     __syncthreads();
 
@@ -323,9 +368,15 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     float okey[E], sn[E][NANG], cs[E][NANG];
     {
         float ll[E];
-        model_step_batch<Mdl, E>(
-            cst, st,
-            [&](int e, int v) { return FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e]; }, sn, cs, ll);
+        if constexpr (FR && raw_normals<Mdl, E>()) {
+            float z[E][K];
+            normals_from_raw<Mdl, M, E>(nz, tid, z);
+            model_step_batch<Mdl, E>(cst, st, [&](int e, int v) { return z[e][v]; }, sn, cs, ll);
+        } else {
+            model_step_batch<Mdl, E>(
+                cst, st,
+                [&](int e, int v) { return FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e]; }, sn, cs, ll);
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) okey[e] = D.log_weights ? ll[e] : __expf(ll[e]);
     }
@@ -345,7 +396,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         k[e] = okey[e];
         ix[e] = E * tid + e;
     }
-    bitonic_sort_desc<M, E>(k, ix, sk, si);
+    sort_subfilter<Mdl, M, E>(k, ix, sk, si);
     stv<E>(D.tkey + base, k);
     __syncthreads();  // normals consumed, sort buffers free: stage the state
 #pragma unroll
@@ -364,7 +415,8 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(D.tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
+    write_partials<Mdl, E, NT, k1_stage_bytes<Mdl, M, FR>()>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn,
+                                                              cs, reinterpret_cast<double*>(stage));
 }
 
 // ---------------------------------------------------------------------------
@@ -422,7 +474,6 @@ __global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restri
     constexpr int NT = M / E, S = Mdl::S, NA = Mdl::NA;
     constexpr int NANG = NA > 0 ? NA : 1;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double red[(NT / 32) * (1 + S + NANG)];
     __shared__ float s_lmax;
     __shared__ FilterDesc sdesc;
     int f, b;
@@ -472,7 +523,8 @@ __global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restri
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(D.tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
+    write_partials<Mdl, E, NT, (size_t)S * M * 4>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn, cs,
+                                                   reinterpret_cast<double*>(stage));
 }
 
 // ---------------------------------------------------------------------------
@@ -1073,8 +1125,8 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
 // ---------------------------------------------------------------------------
 // Kernel-level test entry points (one CTA per sub-filter).
 // ---------------------------------------------------------------------------
-template <int M, int E>
-__global__ void __launch_bounds__(M / E) k_test_sort(float* keys, int32_t* idx)
+template <int M, int E, bool RANK>
+__global__ void __launch_bounds__(M / E) k_test_sort(float* keys, int32_t* idx, int32_t* fallbacks)
 {
     __shared__ float sk[M];
     __shared__ int si[M];
@@ -1086,7 +1138,12 @@ __global__ void __launch_bounds__(M / E) k_test_sort(float* keys, int32_t* idx)
         k[e] = keys[base + e];
         ix[e] = E * threadIdx.x + e;
     }
-    bitonic_sort_desc<M, E>(k, ix, sk, si);
+    if constexpr (RANK) {
+        const bool fell_back = rank_sort_desc<M, E>(k, ix, sk, si);
+        if (fell_back && threadIdx.x == 0 && fallbacks) atomicAdd(fallbacks, 1);
+    } else {
+        bitonic_sort_desc<M, E>(k, ix, sk, si);
+    }
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         keys[base + e] = k[e];

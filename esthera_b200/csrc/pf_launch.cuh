@@ -65,7 +65,8 @@ struct Launch {
 // Members are defined in pf_launch_impl.cuh and instantiated by the pf_inst_*.cu files.
 
 // Model-independent launchers (pf_common.cu).
-cudaError_t launch_test_sort(int M, int E, int nsub, float* keys, int32_t* idx, cudaStream_t st);
+cudaError_t launch_test_sort(int M, int E, int nsub, float* keys, int32_t* idx, int rank, int32_t* fallbacks,
+                             cudaStream_t st);
 cudaError_t launch_test_resample(int res, int M, int E, int nsub, const float* w, const float* u, int32_t* sel,
                                  float* prob, uint32_t* alias, cudaStream_t st);
 cudaError_t launch_mtgp_blocks(int G, uint32_t* states, uint32_t* out, int64_t size, uint32_t mask, int float_out,

@@ -39,7 +39,6 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     constexpr int NANG = NA > 0 ? NA : 1;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ typename Mdl::Consts cst;
-    __shared__ double red[(NT / 32) * (1 + S + NANG)];
     __shared__ double dred[33];
     __shared__ int ired[34];
     __shared__ float s_lmax;
@@ -95,17 +94,15 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     p += sizeof(MtgpSmem);
     float* nz = reinterpret_cast<float*>(p);
     float* stage = nz;
-    {
-        const size_t a = (size_t)(2 * ((K * M + 1) / 2)) * 4, c = (size_t)S * M * 4;
-        p += a > c ? a : c;
-    }
+    p += k1_stage_bytes<Mdl, M, true>();
     float* sk = reinterpret_cast<float*>(p);
     int* si = reinterpret_cast<int*>(p + (size_t)M * 4);
     {
         uint32_t* gst = D.mtgp + (int64_t)b * kMtgpN;
         mtgp_load(*ms, gst, (D.stream_base + b) % kMtgpSets, D.mask, true);
         const int nbm = D.nbm;
-        mtgp_generate_bm(*ms, D.draws, nbm, nz, [&](int k, uint32_t o) { ru[k - nbm] = __uint_as_float(o); });
+        mtgp_generate_bm<raw_normals<Mdl, E>()>(*ms, D.draws, nbm, nz,
+                                                [&](int k, uint32_t o) { ru[k - nbm] = __uint_as_float(o); });
         mtgp_store(*ms, gst, D.draws);
     }
     __syncthreads();
@@ -114,8 +111,14 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     float okey[E], sn[E][NANG], cs[E][NANG];
     {
         float ll[E];
-        model_step_batch<Mdl, E>(
-            cst, st, [&](int e, int v) { return nz[v * M + E * tid + e]; }, sn, cs, ll);
+        if constexpr (raw_normals<Mdl, E>()) {
+            float z[E][K];
+            normals_from_raw<Mdl, M, E>(nz, tid, z);
+            model_step_batch<Mdl, E>(cst, st, [&](int e, int v) { return z[e][v]; }, sn, cs, ll);
+        } else {
+            model_step_batch<Mdl, E>(
+                cst, st, [&](int e, int v) { return nz[v * M + E * tid + e]; }, sn, cs, ll);
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) okey[e] = D.log_weights ? ll[e] : __expf(ll[e]);
     }
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         k[e] = okey[e];
         ix[e] = E * tid + e;
     }
-    bitonic_sort_desc<M, E>(k, ix, sk, si);
+    sort_subfilter<Mdl, M, E>(k, ix, sk, si);
     stv<E>(cur_key + base, k);
     __syncthreads();  // normals consumed, sort buffers free: stage the state
 #pragma unroll
@@ -156,7 +159,8 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(cur_tmp + v * T + base, o);
     }
-    write_partials<Mdl, E>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, red);
+    write_partials<Mdl, E, NT, k1_stage_bytes<Mdl, M, true>()>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn,
+                                                                cs, reinterpret_cast<double*>(stage));
 
     // ---- E (warp 0 wrote the partials)
     if (tid < 32) estimate_last_done<S>(D, X, b, in, step_ctr, tid);

@@ -465,6 +465,13 @@ pf_status pfk_boxmuller(float* data, int64_t n);
 /* nsub independent descending bitonic sorts of m keys; idx receives the permutation
  * (block_sort + bitonic_sort, pf_generic_soa.cu:289-323, bitonic-sort.cu:11-61). */
 pf_status pfk_bitonic_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt);
+/* The same sort as the sampling kernels run it for models whose keys rarely
+ * tie (unicycle, beacon): the network on the keys alone, the permutation
+ * recovered by rank; a sub-filter with equal keys (ties, +0/-0, repeated
+ * -inf) or a NaN key falls back to the (key, index) network, so the result
+ * equals pfk_bitonic_sort's in every case.  *fallbacks receives how many
+ * sub-filters fell back.  (No counterpart in the reference.) */
+pf_status pfk_rank_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt, int32_t* fallbacks);
 /* nsub sub-filters of m weights (linear FP32, slot order) -> sel[nsub*m].
  * u: REFERENCE: m raw uniforms in [1,2) per sub-filter; SYSTEMATIC: 1 value in [0,1);
  * VOSE: 2m values in [0,1) (x, y pairs).  ppt: particles per thread (scan grouping). */

@@ -52,6 +52,35 @@ def test_sort_equals_reference_kernel(gpu, O, m):
 
 
 @pytest.mark.parametrize("m", [32, 64, 128, 256, 512, 1024])
+def test_rank_sort_equals_reference_kernel(gpu, m):
+    """The sampling kernels' sort for small-state models (keys-only network +
+    rank, falling back to the full network on ties) against the reference's
+    block_sort: distinct keys (no fallback), and sub-filters with ties, -inf,
+    +0/-0 and NaN (every one of them falls back)."""
+    E = gpu
+    rng = np.random.default_rng(300 + m)
+    nsub = 8
+    keys = ((rng.permutation(nsub * m) - 0.5 * nsub * m) * 0.013).astype(np.float32)  # distinct
+    b = keys.reshape(nsub, m)
+    b[1, 5] = b[1, 9]                     # a tie
+    b[2, ::3] = -np.inf                   # repeated -inf
+    b[3, 0], b[3, 1] = 0.0, -0.0          # +0 / -0
+    b[4, 7] = np.nan                      # NaN
+    b[5, :] = np.round(b[5, :])           # many ties
+    rk, rp = R.block_sort(keys, m)
+    for ppt in PPT[m]:
+        k, p, fb = E.rank_sort(keys, m, ppt)
+        assert fb == 5, (ppt, fb)
+        assert np.array_equal(k.view(np.uint32), rk.view(np.uint32)) and np.array_equal(p, rp), ppt
+    # all distinct: no sub-filter falls back
+    d = (rng.permutation(nsub * m).astype(np.float32) - 7.5) * 0.37
+    rk, rp = R.block_sort(d, m)
+    for ppt in PPT[m]:
+        k, p, fb = E.rank_sort(d, m, ppt)
+        assert fb == 0 and np.array_equal(k, rk) and np.array_equal(p, rp), ppt
+
+
+@pytest.mark.parametrize("m", [32, 64, 128, 256, 512, 1024])
 def test_multinomial_equals_reference_kernel(gpu, O, m):
     E = gpu
     rng = np.random.default_rng(200 + m)
