@@ -471,10 +471,16 @@ __device__ __forceinline__ float block_max(float v, float* red)
 
 // Canonical FP64 inclusive scan (the oracle's orc_scan_f64): each thread sums
 // its E weights sequentially, lanes combine with a Kogge-Stone scan, warp
-// totals with a second Kogge-Stone scan; cum[] receives M inclusive sums.
-// Returns the total.  red needs 32 doubles.
+// totals with a second Kogge-Stone scan; cum[e] receives the inclusive sum
+// through particle E*tid + e (kept in registers).  *prev receives the
+// inclusive sum through particle E*tid - 1 as the previous thread computed it
+// (-inf for thread 0).  Returns the total.  red needs 2 * 32 doubles; two
+// barriers: every warp forms the prefix of the warp totals itself (the same
+// additions in the same order as one warp scanning them), and the last
+// thread of each warp publishes its last sum for the first thread of the
+// next.
 template <int M, int E>
-__device__ __forceinline__ double scan_f64(const float (&w)[E], double* cum, double* red)
+__device__ __forceinline__ double scan_f64(const float (&w)[E], double (&cum)[E], double* red, double* prev)
 {
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     constexpr int NW = (M / E + 31) / 32;
@@ -489,30 +495,29 @@ __device__ __forceinline__ double scan_f64(const float (&w)[E], double* cum, dou
     }
     double ex = __shfl_up_sync(kFull, inc, 1);
     if (lane == 0) ex = 0.0;
-    __syncthreads();
     if (lane == 31) red[wp] = inc;
     __syncthreads();
-    if (wp == 0) {
-        double v = lane < NW ? red[lane] : 0.0;
+    double v = lane < NW ? red[lane] : 0.0;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const double o = __shfl_up_sync(kFull, v, d);
-            if (lane >= d) v = v + o;
-        }
-        __syncwarp();
-        if (lane < NW) red[lane] = v;  // inclusive warp prefix
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(kFull, v, d);
+        if (lane >= d) v = v + o;
     }
-    __syncthreads();
-    const double base = (wp == 0 ? 0.0 : red[wp - 1]) + ex;
+    const double wpre = __shfl_sync(kFull, v, wp > 0 ? wp - 1 : 0);  // inclusive prefix of the warps before
+    const double base = (wp == 0 ? 0.0 : wpre) + ex;
     double c = base + (double)w[0];
-    cum[E * tid] = c;
+    cum[0] = c;
 #pragma unroll
     for (int e = 1; e < E; ++e) {
         c = c + (double)w[e];
-        cum[E * tid + e] = c;
+        cum[e] = c;
     }
+    double p = __shfl_up_sync(kFull, cum[E - 1], 1);
+    if (lane == 31) red[32 + wp] = cum[E - 1];
     __syncthreads();
-    return cum[M - 1];
+    if (lane == 0) p = wp == 0 ? -INFINITY : red[32 + wp - 1];
+    *prev = p;
+    return red[32 + NW - 1];
 }
 
 // Number of cum[] entries <= x (upper bound), clamped to M-1.
@@ -531,19 +536,19 @@ __device__ __forceinline__ int upper_count(const double* cum, double x)
     return lo < M ? lo : M - 1;
 }
 
-// Systematic selection from the inclusive sums cum[0..M) by interval
-// boundaries: input j is selected by the outputs i with
-// cum[j-1] <= pos(i) < cum[j], pos(i) = (u0 + i) * step (cum[-1] = -inf; the
-// last input also takes every output with pos(i) >= cum[M-1]).  Each thread
-// finds, for its E inputs j = E*tid+e, the first output at or above cum[j-1]
-// (an estimate from t / step, corrected with the exact pos(i) comparisons),
-// writes its inputs' runs of outputs to sidx[0..M), and reads back its own E
-// outputs.  pos(i) and the comparisons are those of upper_count(cum, pos(i)),
-// so every output selects the same input (pos is non-decreasing in i).
-// Synchronises the CTA.
+// Systematic selection from the inclusive sums (scan_f64: this thread's cum[e]
+// and the previous thread's last sum `prev`) by interval boundaries: input j
+// is selected by the outputs i with cum[j-1] <= pos(i) < cum[j],
+// pos(i) = (u0 + i) * step (cum[-1] = -inf; the last input also takes every
+// output with pos(i) >= cum[M-1]).  Each thread finds, for its E inputs
+// j = E*tid+e, the first output at or above cum[j-1] (an estimate from t /
+// step, corrected with the exact pos(i) comparisons), writes its inputs' runs
+// of outputs to sidx[0..M), and reads back its own E outputs.  pos(i) and the
+// comparisons are those of upper_count(cum, pos(i)), so every output selects
+// the same input (pos is non-decreasing in i).  Synchronises the CTA.
 template <int M, int E>
-__device__ __forceinline__ void systematic_select(const double* cum, float u0f, double step, int* sidx,
-                                                  int (&sel)[E])
+__device__ __forceinline__ void systematic_select(const double (&cum)[E], double prev, float u0f, double step,
+                                                  int* sidx, int (&sel)[E])
 {
     const int tid = threadIdx.x;
     const double u0 = (double)u0f;
@@ -557,11 +562,11 @@ __device__ __forceinline__ void systematic_select(const double* cum, float u0f, 
         return i;
     };
     const int j0 = E * tid;
-    int lo = j0 == 0 ? 0 : first_at_or_above(cum[j0 - 1]);
+    int lo = j0 == 0 ? 0 : first_at_or_above(prev);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int j = j0 + e;
-        const int hi = j == M - 1 ? M : first_at_or_above(cum[j]);
+        const int hi = j == M - 1 ? M : first_at_or_above(cum[e]);
         for (int i = lo; i < hi; ++i) sidx[i] = j;
         lo = hi > lo ? hi : lo;
     }

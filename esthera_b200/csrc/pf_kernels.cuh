@@ -792,7 +792,7 @@ template <int S, int M, int E, int RES>
 constexpr size_t k2_smem()
 {
     size_t s = (size_t)M * 4 + (size_t)S * M * 4;  // keys + state tile
-    if (RES == PF_RESAMPLE_SYSTEMATIC) s += (size_t)M * 8;
+    if (RES == PF_RESAMPLE_SYSTEMATIC) s += 0;       // the scan stays in registers, the runs reuse the keys
     else if (RES == PF_RESAMPLE_REFERENCE) s += (size_t)M * 4;
     else s += (size_t)M * 16;  // prob, alias, work list, scratch
     return s;
@@ -998,15 +998,31 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
             }
         }
     }
-    __syncthreads();
+    // this thread's own slots (copied, or patched by this thread) are readable
+    // already; the barrier orders every slot's patch before the reads below
     float w[E];
+    bool nan = false;
 #pragma unroll
-    for (int e = 0; e < E; ++e) w[e] = kb[E * tid + e];
+    for (int e = 0; e < E; ++e) {
+        w[e] = kb[E * tid + e];
+        nan |= w[e] != w[e];
+    }
+    const bool any_nan = __syncthreads_or(nan);
     if (D.log_weights) {
-        float mx = w[0];
+        // the keys are sorted per sub-filter, so their maximum is the head or one
+        // of the weakest slots an exchange may have replaced (the same value as
+        // the CTA-wide maximum); a NaN key breaks the order: then the CTA-wide one
+        const int nxc = exchange_count(D);
+        float mx;
+        if (!any_nan && nxc <= 32 && nxc < M) {
+            mx = kb[0];
+            for (int x = 0; x < nxc; ++x) mx = fmaxf(mx, kb[M - 1 - x]);
+        } else {
+            mx = w[0];
 #pragma unroll
-        for (int e = 1; e < E; ++e) mx = fmaxf(mx, w[e]);
-        mx = block_max(mx, reinterpret_cast<float*>(ired));
+            for (int e = 1; e < E; ++e) mx = fmaxf(mx, w[e]);
+            mx = block_max(mx, reinterpret_cast<float*>(ired));
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) w[e] = pf_expneg(w[e] - mx);
     }
@@ -1041,10 +1057,10 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
         if (!(t2 > 0.0) || t1 * t1 >= (double)D.ess_frac * (double)M * t2) return PF_RS_KEPT;
     }
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
-        double* cum = reinterpret_cast<double*>(scratch);
-        const double tot = scan_f64<M, E>(w, cum, dred);
+        double cum[E], prev;
+        const double tot = scan_f64<M, E>(w, cum, dred, &prev);
         // the keys were read into w before the scan's barriers: kb holds the output runs
-        systematic_select<M, E>(cum, ur[0] - 1.0f, tot / (double)M, reinterpret_cast<int*>(kb), sel);
+        systematic_select<M, E>(cum, prev, ur[0] - 1.0f, tot / (double)M, reinterpret_cast<int*>(kb), sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(scratch);
 #pragma unroll
@@ -1075,7 +1091,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
                                                              int32_t* step_ctr, int virt)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double dred[33];
+    __shared__ double dred[64];
     __shared__ int ired[34];
     int f, b;
     if (cta_map) {
@@ -1156,7 +1172,7 @@ __global__ void __launch_bounds__(M / E) k_test_resample(const float* w_in, cons
                                                          float* prob_out, uint32_t* alias_out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double dred[33];
+    __shared__ double dred[64];
     __shared__ int ired[34];
     const int b = blockIdx.x, tid = threadIdx.x;
     const int64_t base = (int64_t)b * M + E * tid;
@@ -1165,9 +1181,9 @@ __global__ void __launch_bounds__(M / E) k_test_resample(const float* w_in, cons
     for (int e = 0; e < E; ++e) w[e] = w_in[base + e];
     int sel[E];
     if constexpr (RES == PF_RESAMPLE_SYSTEMATIC) {
-        double* cum = reinterpret_cast<double*>(smem);
-        const double tot = scan_f64<M, E>(w, cum, dred);
-        systematic_select<M, E>(cum, u[b], tot / (double)M, reinterpret_cast<int*>(cum + M), sel);
+        double cum[E], prev;
+        const double tot = scan_f64<M, E>(w, cum, dred, &prev);
+        systematic_select<M, E>(cum, prev, u[b], tot / (double)M, reinterpret_cast<int*>(smem), sel);
     } else if constexpr (RES == PF_RESAMPLE_REFERENCE) {
         float* ex = reinterpret_cast<float*>(smem);
 #pragma unroll

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     constexpr int NANG = NA > 0 ? NA : 1;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ typename Mdl::Consts cst;
-    __shared__ double dred[33];
+    __shared__ double dred[64];
     __shared__ int ired[34];
     __shared__ float s_lmax;
     __shared__ uint64_t mbar;
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(M / E) k_resample_only_cta(const FilterDesc* _
 {
     constexpr int S = Mdl::S;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ double dred[33];
+    __shared__ double dred[64];
     __shared__ int ired[34];
     __shared__ uint64_t mbar;
     __shared__ FilterDesc sdesc;
