@@ -91,6 +91,7 @@ def _declare(L):
         "orc_scan_f64": (C.c_double, [fp, C.c_int, C.c_int, dp]),
         "orc_resample_systematic": (C.c_double, [fp, C.c_int, C.c_int, C.c_float, ip]),
         "orc_vose_build": (None, [fp, C.c_int, fp, up]),
+        "orc_vose_scaled": (None, [fp, C.c_int, fp]),
         "orc_vose_draw": (C.c_uint32, [fp, up, C.c_int, C.c_float, C.c_float]),
         "orc_torus_dims": (None, [C.c_int, ip, ip]),
         "orc_exchange_sources": (None, [C.c_int, C.c_int, C.c_int, C.c_int, fp, ip]),
@@ -215,6 +216,45 @@ def vose_build(w, m):
         prob[b * m:(b + 1) * m] = p
         alias[b * m:(b + 1) * m] = a
     return prob, alias
+
+
+def vose_scaled(w, m):
+    """The alias build's starting probabilities (normalised weights x m), per sub-filter."""
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.zeros(len(w), np.float32)
+    for b in range(len(w) // m):
+        o = np.zeros(m, np.float32)
+        lib().orc_vose_scaled(_f(np.ascontiguousarray(w[b * m:(b + 1) * m])), m, _f(o))
+        out[b * m:(b + 1) * m] = o
+    return out
+
+
+def vose_draws(prob, alias, u2, m):
+    """orc_vose_draw for every particle on the given tables; u2: 2 uniforms in [0,1) per particle."""
+    prob = np.ascontiguousarray(prob, np.float32)
+    alias = np.ascontiguousarray(alias, np.uint32)
+    u2 = np.ascontiguousarray(u2, np.float32)
+    n = len(prob)
+    sel = np.zeros(n, np.int32)
+    for b in range(n // m):
+        pb = np.ascontiguousarray(prob[b * m:(b + 1) * m])
+        ab = np.ascontiguousarray(alias[b * m:(b + 1) * m])
+        for i in range(m):
+            k = b * m + i
+            sel[k] = lib().orc_vose_draw(_f(pb), _u(ab), m, C.c_float(float(u2[2 * k])), C.c_float(float(u2[2 * k + 1])))
+    return sel
+
+
+def implied_selection(prob, alias, m):
+    """Per slot, the probability that one alias draw selects it: column c uniform,
+    c itself with probability clamp(prob[c], 0, 1), alias[c] otherwise (FP64)."""
+    prob = np.asarray(prob, np.float64).reshape(-1, m)
+    alias = np.asarray(alias, np.int64).reshape(-1, m)
+    keep = np.clip(prob, 0.0, 1.0)
+    out = keep.copy()
+    for b in range(prob.shape[0]):
+        np.add.at(out[b], alias[b], 1.0 - keep[b])
+    return (out / m).reshape(-1)
 
 
 def scan_f64(w, m, ept):

@@ -251,6 +251,21 @@ static float sum_reduce4(float* arr, int m)
     return arr[0];
 }
 
+/* resampling_valias normalisation (:262-270) and vose_alias_init's scaling by
+ * m (:117): the alias build's starting probabilities */
+void orc_vose_scaled(const float* w, int m, float* scaled)
+{
+    float scratch[1024];
+    memcpy(scratch, w, sizeof(float) * (size_t)m);
+    float sum = sum_reduce4(scratch, m);
+    for (int i = 0; i < m; ++i) {
+        float p = w[i];
+        if (sum > 0.0f) p = p / sum;
+        else p = 1.0f / (float)m;
+        scaled[i] = p * (float)m;
+    }
+}
+
 /* resampling_valias normalisation (:262-270) + vose_alias_init (:111-195) */
 void orc_vose_build(const float* w, int m, float* prob, uint32_t* alias)
 {

@@ -83,6 +83,9 @@ double orc_resample_systematic(const float* w, int m, int ept, float u0, int32_t
  * (ascending slot index where the reference uses atomic_inc/atomic_dec).
  * Restates sum_reduce4 + vose_alias_init + normalisation of
  * resampling_valias (src/partfilt/opencl/resampling-valias.cl:85-195, 262-270). */
+/* The alias build's starting probabilities p_i m (p_i = w_i / sum_reduce4(w),
+ * or 1/m when the sum is not positive; resampling-valias.cl:117, 262-270). */
+void orc_vose_scaled(const float* w, int m, float* scaled);
 void orc_vose_build(const float* w, int m, float* prob, uint32_t* alias);
 /* One draw (vose_alias_generate_next, resampling-valias.cl:198-202); ux, uy in [0,1). */
 uint32_t orc_vose_draw(const float* prob, const uint32_t* alias, int m, float ux, float uy);

@@ -8,6 +8,7 @@ from pathlib import Path
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "_ref" / "libref_kernels.so"
+VALIAS_PATH = Path(__file__).resolve().parent / "_ref" / "libref_valias.so"
 _lib = None
 
 
@@ -142,3 +143,74 @@ def camarm_sampling(state, normals, controls, meas, dt):
     wt = np.zeros(n, np.float32)
     _check(_clib.ref_camarm_sampling(_f(st), _f(nz), _f(c), _f(z), dt, n, _f(so), _f(wt)), "ref_camarm_sampling")
     return so, wt
+
+
+_valias = None
+
+
+def valias_available():
+    return VALIAS_PATH.exists()
+
+
+def valias(weights, u2, m):
+    """The reference's own Vose resampler (resampling-valias.cl, compiled as CUDA
+    by oracle/build_ref_valias.sh): (scaled starting probabilities, final prob,
+    alias, selection) for nsub = len/m sub-filters; u2 holds 2 uniforms in
+    [0,1) per particle.  The tables' order follows the GPU's atomics."""
+    global _valias
+    if _valias is None:
+        L = C.CDLL(str(VALIAS_PATH))
+        fp, up = C.POINTER(C.c_float), C.POINTER(C.c_uint32)
+        L.ref_valias.argtypes = [fp, fp, C.c_int, C.c_int, fp, fp, up, up]
+        L.ref_valias.restype = C.c_int
+        _valias = L
+    w = np.ascontiguousarray(weights, np.float32)
+    u = np.ascontiguousarray(u2, np.float32)
+    n = len(w)
+    scaled, prob = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    alias, sel = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    up = C.POINTER(C.c_uint32)
+    _check(_valias.ref_valias(_f(w), _f(u), m, n // m, _f(scaled), _f(prob), alias.ctypes.data_as(up),
+                              sel.ctypes.data_as(up)), "ref_valias")
+    return scaled, prob, alias, sel.astype(np.int32)
+
+
+DRIVER_PATH = Path(__file__).resolve().parent / "_ref" / "libref_driver.so"
+_driver = None
+
+
+def driver_available():
+    return DRIVER_PATH.exists()
+
+
+def particle_filter(num_particles, num_blocks, num_transfer, resampling_freq, input_file, seed, out_path):
+    """The reference's own driver loop (pf_generic_soa.cu particle_filter, MTGP32
+    build with DEBUG_ESTIMATE, oracle/build_ref_driver.sh) with its streams
+    seeded from `seed`.  Returns (per-step best-particle errors, best-particle
+    states [x, y, vX, vY, angles...] and weights per step, final "N m t e"
+    mean error) parsed from its output, written to out_path."""
+    global _driver
+    if _driver is None:
+        L = C.CDLL(str(DRIVER_PATH))
+        L.ref_particle_filter.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_char_p, C.c_uint, C.c_char_p]
+        L.ref_particle_filter.restype = C.c_int
+        _driver = L
+    rc = _driver.ref_particle_filter(num_particles, num_blocks, num_transfer, resampling_freq,
+                                     str(input_file).encode(), seed, str(out_path).encode())
+    if rc != 0:
+        raise RuntimeError("reference particle_filter returned %d" % rc)
+    errs, best, w, mean = [], [], [], None
+    for line in Path(out_path).read_text().splitlines():
+        if line.startswith("EST "):
+            head, wt = line[4:].split(" w: ")
+            nums = head.replace("x:", "").replace("y:", "").replace("vX:", "").replace("vY:", "")
+            nums = nums.replace("[", " ").replace("]", " ").replace(",", " ").split()
+            best.append([float(v) for v in nums])
+            w.append(float(wt))
+        elif line.startswith("ACT ") and "| err:" in line:
+            errs.append(float(line.split("| err:")[1]))
+        else:
+            tok = line.split()
+            if len(tok) == 4 and tok[0].isdigit():
+                mean = float(tok[3])
+    return np.array(errs), np.array(best, np.float64), np.array(w, np.float64), mean

@@ -1,10 +1,12 @@
-"""The engine's CUDA sort, multinomial resampling and ring routing -- and the
-CPU oracle -- against the reference's OWN CUDA kernels (block_sort with its
-bitonic network, resampling with prefix_sum + binary_search, exchange_ring from
-pf_generic_soa.cu / bitonic-sort.cu), built from the Esthera tree into
-oracle/_ref/libref_kernels.so by oracle/build_ref_kernels.sh and run on the
-same GPU.  Inputs: seeded random keys with heavy ties, positive weights with
-zeros, MTGP-style uniforms in [1, 2)."""
+"""The engine's CUDA sort, multinomial resampling, ring routing and Vose alias
+build -- and the CPU oracle -- against the reference's OWN kernels: the CUDA
+block_sort with its bitonic network, resampling with prefix_sum +
+binary_search and exchange_ring (pf_generic_soa.cu / bitonic-sort.cu, built
+into oracle/_ref/libref_kernels.so by oracle/build_ref_kernels.sh) and the
+OpenCL Vose resampler (resampling-valias.cl, compiled as CUDA into
+oracle/_ref/libref_valias.so by oracle/build_ref_valias.sh), run on the same
+GPU.  Inputs: seeded random keys with heavy ties, positive weights with zeros,
+MTGP-style uniforms in [1, 2)."""
 import sys
 from pathlib import Path
 
@@ -209,3 +211,38 @@ def test_camarm_model_equals_reference_kernel(gpu, O, ang):
     assert ok.mean() > 0.5
     lr = np.log(wt[ok].astype(np.float64))
     assert np.allclose(ll[ok], lr, rtol=1e-4, atol=5e-3)
+
+
+@pytest.mark.parametrize("m", [32, 64, 128, 256, 512, 1024])
+def test_vose_pinned_to_reference_kernel(gpu, O, m):
+    """The engine's Vose alias build and the oracle's against the reference's own
+    resampling-valias.cl (run on this GPU through oracle/build_ref_valias.sh).
+    The reference fills its work lists with atomics, so its tables' order is
+    the hardware's; compared are the parts that do not depend on it:
+    (1) the normalised, scaled starting probabilities, bit for bit (and the
+    engine's final probabilities of the slots that start small, which the
+    pairing never changes); (2) each slot's selection probability implied by
+    the finished tables, within FP32 rounding; (3) the draw rule on the
+    reference's own tables, bit for bit."""
+    _require(R.valias_available(), "libref_valias.so", "build_ref_valias.sh")
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import make_ref_valias_golden as G
+    E = gpu
+    w, u2 = G.inputs(m, 1900 + m)
+    scaled, rprob, ralias, rsel = R.valias(w, u2, m)
+    # (1)
+    assert np.array_equal(scaled.view(np.uint32), O.vose_scaled(w, m).view(np.uint32))
+    for ppt in PPT[m]:
+        eprob, ealias = E.vose_build(w, m, ppt)
+        small = scaled <= 1.0
+        assert np.array_equal(eprob[small], scaled[small]), ppt
+        # (2)
+        ri = O.implied_selection(rprob, ralias, m)
+        ei = O.implied_selection(eprob, ealias, m)
+        assert np.all(np.abs(ri - ei) <= 1e-6 + 1e-4 * ri), (ppt, np.max(np.abs(ri - ei)))
+    wn = w.reshape(-1, m).astype(np.float64)
+    tot = wn.sum(axis=1, keepdims=True)
+    target = np.where(tot > 0, wn / np.where(tot > 0, tot, 1.0), 1.0 / m).reshape(-1)
+    assert np.all(np.abs(ri - target) <= 1e-6 + 1e-4 * target)
+    # (3)
+    assert np.array_equal(O.vose_draws(rprob, ralias, u2, m), rsel)
