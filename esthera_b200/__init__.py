@@ -118,6 +118,8 @@ def _declare(L):
         "pf_version": (C.c_int32, []),
         "pf_device_count": (C.c_int32, []),
         "pf_model_info": (C.c_int, [C.c_int, ip, ip, ip, ip]),
+        "pf_model_list": (C.c_int32, [P, C.c_int32]),
+        "pf_model_name": (C.c_char_p, [C.c_int32]),
         "pf_config_default": (C.c_int, [C.POINTER(PFConfig)]),
         "pf_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, P, C.c_size_t, C.POINTER(P)]),
         "pf_destroy": (C.c_int, [P]),
@@ -260,6 +262,28 @@ def dharm_params(seed):
     p = DhArmParams()
     check(lib().pf_dharm_default_params(seed, C.byref(p)))
     return p
+
+
+MODEL_USER_BASE = 64  # first id of models added with PF_MODEL (esthera_b200_model.cuh)
+MODEL_LINGAUSS = MODEL_USER_BASE  # the linear-Gaussian example model (csrc/pf_model_lingauss.cu)
+
+
+class LinGaussParams(C.Structure):
+    """Parameters of the linear-Gaussian example model (pf_lingauss_params)."""
+    _fields_ = [("dt", C.c_float), ("sigma_v", C.c_float), ("sigma_z", C.c_float), ("init_state", C.c_float * 2)]
+
+
+def model_list():
+    """Ids of every model compiled into the library (built-in and registered with PF_MODEL)."""
+    n = lib().pf_model_list(None, 0)
+    ids = np.zeros(max(n, 1), np.int32)
+    lib().pf_model_list(ids.ctypes.data_as(C.c_void_p), n)
+    return [int(i) for i in ids[:n]]
+
+
+def model_name(model):
+    r = lib().pf_model_name(model)
+    return None if r is None else r.decode()
 
 
 def refarm_params(dt=1.0):

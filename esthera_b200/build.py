@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # inlines a model or a scan computes bit-identical results (the device code
 # writes its multiply-adds as explicit fmaf where it wants them).
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "--fmad=false",
-              "-I" + str(INCLUDE)] + ARCH
+              "-I" + str(INCLUDE), "-I" + str(CSRC)] + ARCH
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-I" + str(INCLUDE)]
 
 

@@ -77,16 +77,56 @@ pf_status pfhost::require_gpu(int device)
 // model table
 // ---------------------------------------------------------------------------
 
+// The registry: a fixed table filled by the registrations that run when the
+// library is loaded (PF_REGISTER_MODEL / PF_MODEL), read-only afterwards.
+namespace {
+constexpr int kMaxModels = 64;
+struct Registry {
+    std::mutex mu;
+    pfhost::ModelEntry e[kMaxModels];
+    int n = 0;
+};
+Registry& registry()
+{
+    static Registry r;
+    return r;
+}
+}  // namespace
+
+bool pfhost::register_model(const ModelEntry& e)
+{
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (e.id < 0 || r.n >= kMaxModels) return false;
+    for (int i = 0; i < r.n; ++i)
+        if (r.e[i].id == e.id) return false;
+    r.e[r.n++] = e;
+    return true;
+}
+
+const pfhost::ModelEntry* pfhost::find_model(int id)
+{
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    for (int i = 0; i < r.n; ++i)
+        if (r.e[i].id == id) return &r.e[i];
+    return nullptr;
+}
+
+int pfhost::registered_models(int* ids, int cap)
+{
+    Registry& r = registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    for (int i = 0; i < r.n && i < cap; ++i) ids[i] = r.e[i].id;
+    return r.n;
+}
+
 bool pfhost::model_info(int model, ModelInfo* mi)
 {
-    switch (model) {
-    case PF_MODEL_UNICYCLE: *mi = {Unicycle::S, Unicycle::K, 2, 16, sizeof(pf_unicycle_params)}; return true;
-    case PF_MODEL_DHARM: *mi = {DhArm::S, DhArm::K, 0, 6, sizeof(pf_dharm_params)}; return true;
-    case PF_MODEL_REFARM: *mi = {RefArm::S, RefArm::K, 5, 7, sizeof(pf_refarm_params)}; return true;
-    case PF_MODEL_BEACON: *mi = {Beacon::S, Beacon::K, 2, 16, sizeof(pf_beacon_params)}; return true;
-    case PF_MODEL_CAMARM: *mi = {CamArm::S, CamArm::K, 5, 7, sizeof(pf_camarm_params)}; return true;
-    }
-    return false;
+    const ModelEntry* e = find_model(model);
+    if (!e) return false;
+    *mi = e->info;
+    return true;
 }
 
 bool pfhost::dependent_launch_pays(int grid, int M, int E, int S, int device)
@@ -117,43 +157,40 @@ extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, in
 
 const float* pfhost::init_state_of(int model, const ModelParams& mp)
 {
-    switch (model) {
-    case PF_MODEL_UNICYCLE: return mp.uni.init_state;
-    case PF_MODEL_DHARM: return mp.arm.init_state;
-    case PF_MODEL_BEACON: return mp.bcn.init_state;
-    case PF_MODEL_CAMARM: return mp.cam.init_state;
-    default: return mp.ref.init_state;
-    }
+    const ModelEntry* e = find_model(model);
+    return reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(&mp) + (e ? e->init_offset : 0));
 }
-
 
 uint32_t pfhost::angle_mask_of(int model)
 {
-    if (model == PF_MODEL_UNICYCLE || model == PF_MODEL_BEACON) return 0x4u;
-    return model == PF_MODEL_DHARM ? 0x3fu : 0x1fu;
+    const ModelEntry* e = find_model(model);
+    return e ? e->angle_mask : 0u;
 }
 
 int pfhost::angle_count_of(int model)
 {
-    if (model == PF_MODEL_UNICYCLE || model == PF_MODEL_BEACON) return 1;
-    return model == PF_MODEL_DHARM ? 6 : 5;
-}
-
-template <class Mdl>
-static ModelOps ops_of()
-{
-    return {Launch<Mdl>::sample_sort,       Launch<Mdl>::sample_weight,    Launch<Mdl>::block_sort,
-            Launch<Mdl>::exchange_resample, Launch<Mdl>::exchange_inplace, Launch<Mdl>::test_model,
-            Launch<Mdl>::step};
+    const ModelEntry* e = find_model(model);
+    return e ? e->angle_count : 0;
 }
 
 ModelOps pfhost::model_ops(int model)
 {
-    if (model == PF_MODEL_UNICYCLE) return ops_of<Unicycle>();
-    if (model == PF_MODEL_DHARM) return ops_of<DhArm>();
-    if (model == PF_MODEL_BEACON) return ops_of<Beacon>();
-    if (model == PF_MODEL_CAMARM) return ops_of<CamArm>();
-    return ops_of<RefArm>();
+    const ModelEntry* e = find_model(model);
+    return e ? e->ops : ModelOps{};
+}
+
+extern "C" int32_t pf_model_list(int32_t* ids, int32_t cap)
+{
+    std::vector<int> v(kMaxModels);
+    const int n = registered_models(v.data(), kMaxModels);
+    for (int i = 0; i < n && i < cap && ids; ++i) ids[i] = v[i];
+    return n;
+}
+
+extern "C" const char* pf_model_name(int32_t model)
+{
+    const ModelEntry* e = find_model(model);
+    return e ? e->name : nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -295,7 +332,7 @@ extern "C" pf_status pf_config_default(pf_config* c)
     return PF_OK;
 }
 
-static int default_ppt(int M)
+int pfhost::default_ppt(int M)
 {
     if (M <= 32) return 1;
     if (M <= 64) return 2;

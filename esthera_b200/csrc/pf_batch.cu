@@ -199,7 +199,7 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     const int M = cfg->particles_per_subfilter;
     if (M < 32 || M > 1024 || (M & (M - 1)))
         return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
-    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : 2;
+    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M);
     if (!me_supported(M, E)) return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E, M);
     if (cfg->rng != PF_RNG_SUBFILTER) return fail(PF_ERR_UNSUPPORTED, "batched filters use per-sub-filter streams");
     if (cfg->pipeline == PF_PIPELINE_PHASED)

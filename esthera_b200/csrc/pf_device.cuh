@@ -891,18 +891,20 @@ __device__ __forceinline__ unsigned vose_draw(const float* prob, const unsigned*
 // propagate in place, return the FP32 log-likelihood, and sin/cos of the
 // angular variables of the new state).
 // ---------------------------------------------------------------------------
+constexpr int kMaxModelParamBytes = 256;  // a registered model's parameter struct fits here
 union ModelParams {
     pf_unicycle_params uni;
     pf_dharm_params arm;
     pf_refarm_params ref;
     pf_beacon_params bcn;
     pf_camarm_params cam;
+    unsigned char raw[kMaxModelParamBytes];  // any other registered model's parameters (esthera_b200_model.cuh)
 };
 
 __device__ __forceinline__ float wrap_pi(float a) { return fmaf(-kTwoPi, floorf((a + kPi) * kInvTwoPi), a); }
 
 struct Unicycle {
-    static constexpr int S = 3, K = 3, NA = 1;
+    static constexpr int S = 3, K = 3, NA = 1, C = 2, Z = 16;
     __host__ __device__ static constexpr int angle_var(int) { return 2; }
     struct Consts {
         float A, B, wd, sq0, sq1, sq2, isr, isb;
@@ -1028,7 +1030,7 @@ struct Unicycle {
 };
 
 struct DhArm {
-    static constexpr int S = 12, K = 6, NA = 6;
+    static constexpr int S = 12, K = 6, NA = 6, C = 0, Z = 6;
     __host__ __device__ static constexpr int angle_var(int a) { return a; }
     struct Consts {
         float dt, sqd, isp, isa;
@@ -1161,7 +1163,7 @@ __device__ __forceinline__ float arm_chain(const ArmConsts& c, float* s, const f
 // position in the camera frame is measured directly; log weight =
 // -(sum 0.1 e^2) (the reference returns its exp).
 struct RefArm {
-    static constexpr int S = 9, K = 9, NA = 5;
+    static constexpr int S = 9, K = 9, NA = 5, C = 5, Z = 7;
     __host__ __device__ static constexpr int angle_var(int a) { return a; }
     using Consts = ArmConsts;
     __device__ static void prepare(Consts& c, const pf_step_input& in, const ModelParams& mp, int lane)
@@ -1186,7 +1188,7 @@ struct RefArm {
 // to pixels (xp = fc_x xd + cc_x, yp = fc_y yd + cc_y); the measured x, y
 // are pixels.  Log weight = -(sum 0.1 e^2).
 struct CamArm {
-    static constexpr int S = 9, K = 9, NA = 5;
+    static constexpr int S = 9, K = 9, NA = 5, C = 5, Z = 7;
     __host__ __device__ static constexpr int angle_var(int a) { return a; }
     struct Consts {
         ArmConsts a;
@@ -1236,7 +1238,7 @@ struct CamArm {
 // h = 1 / (2 sigma_range^2) (1 for the reference's exp(-sum e^2)) and
 // lnorm = log(1e5) - (L/2) log(2 pi), the reference's normalisation.
 struct Beacon {
-    static constexpr int S = 3, K = 3, NA = 1;
+    static constexpr int S = 3, K = 3, NA = 1, C = 2, Z = 16;
     __host__ __device__ static constexpr int angle_var(int) { return 2; }
     struct Consts {
         float dt, hdt, v, w, nv, nw, ng, h, lnorm;

@@ -24,6 +24,11 @@ pf_status fail(pf_status s, const char* fmt, ...);
 
 pf_status require_gpu(int device);
 
+// Particles per thread when a configuration leaves it at 0 (the same for
+// single filters, batches and the server: the same configuration gives the
+// same bits everywhere): 1 for m = 32, 2 for m = 64, else 4.
+int default_ppt(int M);
+
 struct ModelInfo {
     int S, K, C, Z;
     size_t psize;
@@ -54,6 +59,55 @@ struct ModelOps {
                         bool);
 };
 ModelOps model_ops(int model);
+
+// The model registry: every model the library can run, built-in or added with
+// PF_MODEL (esthera_b200_model.cuh), registered once at load time.
+struct ModelEntry {
+    int id;
+    const char* name;
+    ModelInfo info;
+    ModelOps ops;
+    uint32_t angle_mask;  // bit v: state variable v is an angle (circular means)
+    int angle_count;
+    size_t init_offset;   // offset of init_state[] in the parameter struct
+};
+// false (and nothing registered) when the id is taken, negative or the table is full.
+bool register_model(const ModelEntry& e);
+const ModelEntry* find_model(int id);
+int registered_models(int* ids, int cap);
+
+template <class Mdl>
+ModelOps ops_of()
+{
+    return {Launch<Mdl>::sample_sort,       Launch<Mdl>::sample_weight,    Launch<Mdl>::block_sort,
+            Launch<Mdl>::exchange_resample, Launch<Mdl>::exchange_inplace, Launch<Mdl>::test_model,
+            Launch<Mdl>::step};
+}
+
+template <class Mdl, class Params>
+ModelEntry model_entry(int id, const char* name, size_t init_offset)
+{
+    static_assert(sizeof(Params) <= sizeof(ModelParams), "model parameters larger than ModelParams::raw");
+    static_assert(Mdl::S >= 1 && Mdl::S <= PF_MAX_STATE && Mdl::K >= 1 && Mdl::NA >= 0 && Mdl::NA <= Mdl::S,
+                  "model sizes out of range");
+    static_assert(Mdl::C <= PF_MAX_CONTROL && Mdl::Z <= PF_MAX_MEAS, "control / measurement larger than pf_step_input");
+    uint32_t mask = 0;
+    for (int a = 0; a < Mdl::NA; ++a) mask |= 1u << Mdl::angle_var(a);
+    return {id, name, {Mdl::S, Mdl::K, Mdl::C, Mdl::Z, sizeof(Params)}, ops_of<Mdl>(), mask, Mdl::NA, init_offset};
+}
+
+}  // namespace pfhost
+
+// Registers model struct MDL (with parameter struct PARAMS, which has a
+// float init_state[MDL::S] member) under id ID, from one translation unit;
+// the kernels themselves are instantiated where Launch<MDL>'s members are.
+#define PF_CAT_(a, b) a##b
+#define PF_CAT(a, b) PF_CAT_(a, b)
+#define PF_REGISTER_MODEL(MDL, ID, PARAMS, NAME)                                                                \
+    static const bool PF_CAT(pf_model_registered_, __LINE__) =                                               \
+        ::pfhost::register_model(::pfhost::model_entry<MDL, PARAMS>((ID), (NAME), offsetof(PARAMS, init_state)))
+
+namespace pfhost {
 
 // MTGP32 stream state for parameter set `set` seeded with `seed` (351 words).
 void mtgp_init_state_host(uint32_t* st, int set, uint32_t seed);

@@ -207,7 +207,7 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     const int M = cfg->particles_per_subfilter;
     if (M < 32 || M > 1024 || (M & (M - 1)))
         return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
-    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : 2;
+    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M);
     if (!me_supported(M, E)) return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E, M);
     if (cfg->exchange != PF_EXCHANGE_NONE && cfg->exchange != PF_EXCHANGE_RING)
         return fail(PF_ERR_UNSUPPORTED, "served filters exchange by ring (or not at all)");
@@ -356,7 +356,7 @@ static pf_status ensure_map(pf_server* s, int64_t need)
 extern "C" int64_t pf_server_footprint(const pf_server* s, pf_model_id model, int32_t num_particles)
 {
     ModelInfo mi;
-    if (!s || !model_info(model, &mi)) return -1;
+    if (!s || !model_info(model, &mi) || (int)model >= PF_NUM_MODELS) return -1;
     const int M = s->cfg.particles_per_subfilter;
     if (num_particles < M || num_particles % M) return -1;
     const int N = num_particles / M;
@@ -370,6 +370,9 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     *id = -1;
     ModelInfo mi;
     if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    if ((int)model >= PF_NUM_MODELS)
+        return fail(PF_ERR_UNSUPPORTED, "the server runs the built-in models (0..%d); model %d is registered only "
+                                        "for pf_create and batches", PF_NUM_MODELS - 1, (int)model);
     if (params_size != mi.psize) return fail(PF_ERR_INVALID, "model params size %zu, expected %zu", params_size, mi.psize);
     const int M = s->cfg.particles_per_subfilter;
     if (num_particles < M || num_particles % M)

@@ -209,6 +209,16 @@ int32_t pf_device_count(void);
 /* Model sizes: state floats, normals per particle per step, control and measurement floats. */
 pf_status pf_model_info(pf_model_id model, int32_t* num_state, int32_t* num_noise,
                         int32_t* num_control, int32_t* num_meas);
+/* Models compiled into the library: the built-in ones above and any added
+ * with PF_MODEL (esthera_b200_model.cuh, ids >= PF_MODEL_USER_BASE).  The
+ * reference's model plugin is a compile-time #include of one model header
+ * (src/partfilt/cuda/pf_generic_soa.cu:43, src/models/robotarm/cuda/
+ * pf_model_soa.cuh); here every model registers itself into one table when
+ * the library loads.  pf_model_list writes up to cap ids and returns how many
+ * are registered; pf_model_name gives a model's name (NULL if unknown). */
+#define PF_MODEL_USER_BASE 64
+int32_t pf_model_list(int32_t* ids, int32_t cap);
+const char* pf_model_name(int32_t model);
 
 /* ---- plain filter (replaces particle_filter()'s step loop body) ---- */
 pf_status pf_config_default(pf_config* cfg);

@@ -201,3 +201,20 @@ def test_cli_rejects_unknown_model_and_missing_trace(tmp_path):
     r = subprocess.run([str(cli), "-M", "unicycle", "-m", "64", "-N", "2", str(tmp_path / "absent")],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "error" in r.stderr  # PF_ERR_IO before any GPU work
+
+
+def test_model_registry(E):
+    """Every model registers itself at load time: the five built-in ones and the
+    linear-Gaussian example added with PF_MODEL in one file."""
+    ids = E.model_list()
+    assert set(ids) >= {0, 1, 2, 3, 4, E.MODEL_LINGAUSS}
+    assert [E.model_name(i) for i in range(5)] == ["unicycle", "dharm", "refarm", "beacon", "camarm"]
+    assert E.model_name(E.MODEL_LINGAUSS) == "lingauss" and E.model_name(63) is None
+    assert E.model_info(E.MODEL_LINGAUSS) == (2, 1, 0, 1)
+    with pytest.raises(E.PFError) as ei:
+        E.model_info(63)
+    assert ei.value.status == E.PF_ERR_INVALID
+    if E.device_count() == 0:  # no CPU path for a registered model either
+        with pytest.raises(E.PFError) as ei:
+            E.ParticleFilter(E.MODEL_LINGAUSS, E.LinGaussParams(0.1, 0.2, 0.5, (0.0, 1.0)), num_subfilters=4)
+        assert ei.value.status == E.PF_ERR_CUDA
