@@ -145,6 +145,16 @@ def _declare(L):
         "pf_snapshot_size": (C.c_int64, [P]),
         "pf_snapshot": (C.c_int, [P, P]),
         "pf_restore": (C.c_int, [P, P, C.c_size_t]),
+        "pf_shard_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, P, C.c_size_t, C.c_int32, C.c_int32,
+                                      C.POINTER(P)]),
+        "pf_shard_info": (C.c_int, [P, ip, ip, ip, ip, C.POINTER(C.c_int64)]),
+        "pf_shard_sample": (C.c_int, [P, C.POINTER(StepInput)]),
+        "pf_shard_halo_out": (C.c_int, [P, C.c_int32, P]),
+        "pf_shard_halo_in": (C.c_int, [P, C.c_int32, P]),
+        "pf_shard_halo_copy": (C.c_int, [P, C.c_int32, P]),
+        "pf_shard_resample": (C.c_int, [P]),
+        "pf_shard_group_rows": (C.c_int, [P, C.POINTER(C.c_double), fp]),
+        "pf_shard_estimate": (C.c_int, [P, C.POINTER(C.c_double), fp, C.c_int32, C.POINTER(Estimate)]),
         "pf_batch_create": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, C.POINTER(P)]),
         "pf_batch_destroy": (C.c_int, [P]),
         "pf_batch_set_initial_states": (C.c_int, [P, fp]),
@@ -453,6 +463,94 @@ class ParticleFilter:
     def restore(self, buf):
         b = np.ascontiguousarray(buf, np.uint8)
         check(lib().pf_restore(self._h, b.ctypes.data_as(C.c_void_p), b.nbytes))
+
+
+SHARD_ROW = 32  # doubles per group row (PF_SHARD_ROW)
+
+
+class FilterShard(ParticleFilter):
+    """Rows [row0, row1) of a torus-exchange filter whose whole size is
+    config.num_subfilters sub-filters (pf_shard_*).  A step over all shards:
+    sample() on each, send_halos() (or halo_out / halo_in across processes),
+    resample() on each, then estimate() from every shard's group_rows() in row
+    order.  The shards' particles and estimate equal the whole filter's."""
+
+    def __init__(self, model, params, row0, row1, config=None, **cfg):
+        self.model = model
+        self.params = params
+        self.config = config if config is not None else default_config(**cfg)
+        self.num_state, self.num_noise, _, _ = model_info(model)
+        h = C.c_void_p()
+        check(lib().pf_shard_create(C.byref(self.config), model, C.byref(params), C.sizeof(params), row0, row1,
+                                    C.byref(h)))
+        self._h = h
+        r0, r1, b0, ng = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        hb = C.c_int64()
+        check(lib().pf_shard_info(h, C.byref(r0), C.byref(r1), C.byref(b0), C.byref(ng), C.byref(hb)))
+        self.rows = (r0.value, r1.value)
+        self.first_subfilter = b0.value
+        self.num_groups = ng.value
+        self.halo_bytes = hb.value
+        self.m = self.config.particles_per_subfilter
+        self.N_total = self.config.num_subfilters
+        dx, rows = self.info()["torus"]
+        self.N = dx * rows
+        self.T = self.m * self.N
+
+    def sample(self, inp):
+        s = inp if isinstance(inp, StepInput) else step_input(inp)
+        check(lib().pf_shard_sample(self._h, C.byref(s)))
+
+    def halo_out(self, direction):
+        """Block `direction` of this shard's export (0: last row, for the shard below; 1: first row, above)."""
+        b = np.zeros(self.halo_bytes, np.uint8)
+        check(lib().pf_shard_halo_out(self._h, direction, b.ctypes.data_as(C.c_void_p)))
+        return b
+
+    def halo_in(self, direction, buf):
+        """Import block `direction` (0: the row above this shard, 1: the row below)."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        if b.nbytes != self.halo_bytes:
+            raise ValueError("halo block of %d bytes, expected %d" % (b.nbytes, self.halo_bytes))
+        check(lib().pf_shard_halo_in(self._h, direction, b.ctypes.data_as(C.c_void_p)))
+
+    def send_halo(self, direction, to):
+        """Device copy of export block `direction` into shard `to` (its neighbour)."""
+        check(lib().pf_shard_halo_copy(self._h, direction, to._h))
+
+    def resample(self):
+        check(lib().pf_shard_resample(self._h))
+
+    def group_rows(self):
+        rows = np.zeros((self.num_groups, SHARD_ROW), np.float64)
+        st = np.zeros((self.num_groups, self.num_state), np.float32)
+        check(lib().pf_shard_group_rows(self._h, rows.ctypes.data_as(C.POINTER(C.c_double)), _fptr(st)))
+        return rows, st
+
+    def estimate(self, rows, states):
+        """The whole filter's estimate from every shard's group rows, in row order."""
+        r = np.ascontiguousarray(rows, np.float64)
+        st = _f32(states)
+        e = Estimate()
+        check(lib().pf_shard_estimate(self._h, r.ctypes.data_as(C.POINTER(C.c_double)), _fptr(st), r.shape[0],
+                                      C.byref(e)))
+        return estimate_to_numpy(e)
+
+
+def shard_step(shards, inp):
+    """One step of a filter spread over `shards` (in row order, one process)."""
+    for s in shards:
+        s.sample(inp)
+    n = len(shards)
+    for i, s in enumerate(shards):
+        s.send_halo(0, shards[(i + 1) % n])
+        s.send_halo(1, shards[(i - 1) % n])
+    for s in shards:
+        s.resample()
+    parts = [s.group_rows() for s in shards]
+    rows = np.concatenate([p[0] for p in parts])
+    states = np.concatenate([p[1] for p in parts])
+    return shards[0].estimate(rows, states)
 
 
 class FilterBatch:

@@ -259,6 +259,13 @@ struct pf_filter {
     int q_active = 0;   // the device counter holds q_next (else set it before the next submit)
     int q_pending = 0;  // submitted, not yet collected
     int32_t q_next = 0; // step number (and slot, modulo the depth) of the next submit
+    // a shard of a larger filter (pf_shard_*): global sub-filters b0 ..
+    // b0 + N - 1 (rows r0 .. of the global dx x gdy torus of gN sub-filters)
+    int shard = 0, b0 = 0, r0 = 0, gdy = 0, gN = 0;
+    float *halo_in = nullptr, *halo_out = nullptr;  // [2][1+S][dx*t] each
+    double* rows = nullptr;                         // the last step's group rows [ng][kPartStride]
+    float* states = nullptr;                        // and their winners' states [ng][S]
+    cudaEvent_t ev_sampled = nullptr;
     // per-phase timing: events recorded between the launches of a step
     int timing = 0;
     cudaEvent_t ev[8] = {};
@@ -290,6 +297,7 @@ static void release(pf_filter* f)
 {
     if (!f) return;
     if (f->graph) cudaGraphExecDestroy(f->graph);
+    if (f->ev_sampled) cudaEventDestroy(f->ev_sampled);
     for (cudaEvent_t e : f->ev)
         if (e) cudaEventDestroy(e);
     for (int i = 0; i < PF_QUEUE_DEPTH; ++i) {
@@ -450,6 +458,11 @@ static void fill_desc(pf_filter* f, FilterDesc& D, pf_estimate* est)
     D.gpart = f->gpart;
     D.angle_mask = f->angle_mask;
     D.na = f->na;
+    D.shard = f->shard;
+    D.b0 = f->b0;
+    D.r0 = f->r0;
+    D.gdy = f->gdy;
+    D.halo = f->halo_in;
     D.mp = f->mp;
 }
 
@@ -821,6 +834,7 @@ extern "C" const char* pf_phase_name(pf_filter* f, int32_t i)
 extern "C" pf_status pf_step(pf_filter* f, const pf_step_input* in, pf_estimate* out)
 {
     if (!f || !in) return fail(PF_ERR_INVALID, "null argument");
+    if (f->shard) return fail(PF_ERR_INVALID, "a shard steps through pf_shard_sample / pf_shard_resample");
     CU(cudaSetDevice(f->cfg.device));
     *f->h_in = *in;
     CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
@@ -881,6 +895,7 @@ extern "C" pf_status pf_run_device(pf_filter* f, const pf_step_input* d_inputs, 
                                    int32_t capacity, int32_t steps)
 {
     if (!f || !d_inputs || !d_estimates || capacity < 1 || steps < 0) return fail(PF_ERR_INVALID, "bad argument");
+    if (f->shard) return fail(PF_ERR_INVALID, "a shard steps through pf_shard_sample / pf_shard_resample");
     CU(cudaSetDevice(f->cfg.device));
     pf_status s = ensure_run_graph(f, d_inputs, d_estimates, capacity);
     if (s != PF_OK) return s;
@@ -924,6 +939,7 @@ static pf_status queue_setup(pf_filter* f)
 extern "C" pf_status pf_step_submit(pf_filter* f, const pf_step_input* in)
 {
     if (!f || !in) return fail(PF_ERR_INVALID, "null argument");
+    if (f->shard) return fail(PF_ERR_INVALID, "a shard steps through pf_shard_sample / pf_shard_resample");
     CU(cudaSetDevice(f->cfg.device));
     pf_status s = queue_setup(f);
     if (s != PF_OK) return s;
@@ -1296,5 +1312,225 @@ extern "C" pf_status pfk_model_step(pf_model_id model, const void* params, size_
                                    (float*)dl.p, 0));
     CU(cudaMemcpy(state, ds.p, (size_t)mi.S * n * 4, cudaMemcpyDeviceToHost));
     CU(cudaMemcpy(loglik, dl.p, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Shards: one filter's torus rows spread over several filters (devices,
+// processes).  The reference runs one filter per process
+// (src/partfilt/cuda/pf_generic_soa.cu:686); its torus exchange
+// (src/partfilt/cuda/pf_generic.cu:352-393, dims :682-683) is what crosses
+// the shard boundaries here: between a step's sampling and its resampling
+// each shard hands the sorted top t of its first and last rows to the shards
+// above and below, and the group partial rows of all shards are combined into
+// the filter's estimate in group order.  With shard boundaries on whole rows
+// and on multiples of 32 sub-filters, the shards' particles, sorted copies and
+// estimate equal the unsharded filter's bit for bit.
+// ---------------------------------------------------------------------------
+static_assert(PF_SHARD_ROW == kPartStride, "group row width");
+static int64_t halo_block_floats(const pf_filter* f) { return (int64_t)(1 + f->mi.S) * f->dx * f->t; }
+
+extern "C" pf_status pf_shard_create(const pf_config* cfg, pf_model_id model, const void* params, size_t params_size,
+                                     int32_t row0, int32_t row1, pf_filter** out)
+{
+    if (!cfg || !out) return fail(PF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->exchange != PF_EXCHANGE_TORUS || cfg->num_transfer < 1)
+        return fail(PF_ERR_UNSUPPORTED, "shards run the torus exchange (t >= 1)");
+    if (cfg->rng != PF_RNG_SUBFILTER) return fail(PF_ERR_UNSUPPORTED, "shards draw one MTGP32 stream per sub-filter");
+    if (cfg->exchange_period > 1) return fail(PF_ERR_UNSUPPORTED, "shards exchange every step");
+    const int N = cfg->num_subfilters;
+    ModelInfo mi;
+    if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
+    int E = 0;
+    TRYS(validate(cfg, model, mi, &E));  // the whole filter's configuration (torus dims, 5 t <= m)
+    int dx = 0, dy = 0;
+    torus_dims(N, &dx, &dy);
+    if (row0 < 0 || row1 <= row0 || row1 > dy)
+        return fail(PF_ERR_INVALID, "rows [%d, %d) outside the %d x %d torus", row0, row1, dx, dy);
+    if (row1 - row0 == dy) return fail(PF_ERR_INVALID, "a shard holding every row is the whole filter: use pf_create");
+    const int b0 = row0 * dx, n = (row1 - row0) * dx;
+    if (b0 % 32 != 0 || (n % 32 != 0 && b0 + n != N))
+        return fail(PF_ERR_UNSUPPORTED, "shard boundaries must fall on multiples of 32 sub-filters (the estimate's "
+                                        "groups); rows [%d, %d) of width %d start at sub-filter %d", row0, row1, dx, b0);
+    pf_config c = *cfg;
+    c.num_subfilters = n;
+    c.stream_offset = cfg->stream_offset + b0;  // global sub-filter b draws the stream of the whole filter's b
+    c.pipeline = PF_PIPELINE_SPLIT;
+    c.exchange = PF_EXCHANGE_RING;  // the shard's rows need not form a torus of their own
+    pf_filter* f = nullptr;
+    pf_status s = pf_create(&c, model, params, params_size, &f);
+    if (s != PF_OK) return s;
+    f->cfg.exchange = PF_EXCHANGE_TORUS;
+    f->shard = 1;
+    f->b0 = b0;
+    f->r0 = row0;
+    f->gdy = dy;
+    f->gN = N;
+    f->dx = dx;
+    f->dy = row1 - row0;
+    const int64_t hb = halo_block_floats(f);
+    const int ng = (n + 31) / 32;
+#define TRYR(x)              \
+    do {                     \
+        pf_status s_ = (x);  \
+        if (s_ != PF_OK) {   \
+            release(f);      \
+            return s_;       \
+        }                    \
+    } while (0)
+    TRYR(dalloc(f, &f->halo_in, 2 * (size_t)hb));
+    TRYR(dalloc(f, &f->halo_out, 2 * (size_t)hb));
+    TRYR(dalloc(f, &f->rows, (size_t)ng * kPartStride));
+    TRYR(dalloc(f, &f->states, (size_t)ng * f->mi.S));
+    if (cudaMemset(f->halo_in, 0, 2 * (size_t)hb * 4) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f->ev_sampled, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        release(f);
+        return fail(PF_ERR_CUDA, "shard set-up failed");
+    }
+    TRYR(upload_descs(f, nullptr));
+#undef TRYR
+    *out = f;
+    return PF_OK;
+}
+
+static pf_status need_shard(const pf_filter* f)
+{
+    if (!f) return fail(PF_ERR_INVALID, "null argument");
+    if (!f->shard) return fail(PF_ERR_INVALID, "not a shard (pf_shard_create)");
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_info(pf_filter* f, int32_t* row0, int32_t* row1, int32_t* first_subfilter,
+                                   int32_t* num_groups, int64_t* halo_bytes)
+{
+    TRYS(need_shard(f));
+    if (row0) *row0 = f->r0;
+    if (row1) *row1 = f->r0 + f->dy;
+    if (first_subfilter) *first_subfilter = f->b0;
+    if (num_groups) *num_groups = (f->N + 31) / 32;
+    if (halo_bytes) *halo_bytes = 4 * halo_block_floats(f);
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_sample(pf_filter* f, const pf_step_input* in)
+{
+    TRYS(need_shard(f));
+    if (!in) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    *f->h_in = *in;
+    CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
+    InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
+    CU(f->ops.sample_sort(f->M, f->E, true, f->N, f->stream, f->d_desc, nullptr, ir));
+    CU(launch_shard_pack(f->d_desc, f->halo_out, f->mi.S, f->dx * f->t, f->stream));
+    CU(cudaEventRecord(f->ev_sampled, f->stream));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_halo_out(pf_filter* f, int32_t dir, void* host_buf)
+{
+    TRYS(need_shard(f));
+    if (!host_buf || (dir != 0 && dir != 1)) return fail(PF_ERR_INVALID, "bad argument");
+    CU(cudaSetDevice(f->cfg.device));
+    const int64_t hb = halo_block_floats(f);
+    CU(cudaMemcpyAsync(host_buf, f->halo_out + dir * hb, 4 * (size_t)hb, cudaMemcpyDeviceToHost, f->stream));
+    CU(cudaStreamSynchronize(f->stream));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_halo_in(pf_filter* f, int32_t dir, const void* host_buf)
+{
+    TRYS(need_shard(f));
+    if (!host_buf || (dir != 0 && dir != 1)) return fail(PF_ERR_INVALID, "bad argument");
+    CU(cudaSetDevice(f->cfg.device));
+    const int64_t hb = halo_block_floats(f);
+    CU(cudaMemcpyAsync(f->halo_in + dir * hb, host_buf, 4 * (size_t)hb, cudaMemcpyHostToDevice, f->stream));
+    CU(cudaStreamSynchronize(f->stream));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_halo_copy(pf_filter* from, int32_t dir, pf_filter* to)
+{
+    TRYS(need_shard(from));
+    TRYS(need_shard(to));
+    if (dir != 0 && dir != 1) return fail(PF_ERR_INVALID, "dir must be 0 or 1");
+    if (from->gN != to->gN || from->dx != to->dx || from->t != to->t || from->mi.S != to->mi.S || from->M != to->M)
+        return fail(PF_ERR_INVALID, "the shards belong to different filters");
+    // block 0 carries from's last row to the shard below it (its row above),
+    // block 1 from's first row to the shard above it (its row below)
+    const int gdy = from->gdy;
+    const bool adjacent = dir == 0 ? to->r0 == (from->r0 + from->dy) % gdy : (to->r0 + to->dy) % gdy == from->r0;
+    if (!adjacent)
+        return fail(PF_ERR_INVALID, "the shard at rows [%d, %d) is not the %s neighbour of the shard at rows [%d, %d)",
+                    to->r0, to->r0 + to->dy, dir == 0 ? "lower" : "upper", from->r0, from->r0 + from->dy);
+    const int64_t hb = halo_block_floats(from);
+    CU(cudaSetDevice(to->cfg.device));
+    CU(cudaStreamWaitEvent(to->stream, from->ev_sampled, 0));
+    if (from->cfg.device == to->cfg.device)
+        CU(cudaMemcpyAsync(to->halo_in + dir * hb, from->halo_out + dir * hb, 4 * (size_t)hb,
+                           cudaMemcpyDeviceToDevice, to->stream));
+    else
+        CU(cudaMemcpyPeerAsync(to->halo_in + dir * hb, to->cfg.device, from->halo_out + dir * hb, from->cfg.device,
+                               4 * (size_t)hb, to->stream));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_resample(pf_filter* f)
+{
+    TRYS(need_shard(f));
+    CU(cudaSetDevice(f->cfg.device));
+    InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
+    CU(f->ops.exchange_resample(f->M, f->E, f->cfg.resampler, f->N, f->stream, f->d_desc, nullptr, ir, nullptr, 1));
+    const int ng = (f->N + 31) / 32;
+    CU(launch_shard_rows(f->d_desc, ng, f->rows, f->states, f->mi.S, 2 + f->mi.S + f->na, f->stream));
+    CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate) + sizeof(int32_t), cudaMemcpyDeviceToHost, f->stream));
+    CU(cudaStreamSynchronize(f->stream));
+    f->steps_done++;
+    return check_status(*reinterpret_cast<const int32_t*>(f->h_est + 1));
+}
+
+extern "C" pf_status pf_shard_group_rows(pf_filter* f, double* rows, float* states)
+{
+    TRYS(need_shard(f));
+    if (!rows || !states) return fail(PF_ERR_INVALID, "null argument");
+    CU(cudaSetDevice(f->cfg.device));
+    const int ng = (f->N + 31) / 32;
+    CU(cudaMemcpy(rows, f->rows, (size_t)ng * kPartStride * 8, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(states, f->states, (size_t)ng * f->mi.S * 4, cudaMemcpyDeviceToHost));
+    return PF_OK;
+}
+
+extern "C" pf_status pf_shard_estimate(pf_filter* f, const double* rows, const float* states, int32_t num_groups,
+                                       pf_estimate* out)
+{
+    TRYS(need_shard(f));
+    const int S = f->mi.S, ngt = (f->gN + 31) / 32, NV = 2 + S + f->na;
+    if (!rows || !states || !out || num_groups != ngt)
+        return fail(PF_ERR_INVALID, "the estimate takes the rows of all %d groups", ngt);
+    CU(cudaSetDevice(f->cfg.device));
+    // winner states at their filter-wide sub-filter index (rows[g][NV+1])
+    std::vector<float> best((size_t)S * f->gN, 0.0f);
+    for (int g = 0; g < ngt; ++g) {
+        const double wi = rows[(size_t)g * kPartStride + NV + 1];
+        if (!(wi >= 0.0) || wi >= (double)f->gN) continue;
+        for (int v = 0; v < S; ++v) best[(size_t)v * f->gN + (size_t)wi] = states[(size_t)g * S + v];
+    }
+    DevBuf dr, db, de;
+    TRYS(dev_buf(dr, (size_t)ngt * kPartStride * 8));
+    TRYS(dev_buf(db, best.size() * 4));
+    TRYS(dev_buf(de, sizeof(pf_estimate)));
+    CU(cudaMemcpy(dr.p, rows, (size_t)ngt * kPartStride * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(db.p, best.data(), best.size() * 4, cudaMemcpyHostToDevice));
+    FilterDesc D;
+    fill_desc(f, D, static_cast<pf_estimate*>(de.p));
+    D.gpart = static_cast<double*>(dr.p);
+    D.N = f->gN;
+    D.T = f->gN;
+    D.M = 1;
+    D.b0 = 0;
+    CU(launch_shard_estimate(D, S, static_cast<const float*>(db.p), static_cast<pf_estimate*>(de.p), ngt,
+                             f->steps_done, 0));
+    CU(cudaMemcpy(out, de.p, sizeof(pf_estimate), cudaMemcpyDeviceToHost));
     return PF_OK;
 }

@@ -348,6 +348,77 @@ cudaError_t launch_test_bounded_wait_mixed(const int32_t* limits, int nthreads, 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Shards (pf_shard_*): the halo export of a step and the group rows.
+// ---------------------------------------------------------------------------
+// The sorted top t of the shard's last row (block 0, the shard below takes it
+// as its top halo) and first row (block 1, the shard above's bottom halo):
+// out[h][1+S][dx*t], key row then state rows, slot x*t + j of row sub-filter x.
+__global__ void k_shard_pack(const FilterDesc* __restrict__ descs, float* __restrict__ out, int S)
+{
+    const FilterDesc& D = descs[0];
+    const int P = D.dx * D.t, rows = D.N / D.dx;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < 2 * P; i += blockDim.x * gridDim.x) {
+        const int h = i / P, idx = i - h * P, x = idx / D.t, j = idx - x * D.t;
+        const int b = (h == 0 ? rows - 1 : 0) * D.dx + x;
+        const int64_t g = (int64_t)b * D.M + j;
+        float* o = out + (int64_t)h * (1 + S) * P + idx;
+        o[0] = D.tkey[g];
+        for (int v = 0; v < S; ++v) o[(int64_t)(1 + v) * P] = D.tmp[v * D.T + g];
+    }
+}
+
+cudaError_t launch_shard_pack(const FilterDesc* d, float* out, int S, int P, cudaStream_t st)
+{
+    k_shard_pack<<<(2 * P + 255) / 256, 256, 0, st>>>(d, out, S);
+    return cudaGetLastError();
+}
+
+// Each local group's partial row (kPartStride doubles, its winner as a
+// filter-wide index) and that winner's state (the best slot of the winning
+// sub-filter).
+__global__ void k_shard_rows(const FilterDesc* __restrict__ descs, double* __restrict__ rows, float* __restrict__ states,
+                             int S, int NV)
+{
+    const FilterDesc& D = descs[0];
+    const int g = blockIdx.x;
+    const double* r = D.gpart + (int64_t)g * kPartStride;
+    for (int j = threadIdx.x; j < kPartStride; j += blockDim.x) rows[(int64_t)g * kPartStride + j] = r[j];
+    const int b = (int)r[NV + 1] - D.b0;
+    for (int v = threadIdx.x; v < S; v += blockDim.x) states[(int64_t)g * S + v] = D.tmp[v * D.T + (int64_t)b * D.M];
+}
+
+cudaError_t launch_shard_rows(const FilterDesc* d, int ng, double* rows, float* states, int S, int NV, cudaStream_t st)
+{
+    k_shard_rows<<<ng, 32, 0, st>>>(d, rows, states, S, NV);
+    return cudaGetLastError();
+}
+
+// The filter-wide estimate from every shard's group rows, in group order (the
+// same combination as a whole filter's last group makes): D.gpart holds the
+// rows, best_src[v * D.T + b] the winner states at their sub-filter b.
+template <int S>
+__global__ void k_shard_estimate(FilterDesc D, const float* __restrict__ best_src, pf_estimate* out, int ng,
+                                 int32_t step_no)
+{
+    if (threadIdx.x >= 32) return;
+    estimate_final<S>(D, threadIdx.x, ng, 2 + S + D.na, best_src, *out, step_no);
+}
+
+cudaError_t launch_shard_estimate(const FilterDesc& D, int S, const float* best_src, pf_estimate* out, int ng,
+                                  int32_t step_no, cudaStream_t st)
+{
+#define PF_SE(s)                                                                 \
+    if (S == s) {                                                                \
+        k_shard_estimate<s><<<1, 32, 0, st>>>(D, best_src, out, ng, step_no);    \
+        return cudaGetLastError();                                               \
+    }
+    PF_SE(1) PF_SE(2) PF_SE(3) PF_SE(4) PF_SE(5) PF_SE(6) PF_SE(7) PF_SE(8)
+    PF_SE(9) PF_SE(10) PF_SE(11) PF_SE(12) PF_SE(13) PF_SE(14) PF_SE(15) PF_SE(16)
+#undef PF_SE
+    return cudaErrorInvalidValue;
+}
+
 // A run's device step counter, advanced (or set) by a launch of its own once
 // every kernel of the step that reads it is enqueued before it.
 __global__ void k_counter_update(int32_t* ctr, int32_t set, int32_t value)

@@ -49,6 +49,13 @@ struct FilterDesc {
     int32_t na;        // angular state variables (circular means)
     int32_t exch_period;  // exchange on steps with step % period == 0 (<= 1: every step)
     int32_t* status;      // PF_STATUS_* bits set by the kernels (0: all well)
+    // a shard of a larger filter (pf_shard_*): this filter's sub-filters are
+    // the global ones b0 .. b0+N-1, whole rows r0 .. r0 + N/dx - 1 of the
+    // global dx x gdy torus; the rows just outside come from the neighbouring
+    // shards through `halo`
+    int32_t shard;        // 0: a whole filter
+    int32_t b0, r0, gdy;
+    const float* halo;    // [2][1+S][dx*t]: block 0 row r0-1 (top), block 1 the row after the last (bottom); key row then state rows
     ModelParams mp;
 };
 
@@ -540,14 +547,47 @@ __device__ __forceinline__ int64_t exchange_source(const FilterDesc& D, int b, i
     if (D.exchange == PF_EXCHANGE_RING) return (int64_t)((b - 1 + N) % N) * M + x;
     if (D.exchange == PF_EXCHANGE_ALL2ALL) return D.a2a[x];
     const int k = x / t, j = x - k * t;
-    const int dx = D.dx, dy = D.dy;
-    const int cx = b % dx, cy = b / dx;
+    const int dx = D.dx, dy = D.shard ? D.gdy : D.dy;
+    const int bg = b + D.b0;
+    const int cx = bg % dx, cy = bg / dx;
     int from;
     if (k == 0) from = cy * dx + (cx + 1) % dx;            // right neighbour sent "left"
     else if (k == 1) from = cy * dx + (cx - 1 + dx) % dx;  // left neighbour sent "right"
     else if (k == 2) from = ((cy + 1) % dy) * dx + cx;     // bottom neighbour sent "top"
     else from = ((cy - 1 + dy) % dy) * dx + cx;            // top neighbour sent "bottom"
+    if (D.shard) {
+        // a row of this shard, or the halo row above (block 0) / below (block 1):
+        // halo slots are returned as -(1 + index into a block's rows)
+        const int fy = from / dx, fx = from - fy * dx, rows = N / dx;
+        const int ry = (fy - D.r0 + dy) % dy;
+        if (ry < rows) return (int64_t)(from - D.b0) * M + j;
+        const int h = ry == dy - 1 ? 0 : 1;
+        return -(1 + ((int64_t)(h * dx + fx) * t + j));
+    }
     return (int64_t)from * M + j;
+}
+
+// The sorted key and state of exchange source g (exchange_source): this
+// filter's sorted copy, or a shard's halo block.
+template <int S>
+__device__ __forceinline__ void exchange_fetch(const FilterDesc& D, const float* __restrict__ src_key,
+                                               const float* __restrict__ src_tmp, int64_t T, int64_t g, float& key,
+                                               float (&v)[S])
+{
+    if (g >= 0) {
+        key = src_key[g];
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = src_tmp[s * T + g];
+    } else {
+        const int64_t i = -(g + 1);  // (h dx + x) t + j
+        const int P = D.dx * D.t;
+        const int h = (int)(i / P);
+        const float* blk = D.halo + (int64_t)h * (1 + S) * P;
+        const int64_t o = i - (int64_t)h * P;
+        key = blk[o];
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = blk[(int64_t)(1 + s) * P + o];
+    }
 }
 
 __device__ __forceinline__ int exchange_count(const FilterDesc& D)
@@ -567,12 +607,9 @@ __global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const i
     const FilterDesc& D = descs[f];
     const int nx = exchange_count(D);
     for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-        const int64_t g = exchange_source(D, b, x);
         const int64_t d = (int64_t)b * D.M + D.M - 1 - x;
-        const float kk = D.tkey[g];
-        float v[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) v[s] = D.tmp[s * D.T + g];
+        float kk, v[S];
+        exchange_fetch<S>(D, D.tkey, D.tmp, D.T, exchange_source(D, b, x), kk, v);
         D.tkey[d] = kk;
 #pragma unroll
         for (int s = 0; s < S; ++s) D.tmp[s * D.T + d] = v[s];
@@ -696,6 +733,40 @@ __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, in
     __syncwarp();
 }
 
+// The global estimate from the group partial rows gpart[0..ng) (one warp): the
+// global maximum, the first-maximum winner, then estimate_write (whose winner
+// state is read at best_src + v T + winner M).
+template <int S>
+__device__ __forceinline__ void estimate_final(const FilterDesc& D, int lane, int ng, int NV,
+                                               const float* __restrict__ best_src, pf_estimate& E, int32_t step_no)
+{
+    double gm = -INFINITY;
+    float bk = -INFINITY;
+    int bi = 0x7fffffff;
+#pragma unroll 2
+    for (int q = lane; q < ng; q += 32) {
+        const double* gq = D.gpart + (int64_t)q * kPartStride;
+        gm = fmax(gm, __ldcg(gq));
+        const float k = (float)__ldcg(gq + NV);
+        const int i = (int)__ldcg(gq + NV + 1);
+        if (k > bk || (k == bk && i < bi)) {
+            bk = k;
+            bi = i;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gm = fmax(gm, __shfl_xor_sync(kFull, gm, o));
+        const float ok = __shfl_xor_sync(kFull, bk, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        if (ok > bk || (ok == bk && oi < bi)) {
+            bk = ok;
+            bi = oi;
+        }
+    }
+    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, best_src, E, step_no);
+}
+
 template <int S>
 __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, const InputRef& in, int32_t* step_ctr)
 {
@@ -740,8 +811,9 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
     if (lane == 0) {
         go[0] = D.log_weights ? gl : 0.0;
         go[NV] = (double)wk;
-        go[NV + 1] = (double)wi;
+        go[NV + 1] = (double)(wi + D.b0);  // the filter-wide index (a shard's sub-filters start at b0)
     }
+    if (D.shard) return;  // the shards' group rows are combined across shards (pf_shard_estimate)
     __syncwarp();
     __threadfence();
     int last = 0;
@@ -749,31 +821,7 @@ __device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, cons
     last = __shfl_sync(kFull, last, 0);
     if (!last) return;
     __threadfence();
-    double gm = -INFINITY;
-    float bk = -INFINITY;
-    int bi = 0x7fffffff;
-#pragma unroll 2
-    for (int q = lane; q < ng; q += 32) {
-        const double* gq = D.gpart + (int64_t)q * kPartStride;
-        gm = fmax(gm, __ldcg(gq));
-        const float k = (float)__ldcg(gq + NV);
-        const int i = (int)__ldcg(gq + NV + 1);
-        if (k > bk || (k == bk && i < bi)) {
-            bk = k;
-            bi = i;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gm = fmax(gm, __shfl_xor_sync(kFull, gm, o));
-        const float ok = __shfl_xor_sync(kFull, bk, o);
-        const int oi = __shfl_xor_sync(kFull, bi, o);
-        if (ok > bk || (ok == bk && oi < bi)) {
-            bk = ok;
-            bi = oi;
-        }
-    }
-    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, D.tmp, D.est[step_index(in)], in.ctr ? *in.ctr + 1 : 0);
+    estimate_final<S>(D, lane, ng, NV, D.tmp, D.est[step_index(in)], in.ctr ? *in.ctr + 1 : 0);
     if (lane == 0) {
         *D.est_ctr = 0;
         __threadfence();
@@ -951,12 +999,7 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int x = M - 1 - (E * tid + e);
-                if (x < nx) {
-                    const int64_t g = exchange_source(D, b, x);
-                    xk[e] = src_key[g];
-#pragma unroll
-                    for (int v = 0; v < S; ++v) xs[e][v] = src_tmp[v * T + g];
-                }
+                if (x < nx) exchange_fetch<S>(D, src_key, src_tmp, T, exchange_source(D, b, x), xk[e], xs[e]);
             }
         }
         __syncthreads();  // the mbarrier is initialised
@@ -990,10 +1033,10 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
             for (int e = 0; e < E; ++e) {
                 const int x = M - 1 - (E * tid + e);
                 if (x < nx) {
-                    const int64_t g = exchange_source(D, b, x);
-                    kb[E * tid + e] = src_key[g];
+                    float xv[S];
+                    exchange_fetch<S>(D, src_key, src_tmp, T, exchange_source(D, b, x), kb[E * tid + e], xv);
 #pragma unroll
-                    for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = src_tmp[v * T + g];
+                    for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = xv[v];
                 }
             }
         }

@@ -78,6 +78,11 @@ cudaError_t launch_a2a_merge(int nfilters, const FilterDesc* d, cudaStream_t st)
 cudaError_t launch_exchange_sources(const FilterDesc* d, int32_t* src, cudaStream_t st);
 cudaError_t launch_a2a_merge_step(const FilterDesc* d, const StepState& X, cudaStream_t st);
 cudaError_t launch_test_bounded_wait(int limit, int32_t* status, cudaStream_t st);
+// shards (pf_shard_*)
+cudaError_t launch_shard_pack(const FilterDesc* d, float* out, int S, int P, cudaStream_t st);
+cudaError_t launch_shard_rows(const FilterDesc* d, int ng, double* rows, float* states, int S, int NV, cudaStream_t st);
+cudaError_t launch_shard_estimate(const FilterDesc& D, int S, const float* best_src, pf_estimate* out, int ng,
+                                  int32_t step_no, cudaStream_t st);
 constexpr int kMixedWaitSrcBytes = 32768;  // the source buffer launch_test_bounded_wait_mixed copies
 cudaError_t launch_test_bounded_wait_mixed(const int32_t* limits, int nthreads, const void* src, int32_t* outcome,
                                            int32_t* copied, cudaStream_t st);

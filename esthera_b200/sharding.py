@@ -113,7 +113,8 @@ class TorusShard:
 
 def halo_exchange(dist, shard, to_up, to_down):
     """Send this rank's first-row halo up and last-row halo down, receive the
-    neighbours' (torch tensors (state, keys)); returns (from_up, from_down).
+    neighbours' (tuples of torch tensors, e.g. (state, keys), the same shapes
+    on every rank); returns (from_up, from_down).
     Sends are posted down-halo first and receives up-halo first, so that with
     two ranks (the same peer above and below) the messages pair up in order
     on backends without tags; the tags say the same for those that use them.
@@ -121,8 +122,8 @@ def halo_exchange(dist, shard, to_up, to_down):
     import torch
     if shard.world == 1:
         return to_down, to_up
-    from_up = (torch.empty_like(to_up[0]), torch.empty_like(to_up[1]))
-    from_down = (torch.empty_like(to_down[0]), torch.empty_like(to_down[1]))
+    from_up = tuple(torch.empty_like(x) for x in to_up)
+    from_down = tuple(torch.empty_like(x) for x in to_down)
     ops = []
     for x in to_down:
         ops.append(dist.P2POp(dist.isend, x.contiguous(), shard.down, tag=1))
@@ -135,6 +136,64 @@ def halo_exchange(dist, shard, to_up, to_down):
     for r in dist.batch_isend_irecv(ops):
         r.wait()
     return from_up, from_down
+
+
+class ShardedFilter:
+    """This rank's rows of a torus-exchange filter of config.num_subfilters
+    sub-filters, stepped together with the other ranks' rows (pf_shard_*, one
+    process per GPU).  Per step: sampling on every rank; two halo blocks of
+    halo_bytes to each neighbouring rank (halo_exchange: the first row's top t
+    to the rank above, the last row's to the rank below); resampling; one
+    all_gather of the group rows (ceil(n / 32) rows of 32 doubles and the
+    groups' winner states per rank) from which every rank forms the same
+    estimate.  The ranks' particles and the estimate equal the whole filter's
+    on one GPU bit for bit.  The rows split evenly: dy / world rows per rank,
+    each rank's first sub-filter a multiple of 32.  Halos and group rows travel
+    as CPU tensors on gloo and as CUDA tensors on NCCL."""
+
+    def __init__(self, dist, model, params, config=None, **cfg):
+        from . import FilterShard, default_config
+        self.dist = dist
+        self.world, self.rank = dist.get_world_size(), dist.get_rank()
+        c = config if config is not None else default_config(**cfg)
+        self.geom = TorusShard(c.num_subfilters, c.particles_per_subfilter, c.num_transfer, self.world, self.rank)
+        g = self.geom
+        self.shard = FilterShard(model, params, g.row0, g.row0 + g.rows, config=c)
+        import torch
+        self.device = (torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl"
+                       else torch.device("cpu"))
+
+    def set_initial_state(self, state):
+        self.shard.set_initial_state(state)
+
+    def particles(self):
+        """This rank's particles, num_state x (its sub-filters x m)."""
+        return self.shard.particles()
+
+    def _t(self, a):
+        import torch
+        return torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+
+    def step(self, inp):
+        """One step of the whole filter; returns its estimate (ESTIMATE_DTYPE record)."""
+        sh, dist = self.shard, self.dist
+        sh.sample(inp)
+        to_up, to_down = sh.halo_out(1), sh.halo_out(0)
+        from_up, from_down = halo_exchange(dist, self.geom, (self._t(to_up),), (self._t(to_down),))
+        sh.halo_in(0, from_up[0].cpu().numpy())    # the row above this rank's first row
+        sh.halo_in(1, from_down[0].cpu().numpy())  # the row below its last row
+        sh.resample()
+        rows, states = sh.group_rows()
+        r, st = self._t(rows), self._t(states)
+        all_r = [r.new_empty(r.shape) for _ in range(self.world)]
+        all_s = [st.new_empty(st.shape) for _ in range(self.world)]
+        dist.all_gather(all_r, r)
+        dist.all_gather(all_s, st)
+        return sh.estimate(np.concatenate([x.cpu().numpy() for x in all_r]),
+                           np.concatenate([x.cpu().numpy() for x in all_s]))
+
+    def close(self):
+        self.shard.close()
 
 
 # ---------------------------------------------------------------------------

@@ -286,6 +286,40 @@ int64_t pf_snapshot_size(pf_filter* f);
 pf_status pf_snapshot(pf_filter* f, void* host_buf);
 pf_status pf_restore(pf_filter* f, const void* host_buf, size_t size);
 
+/* ---- shards: one filter's torus rows spread over several filters ----
+ * The reference runs a filter in one process (particle_filter,
+ * pf_generic_soa.cu:686) with the torus exchange of pf_generic.cu:352-393 on
+ * a dx x dy grid (pf_generic_soa.cu:682-683).  A shard holds rows
+ * [row0, row1) of that grid (cfg->num_subfilters is the WHOLE filter's N; the
+ * exchange must be the torus, every step, with per-sub-filter streams).  Its
+ * first sub-filter row0*dx and its size must be multiples of 32 (the size may
+ * instead end at N).  A step is:
+ *   pf_shard_sample on every shard;
+ *   pf_shard_halo_copy(s, 0, lower(s)) and pf_shard_halo_copy(s, 1, upper(s))
+ *     for every shard s (or pf_shard_halo_out / pf_shard_halo_in through host
+ *     buffers of halo_bytes, e.g. across processes), where lower(s) is the
+ *     shard whose first row follows s's last row and upper(s) the shard whose
+ *     last row precedes s's first row (both on the torus);
+ *   pf_shard_resample on every shard;
+ *   pf_shard_group_rows on every shard, concatenated in row order into
+ *     num_groups = ceil(N / 32) rows of PF_SHARD_ROW doubles and
+ *     num_groups x S winner states, then pf_shard_estimate on any shard.
+ * The shards' particles and the estimate then equal the whole filter's bit for
+ * bit.  pf_step, pf_run_device and pf_step_submit reject a shard. */
+#define PF_SHARD_ROW 32
+pf_status pf_shard_create(const pf_config* cfg, pf_model_id model, const void* params, size_t params_size,
+                          int32_t row0, int32_t row1, pf_filter** out);
+pf_status pf_shard_info(pf_filter* f, int32_t* row0, int32_t* row1, int32_t* first_subfilter, int32_t* num_groups,
+                        int64_t* halo_bytes);
+pf_status pf_shard_sample(pf_filter* f, const pf_step_input* in);
+pf_status pf_shard_halo_out(pf_filter* f, int32_t dir, void* host_buf);
+pf_status pf_shard_halo_in(pf_filter* f, int32_t dir, const void* host_buf);
+pf_status pf_shard_halo_copy(pf_filter* from, int32_t dir, pf_filter* to);
+pf_status pf_shard_resample(pf_filter* f);
+pf_status pf_shard_group_rows(pf_filter* f, double* rows, float* states);
+pf_status pf_shard_estimate(pf_filter* f, const double* rows, const float* states, int32_t num_groups,
+                            pf_estimate* out);
+
 /* ---- batched filters: many independent filters of uneven sizes stepped together ----
  * The reference runs one filter per process (particle_filter, pf_generic_soa.cu:686);
  * these calls have no counterpart there.  Every filter shares cfg's model, m,

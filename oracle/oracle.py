@@ -38,7 +38,8 @@ class OrcFilter(C.Structure):
                 ("log_weights", C.c_int), ("freq", C.c_float), ("seed", C.c_uint32), ("mask", C.c_uint32),
                 ("T", C.c_int64), ("state", C.POINTER(C.c_float)), ("tmp", C.POINTER(C.c_float)),
                 ("tkey", C.POINTER(C.c_float)), ("mtgp", C.POINTER(C.c_uint32)), ("streams", C.c_int),
-                ("rbuf", C.POINTER(C.c_float)), ("rtotal", C.c_int64), ("ess_frac", C.c_float)]
+                ("rbuf", C.POINTER(C.c_float)), ("rtotal", C.c_int64), ("ess_frac", C.c_float),
+                ("soff", C.c_int)]
 
 
 class OrcEstimate(C.Structure):
@@ -100,6 +101,7 @@ def _declare(L):
                                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                       C.c_uint32, C.c_uint32, fp]),
         "orc_filter_free": (None, [C.POINTER(OrcFilter)]),
+        "orc_filter_set_stream_offset": (C.c_int, [C.POINTER(OrcFilter), C.c_int]),
         "orc_filter_step": (C.c_int, [C.POINTER(OrcFilter), fp, fp, C.POINTER(OrcEstimate), ip, C.c_int]),
         "orc_filter_sample": (C.c_int, [C.POINTER(OrcFilter), fp, fp, C.POINTER(OrcEstimate), C.c_int]),
         "orc_filter_resample": (C.c_int, [C.POINTER(OrcFilter), ip, C.c_int]),
@@ -378,6 +380,11 @@ class Filter:
         sel = np.zeros(self.m * self.N, np.int32)
         lib().orc_filter_resample(C.byref(self.f), _i(sel), threads)
         return sel
+
+    def set_stream_offset(self, off):
+        """Sub-filter b draws the stream of a larger filter's sub-filter off + b."""
+        if lib().orc_filter_set_stream_offset(C.byref(self.f), off) != 0:
+            raise ValueError("stream offsets need one stream per sub-filter")
 
     def set_sorted(self, soa, keys):
         """Replace the sorted copy (S x T states, T keys) between sample() and resample()."""

@@ -663,6 +663,16 @@ int orc_filter_init(orc_filter* f, const orc_model* mdl, int m, int N, int t, in
     return 0;
 }
 
+int orc_filter_set_stream_offset(orc_filter* f, int off)
+{
+    if (f->rng != ORC_RNG_SUBFILTER || off < 0) return -1;
+    f->soff = off;
+    for (int b = 0; b < f->N; ++b)
+        orc_mtgp_init_state(f->mtgp + (int64_t)b * ORC_MTGP_N, (off + b) % ORC_MTGP_SETS,
+                            f->seed + (uint32_t)(off + b) + 1u);
+    return 0;
+}
+
 void orc_filter_free(orc_filter* f)
 {
     free(f->state); free(f->tmp); free(f->tkey); free(f->mtgp); free(f->rbuf);
@@ -699,7 +709,7 @@ int orc_filter_sample(orc_filter* f, const float* control, const float* meas, or
 #pragma omp parallel for num_threads(threads) schedule(static)
         for (int b = 0; b < N; ++b) {
             float* buf = f->rbuf + (int64_t)b * draws;
-            orc_mtgp_generate(f->mtgp + (int64_t)b * ORC_MTGP_N, b % ORC_MTGP_SETS, f->mask, 1, draws,
+            orc_mtgp_generate(f->mtgp + (int64_t)b * ORC_MTGP_N, (f->soff + b) % ORC_MTGP_SETS, f->mask, 1, draws,
                               (uint32_t*)buf);
             orc_boxmuller(buf, nb);
         }

@@ -169,6 +169,8 @@ typedef struct {
     float ess_frac;   /* > 0: a sub-filter resamples only while (sum w)^2 / sum w^2 < ess_frac * m
                          (the reference's ADAPTIVE_RESAMPLING test, resampling-valias.cl:273-284,
                          with its threshold thr = 1 / (ess_frac * m)); 0 after init */
+    int soff;         /* ORC_RNG_SUBFILTER: sub-filter b draws the stream of a whole filter's
+                         sub-filter soff + b (orc_filter_set_stream_offset); 0 after init */
 } orc_filter;
 
 typedef struct {
@@ -194,6 +196,11 @@ int orc_filter_step(orc_filter* f, const float* control, const float* meas,
  * resampling from tmp / tkey with this step's uniforms into state.  A test
  * may replace tmp / tkey in between (e.g. with a device's own sorted copy) to
  * check exchange routing and resampling given identical weights. */
+/* ORC_RNG_SUBFILTER: re-seed so that sub-filter b draws stream off + b
+ * (parameter set (off + b) mod 200, seed + off + b + 1), the streams of rows
+ * of a larger filter that starts at sub-filter off.  Returns -1 for the
+ * reference layout. */
+int orc_filter_set_stream_offset(orc_filter* f, int off);
 int orc_filter_sample(orc_filter* f, const float* control, const float* meas,
                       orc_estimate* est, int threads);
 int orc_filter_resample(orc_filter* f, int32_t* sel, int threads);

@@ -156,3 +156,78 @@ def test_move_filters_between_ranks():
         if p.is_alive():
             p.kill()
     assert all(v is True for v in res.values()), res
+
+
+def _oracle_shard_rank(rank, world, port, N, m, t, res, steps, q):
+    """One rank of the oracle filter split by rows: its own sub-filters with
+    their whole-filter streams, the halos of the neighbouring ranks through
+    halo_exchange, the exchange applied to its sorted copy, then resampling."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+        import sys
+        sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+        import oracle as O
+        import workload as Wk
+        from esthera_b200.sharding import TorusShard, halo_exchange
+        p = Wk.params(0, 5)
+        control, meas, _, _ = Wk.make_trace(0, p, 5, steps)
+        md = O.model_from_params(0, p)
+        sh = TorusShard(N, m, t, world, rank)
+        f = O.Filter(md, m, sh.num_subfilters, t, O.EXCH_NONE, res, O.RNG_SUBFILTER, 96, 4, 1, 1.0, 0xF000000D, 0,
+                     np.array(p.init_state[:3], np.float32))
+        f.set_stream_offset(sh.first_subfilter)
+        tt = lambda h: (torch.from_numpy(np.ascontiguousarray(h[0])), torch.from_numpy(np.ascontiguousarray(h[1])))
+        for k in range(steps):
+            f.sample(control[k], meas[k], threads=1)
+            s, kk = f.sorted()
+            up, down = sh.halos_out(s, kk)
+            fu, fd = halo_exchange(dist, sh, tt(up), tt(down))
+            es, ek = sh.apply_exchange(s, kk, (fu[0].numpy(), fu[1].numpy()), (fd[0].numpy(), fd[1].numpy()))
+            f.set_sorted(es, ek)
+            f.resample(threads=1)
+        out = (rank, sh.first_subfilter, f.state())
+        f.close()
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put(out)
+    except Exception as e:  # report, never hang the parent
+        q.put((rank, repr(e), None))
+
+
+@pytest.mark.parametrize("world,N,t,res", [(2, 64, 2, 1), (2, 128, 1, 2), (4, 128, 1, 0)])
+def test_sharded_oracle_filter_matches_whole(world, N, t, res):
+    """The row-sharded step (per-rank streams at their whole-filter offsets,
+    halo rows between neighbouring ranks, no collective over particles) gives
+    the whole filter's particles bit for bit, through gloo ranks on CPU."""
+    import multiprocessing as mp
+    import oracle as O
+    import workload as Wk
+    m, steps = 64, 4
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_oracle_shard_rank, args=(r, world, port, N, m, t, res, steps, q))
+             for r in range(world)]
+    for pr in procs:
+        pr.start()
+    got = [q.get(timeout=240) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+    for g in got:
+        assert g[2] is not None, g[1]
+    p = Wk.params(0, 5)
+    control, meas, _, _ = Wk.make_trace(0, p, 5, steps)
+    md = O.model_from_params(0, p)
+    f = O.Filter(md, m, N, t, O.EXCH_TORUS, res, O.RNG_SUBFILTER, 96, 4, 1, 1.0, 0xF000000D, 0,
+                 np.array(p.init_state[:3], np.float32))
+    for k in range(steps):
+        f.step(control[k], meas[k], threads=1)
+    whole = f.state()
+    f.close()
+    for rank, b0, st in got:
+        assert np.array_equal(st, whole[:, b0 * m:b0 * m + st.shape[1]]), rank
