@@ -167,6 +167,7 @@ def _declare(L):
         "pf_batch_info": (C.c_int, [P, ip, C.POINTER(C.c_int64), ip, ip, C.POINTER(C.c_int64)]),
         "pf_batch_filter_info": (C.c_int, [P, C.c_int32, ip, ip, C.POINTER(C.c_int64)]),
         "pf_batch_get_sorted": (C.c_int, [P, C.c_int32, fp, fp]),
+        "pf_batch_filter_shape": (C.c_int, [P, C.c_int32, ip, ip]),
         "pf_batch_autotune": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, P, fp, C.c_int32,
                                         C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32, C.c_float,
                                         C.POINTER(TuneEntry), C.c_int32, ip, C.POINTER(PFConfig)]),
@@ -599,6 +600,12 @@ class FilterBatch:
         n, so, po = C.c_int32(), C.c_int32(), C.c_int64()
         check(lib().pf_batch_filter_info(self._h, f, C.byref(n), C.byref(so), C.byref(po)))
         return {"num_subfilters": n.value, "stream_offset": so.value, "particle_offset": po.value}
+
+    def filter_shape(self, f):
+        """(sub-filter size m_f, particles per thread) of filter f."""
+        m, e = C.c_int32(), C.c_int32()
+        check(lib().pf_batch_filter_shape(self._h, f, C.byref(m), C.byref(e)))
+        return m.value, e.value
 
     def set_initial_states(self, states):
         a = _f32(states).reshape(self.F, self.num_state)

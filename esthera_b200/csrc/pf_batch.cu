@@ -1,13 +1,16 @@
 // pf_batch.cu -- batched filters (include/esthera_b200.h, pf_batch_*): many
 // independent filters of uneven particle counts stepped by one sequence of
-// launches.  All filters share the model, the sub-filter size m, the
-// resampler and the exchange settings; each has its own particle count (a
-// multiple of m), model parameters, MTGP32 streams, inputs and estimates.
+// launches.  All filters share the model, the resampler and the exchange
+// settings; each has its own particle count, model parameters, MTGP32
+// streams, inputs and estimates.  The configured sub-filter size m is an upper
+// bound: filter f runs sub-filters of m_f particles, the largest power of two
+// <= m that divides its count (and, for the torus, gives a valid grid).
 //
-// One CTA per sub-filter of every filter: a CTA -> (filter, sub-filter) map
-// drives the split pipeline's two kernels (k_sample_sort, k_exchange_resample)
-// over the whole batch, the exchange stays inside each filter, and a run of
-// many steps is captured once into a CUDA graph and replayed by one launch.
+// One CTA per sub-filter of every filter: per sub-filter size, a CTA ->
+// (filter, sub-filter) map drives the split pipeline's two kernels
+// (k_sample_sort, k_exchange_resample) over that size's filters, the exchange
+// stays inside each filter, and a run of many steps is captured once into a
+// CUDA graph and replayed by one launch.
 // Sub-filter b of filter f draws from stream stream_offset + first(f) + b,
 // first(f) = the number of sub-filters of filters 0..f-1, so filter f alone
 // (pf_create with that stream offset) reproduces its batched results exactly.
@@ -46,13 +49,17 @@ struct pf_batch {
     int model = 0;
     ModelInfo mi{};
     ModelOps ops{};
-    int F = 0, M = 0, E = 0, S = 0, t = 0;
+    int F = 0, M = 0, E = 0, S = 0, t = 0;  // M, E: the configured (largest) sub-filter size and its ppt
     int64_t P = 0;   // particles in all filters
     int NS = 0;      // sub-filters in all filters
     std::vector<int32_t> nsub, sub_off, grp_off;  // grp_off: first estimate group (32 sub-filters) of a filter
-    std::vector<int64_t> part_off;
+    std::vector<int32_t> mf;                      // each filter's sub-filter size
+    std::vector<int64_t> part_off, ru_off;
+    struct Group {
+        int M, E, NS, map_off;  // one sub-filter size: its ppt, sub-filters and first map entry
+    };
+    std::vector<Group> groups;
     std::vector<ModelParams> mp;
-    int64_t nbm = 0, draws = 0;
     cudaStream_t stream = nullptr;
     std::vector<void*> allocs;
     int64_t dev_bytes = 0;
@@ -115,18 +122,20 @@ static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate
     memset(&D, 0, sizeof(D));
     const int64_t p0 = B->part_off[f];
     const int64_t s0 = B->sub_off[f];
-    const int N = B->nsub[f];
-    D.T = (int64_t)B->M * N;
+    const int N = B->nsub[f], M = B->mf[f];
+    const int64_t nbm = 2 * (((int64_t)B->mi.K * M + 1) / 2);
+    const int64_t draws = nbm + 1 + resample_draws(B->cfg.resampler, M);
+    D.T = (int64_t)M * N;
     D.state = B->state + (int64_t)B->S * p0;
     D.tmp = B->tmp + (int64_t)B->S * p0;
     D.tkey = B->tkey + p0;
     D.winner = B->winner + s0;
     D.part = B->part + s0 * kPartStride;
     D.mtgp = B->mtgp + s0 * kMtgpN;
-    D.ru = B->ru + s0 * (B->draws - B->nbm);
+    D.ru = B->ru + B->ru_off[f];
     D.est = est;
     D.N = N;
-    D.M = B->M;
+    D.M = M;
     D.t = B->t;
     D.exchange = B->cfg.exchange;
     D.resampler = B->cfg.resampler;
@@ -134,9 +143,9 @@ static void fill_batch_desc(const pf_batch* B, int f, FilterDesc& D, pf_estimate
     D.log_weights = B->cfg.log_weights ? 1 : 0;
     D.inplace = (B->cfg.resampling_freq < 1.0f || B->cfg.ess_fraction > 0.0f) ? 1 : 0;
     D.rng_fused = 1;
-    D.draws = (int32_t)B->draws;
-    D.nbm = (int32_t)B->nbm;
-    D.ru_stride = (int32_t)(B->draws - B->nbm);
+    D.draws = (int32_t)draws;
+    D.nbm = (int32_t)nbm;
+    D.ru_stride = (int32_t)(draws - nbm);
     D.mask = B->cfg.mtgp_mask;
     D.stream_base = B->cfg.stream_offset + (int32_t)s0;
     D.exch_period = B->cfg.exchange_period;
@@ -176,11 +185,14 @@ static pf_status batch_status(int32_t st)
 
 static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRef in, int32_t* ctr_inc)
 {
-    const int M = B->M, E = B->E;
-    CU(B->ops.sample_sort(M, E, true, B->NS, B->stream, desc, B->map, in));
-    // a programmatic dependent of the sampling kernel when that pays (starts in its last wave, waits for the grid)
-    const int virt = dependent_launch_pays((int)B->NS, M, E, B->mi.S, B->cfg.device) ? 3 : 1;
-    CU(B->ops.exchange_resample(M, E, B->cfg.resampler, B->NS, B->stream, desc, B->map, in, nullptr, virt));
+    for (const pf_batch::Group& g : B->groups) {
+        const int2* map = B->map + g.map_off;
+        CU(B->ops.sample_sort(g.M, g.E, true, g.NS, B->stream, desc, map, in));
+        // a programmatic dependent of the sampling kernel when that pays (starts in its last wave, waits for
+        // the grid)
+        const int virt = dependent_launch_pays(g.NS, g.M, g.E, B->mi.S, B->cfg.device) ? 3 : 1;
+        CU(B->ops.exchange_resample(g.M, g.E, B->cfg.resampler, g.NS, B->stream, desc, map, in, nullptr, virt));
+    }
     if (ctr_inc) CU(launch_counter_inc(ctr_inc, B->stream));
     return PF_OK;
 }
@@ -220,18 +232,27 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     if (cfg->stream_offset < 0 || cfg->exchange_period < 0)
         return fail(PF_ERR_INVALID, "stream_offset and exchange_period must be >= 0");
     int64_t P = 0, NS = 0;
+    std::vector<int32_t> mf(num_filters);
     for (int f = 0; f < num_filters; ++f) {
         const int32_t n = num_particles[f];
-        if (n < M || n % M) return fail(PF_ERR_INVALID, "filter %d: %d particles is not a multiple of m=%d", f, n, M);
-        const int N = n / M;
-        if (cfg->exchange == PF_EXCHANGE_TORUS) {
-            int dx, dy;
-            torus_dims(N, &dx, &dy);
-            if (dx * dy != N)
-                return fail(PF_ERR_INVALID, "filter %d: torus exchange needs N = dx*dy (N=%d)", f, N);
+        // the largest power of two m' <= m dividing n whose grid and exchange fit
+        int mm = 0;
+        for (int c = M; c >= 32 && !mm; c >>= 1) {
+            if (n < c || n % c) continue;
+            if (cfg->exchange == PF_EXCHANGE_TORUS) {
+                int dx, dy;
+                torus_dims(n / c, &dx, &dy);
+                if (dx * dy != n / c || 5 * cfg->num_transfer > c) continue;
+            }
+            if (cfg->exchange == PF_EXCHANGE_RING && 2 * cfg->num_transfer > c) continue;
+            mm = c;
         }
+        if (!mm)
+            return fail(PF_ERR_INVALID, "filter %d: no sub-filter size in [32, %d] divides %d particles%s", f, M, n,
+                        cfg->exchange == PF_EXCHANGE_TORUS ? " into a torus" : "");
+        mf[f] = mm;
         P += n;
-        NS += N;
+        NS += n / mm;
     }
     if (NS > INT32_MAX / 2 || P > ((int64_t)1 << 34)) return fail(PF_ERR_INVALID, "batch too large");
     pf_status s = require_gpu(cfg->device);
@@ -254,13 +275,17 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     B->part_off.resize(num_filters);
     B->grp_off.resize(num_filters);
     B->mp.resize(num_filters);
-    int64_t po = 0;
+    B->mf = mf;
+    B->ru_off.resize(num_filters);
+    int64_t po = 0, ro = 0;
     int so = 0, go = 0;
     for (int f = 0; f < num_filters; ++f) {
-        B->nsub[f] = num_particles[f] / M;
+        B->nsub[f] = num_particles[f] / mf[f];
         B->sub_off[f] = so;
         B->part_off[f] = po;
         B->grp_off[f] = go;
+        B->ru_off[f] = ro;
+        ro += (int64_t)B->nsub[f] * (1 + resample_draws(cfg->resampler, mf[f]));
         so += B->nsub[f];
         go += (B->nsub[f] + 31) / 32;
         po += num_particles[f];
@@ -280,8 +305,17 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
             }
         }
     }
-    B->nbm = 2 * (((int64_t)mi.K * M + 1) / 2);
-    B->draws = B->nbm + 1 + resample_draws(cfg->resampler, M);
+    // one group of launches per sub-filter size, the largest first
+    for (int c = M; c >= 32; c >>= 1) {
+        int ns = 0;
+        for (int f = 0; f < num_filters; ++f)
+            if (mf[f] == c) ns += B->nsub[f];
+        if (!ns) continue;
+        const int ec = c == M ? E : (cfg->particles_per_thread > 0 && me_supported(c, cfg->particles_per_thread)
+                                         ? cfg->particles_per_thread
+                                         : default_ppt(c));
+        B->groups.push_back(pf_batch::Group{c, ec, ns, 0});
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         release(B);
@@ -301,7 +335,7 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     TRY(balloc(B, &B->winner, (size_t)NS));
     TRY(balloc(B, &B->part, (size_t)NS * kPartStride));
     TRY(balloc(B, &B->mtgp, (size_t)NS * kMtgpN));
-    TRY(balloc(B, &B->ru, (size_t)NS * (B->draws - B->nbm)));
+    TRY(balloc(B, &B->ru, (size_t)ro));
     TRY(balloc(B, &B->gpart, (size_t)go * kPartStride));
     TRY(balloc(B, &B->est_ctr, (size_t)num_filters));
     TRY(balloc(B, &B->ctr, 1));
@@ -316,15 +350,21 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
     }
     {
-        // group leaders (sub-filters 0, 32, 64, ... of each filter) first: the
-        // resampling kernel's CTAs that combine the estimates run in its first wave
+        // per sub-filter size, group leaders (sub-filters 0, 32, 64, ... of each
+        // filter) first: the resampling kernel's CTAs that combine the
+        // estimates run in its first wave
         std::vector<int2> map;
         map.reserve((size_t)NS);
-        for (int f = 0; f < num_filters; ++f)
-            for (int b = 0; b < B->nsub[f]; b += 32) map.push_back(make_int2(f, b));
-        for (int f = 0; f < num_filters; ++f)
-            for (int b = 0; b < B->nsub[f]; ++b)
-                if (b & 31) map.push_back(make_int2(f, b));
+        for (pf_batch::Group& g : B->groups) {
+            g.map_off = (int)map.size();
+            for (int f = 0; f < num_filters; ++f)
+                if (mf[f] == g.M)
+                    for (int b = 0; b < B->nsub[f]; b += 32) map.push_back(make_int2(f, b));
+            for (int f = 0; f < num_filters; ++f)
+                if (mf[f] == g.M)
+                    for (int b = 0; b < B->nsub[f]; ++b)
+                        if (b & 31) map.push_back(make_int2(f, b));
+        }
         if (cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
             launch_mtgp_init(B->mtgp, (int)NS, cfg->stream_offset, cfg->seed, B->stream) != cudaSuccess ||
             cudaStreamSynchronize(B->stream) != cudaSuccess) {
@@ -385,7 +425,7 @@ extern "C" pf_status pf_batch_get_particles(pf_batch* B, int32_t filter, float* 
     if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
     CU(cudaSetDevice(B->cfg.device));
     CU(cudaStreamSynchronize(B->stream));
-    const int64_t T = (int64_t)B->M * B->nsub[filter];
+    const int64_t T = (int64_t)B->mf[filter] * B->nsub[filter];
     for (int v = 0; v < B->S; ++v)
         CU(cudaMemcpy(soa + v * T, B->state + (int64_t)B->S * B->part_off[filter] + v * T, (size_t)T * 4,
                       cudaMemcpyDeviceToHost));
@@ -524,13 +564,26 @@ extern "C" pf_status pf_batch_filter_info(pf_batch* B, int32_t filter, int32_t* 
     return PF_OK;
 }
 
+extern "C" pf_status pf_batch_filter_shape(pf_batch* B, int32_t filter, int32_t* particles_per_subfilter,
+                                           int32_t* particles_per_thread)
+{
+    if (!B) return fail(PF_ERR_INVALID, "null argument");
+    if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
+    for (const pf_batch::Group& g : B->groups)
+        if (g.M == B->mf[filter]) {
+            if (particles_per_subfilter) *particles_per_subfilter = g.M;
+            if (particles_per_thread) *particles_per_thread = g.E;
+        }
+    return PF_OK;
+}
+
 extern "C" pf_status pf_batch_get_sorted(pf_batch* B, int32_t filter, float* soa, float* keys)
 {
     if (!B || !soa || !keys) return fail(PF_ERR_INVALID, "null argument");
     if (filter < 0 || filter >= B->F) return fail(PF_ERR_INVALID, "filter %d out of range", filter);
     CU(cudaSetDevice(B->cfg.device));
     CU(cudaStreamSynchronize(B->stream));
-    const int64_t T = (int64_t)B->M * B->nsub[filter];
+    const int64_t T = (int64_t)B->mf[filter] * B->nsub[filter];
     const int64_t p0 = B->part_off[filter];
     for (int v = 0; v < B->S; ++v)
         CU(cudaMemcpy(soa + v * T, B->tmp + (int64_t)B->S * p0 + v * T, (size_t)T * 4, cudaMemcpyDeviceToHost));

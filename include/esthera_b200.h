@@ -322,14 +322,19 @@ pf_status pf_shard_estimate(pf_filter* f, const double* rows, const float* state
 
 /* ---- batched filters: many independent filters of uneven sizes stepped together ----
  * The reference runs one filter per process (particle_filter, pf_generic_soa.cu:686);
- * these calls have no counterpart there.  Every filter shares cfg's model, m,
+ * these calls have no counterpart there.  Every filter shares cfg's model,
  * resampler and exchange settings (exchange stays inside each filter: none,
  * ring, or torus when every filter's N = dx*dy; all-to-all is not offered) and
  * runs the split pipeline with per-sub-filter streams.  Filter f has
- * num_particles[f] particles (a positive multiple of m) and params + f
- * (params_size bytes each); its sub-filter b uses stream cfg.stream_offset +
+ * num_particles[f] particles and params + f (params_size bytes each).  cfg's m
+ * is the largest sub-filter size: filter f runs sub-filters of m_f particles,
+ * the largest power of two in [32, m] that divides num_particles[f] (and for
+ * the torus gives N = dx*dy and 5t <= m_f; for the ring 2t <= m_f), with cfg's
+ * particles per thread where that is built for m_f, else the default
+ * (pf_batch_filter_shape).  Its sub-filter b uses stream cfg.stream_offset +
  * first(f) + b, first(f) = sub-filters of filters 0..f-1 (pf_batch_filter_info),
- * so a pf_filter created with that stream_offset reproduces filter f exactly. */
+ * so a pf_filter created with that stream_offset, m_f and ppt reproduces
+ * filter f exactly. */
 typedef struct pf_batch pf_batch;
 pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, int32_t num_filters,
                           const int32_t* num_particles, const void* params, size_t params_size, pf_batch** out);
@@ -354,6 +359,9 @@ pf_status pf_batch_info(pf_batch* b, int32_t* num_filters, int64_t* total_partic
                         int32_t* particles_per_thread, int64_t* device_bytes);
 pf_status pf_batch_filter_info(pf_batch* b, int32_t filter, int32_t* num_subfilters, int32_t* stream_offset,
                                int64_t* particle_offset);
+/* Filter f's sub-filter size m_f and particles per thread. */
+pf_status pf_batch_filter_shape(pf_batch* b, int32_t filter, int32_t* particles_per_subfilter,
+                                int32_t* particles_per_thread);
 /* Filter f's sorted (pre-exchange) particles and keys of the last step (host, SoA). */
 pf_status pf_batch_get_sorted(pf_batch* b, int32_t filter, float* soa, float* keys);
 

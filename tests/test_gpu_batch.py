@@ -58,6 +58,34 @@ def test_batch_equals_single_filters(gpu, m, ppt, exch, t, period, res, counts):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("m,exch,t,res", [(1024, 1, 2, 1), (512, 2, 1, 2), (1024, 0, 0, 0)])
+def test_mixed_subfilter_sizes_equal_single_filters(gpu, m, exch, t, res):
+    """m is an upper bound: each filter runs the largest power-of-two
+    sub-filter size that divides its count (and fits the torus), in one launch
+    group per size, and still equals the same filter run alone."""
+    E = gpu
+    counts = [256, 768, 1536, 4096, 5120, 96, 1024]
+    steps = 5
+    params, inputs, _ = batch_setup(E, counts, steps)
+    cfg = dict(num_transfer=t, exchange=exch, resampler=res, particles_per_thread=4)
+    B = E.FilterBatch(UNI, params, counts, particles_per_subfilter=m, **cfg)
+    shapes = [B.filter_shape(f) for f in range(len(counts))]
+    for n, (mf, ppt) in zip(counts, shapes):
+        assert mf <= m and n % mf == 0 and (2 * mf > m or n % (2 * mf) != 0 or exch == 2)
+    assert len({mf for mf, _ in shapes}) >= 3
+    best = [B.step(inputs[:, k]) for k in range(steps)]
+    for f, n in enumerate(counts):
+        mf, ppt = shapes[f]
+        fi = B.filter_info(f)
+        assert fi["num_subfilters"] == n // mf
+        c = dict(cfg, particles_per_thread=ppt)
+        s = single(E, params[f], c, fi["stream_offset"], n, mf)
+        for k in range(steps):
+            assert same_estimate(best[k][f], s.step(inputs[f, k])), (f, k)
+        assert np.array_equal(B.particles(f), s.particles()), f
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("period", [1, 2])
 def test_batch_graph_equals_host_steps(gpu, period):
     """pf_batch_submit (graph of many steps, device counter) == pf_batch_step."""
@@ -138,7 +166,7 @@ def test_batch_rejects_bad_shapes(E):
         EB.FilterBatch(UNI, p, [256, 512], particles_per_subfilter=256, exchange=3)
     assert ei.value.status == EB.PF_ERR_UNSUPPORTED
     with pytest.raises(EB.PFError) as ei:
-        EB.FilterBatch(UNI, p, [256, 7 * 256], particles_per_subfilter=256, exchange=2)
+        EB.FilterBatch(UNI, p, [256, 5 * 32], particles_per_subfilter=256, exchange=2)  # 5 sub-filters of 32
     assert ei.value.status == EB.PF_ERR_INVALID
 
 
@@ -150,14 +178,11 @@ def test_batch_autotune(gpu):
     counts = [256, 768, 1536, 512]
     steps = 12
     params, inputs, truth = batch_setup(E, counts, steps)
-    best, rows = E.batch_autotune(UNI, params, counts, inputs, truth, m_list=(128, 256, 512), ppt_list=(2, 4),
+    best, rows = E.batch_autotune(UNI, params, counts, inputs, truth, m_list=(128, 256, 512, 1024), ppt_list=(2, 4),
                                   period_list=(1, 2), burn_in=2, rmse_tol=0.5, num_transfer=1, exchange=1)
-    assert len(rows) == 3 * 2 * 2
-    for r in rows:
-        if r["particles_per_subfilter"] == 512:      # 768 is not a multiple of 512
-            assert r["status"] == E.PF_ERR_INVALID and not r["accepted"]
-        else:
-            assert r["status"] == E.PF_OK and r["ms_per_step"] > 0 and np.isfinite(r["rmse"])
+    assert len(rows) == 4 * 2 * 2
+    for r in rows:  # m = 512 / 1024 cap each filter's sub-filters at a size dividing its count
+        assert r["status"] == E.PF_OK and r["ms_per_step"] > 0 and np.isfinite(r["rmse"])
     ok = [r for r in rows if r["accepted"]]
     pick = max(ok, key=lambda r: r["particle_steps_per_s"])
     assert (best.particles_per_subfilter, best.particles_per_thread, best.exchange_period) == (
