@@ -267,9 +267,12 @@ def reference_arm(args, rank, world):
 def run_batched(E, torch, args, local):
     """Batched uneven filters: 4096 unicycle filters, counts log-uniform over
     [256, 65536] rounded to 256, 200 steps, one graph-captured launch per run;
-    m / particles per thread / exchange period picked by pf_batch_autotune on a
-    256-filter slice; compared with looping the plain single-filter path
-    (pf_step per filter and step) over a sample of the same filters."""
+    largest sub-filter size / particles per thread / threads per particle /
+    exchange period picked by pf_batch_autotune on a 256-filter slice (each
+    filter runs the largest sub-filter size up to the picked one that divides
+    its count); compared with looping the plain single-filter path (pf_step per
+    filter and step, each filter's own sub-filter size) over a sample of the
+    same filters."""
     from esthera_b200 import workloads as W
     steps = args.batch_steps
     counts, params, inputs, truth = W.batched_unicycle(args.batch_filters, steps)
@@ -280,13 +283,16 @@ def run_batched(E, torch, args, local):
     sl = np.arange(0, F, max(1, F // 256))[:256]
     t0 = time.time()
     best, table = E.batch_autotune(E.MODEL_UNICYCLE, [params[i] for i in sl], counts[sl], inputs[sl, :16],
-                                   truth[sl, :16], m_list=(128, 256, 512, 1024), ppt_list=(1, 2, 4, 8),
+                                   truth[sl, :16], m_list=(128, 256, 512, 1024), ppt_list=(2, 4), tpp_list=(1, 2),
                                    period_list=(1, 2, 4), burn_in=4, rmse_tol=0.02, **base)
     tune_s = time.time() - t0
     cfg = dict(base, particles_per_subfilter=best.particles_per_subfilter,
-               particles_per_thread=best.particles_per_thread, exchange_period=best.exchange_period)
+               particles_per_thread=best.particles_per_thread, threads_per_particle=best.threads_per_particle,
+               exchange_period=best.exchange_period)
     B = E.FilterBatch(E.MODEL_UNICYCLE, params, counts, **cfg)
     info = B.info()
+    shapes = [B.filter_shape(f) for f in range(F)]
+    offsets = [B.filter_info(f)["stream_offset"] for f in range(F)]
     d_in = torch.from_numpy(np.ascontiguousarray(inputs).view(np.uint8).reshape(-1).copy()).cuda()
     d_est = torch.zeros(F * steps * E.ESTIMATE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.ExternalStream(B.stream(), device=torch.device("cuda", local))
@@ -317,21 +323,23 @@ def run_batched(E, torch, args, local):
         ev1.synchronize()
         lat.append(ev0.elapsed_time(ev1))
     B.close()
-    # plain path: one filter at a time through pf_step (same m, ppt, period and
-    # streams, so the results are identical to the batched ones)
+    # plain path: one filter at a time through pf_step (each filter's own m and
+    # ppt, the same period and streams, so the results are identical to the
+    # batched ones)
     sample = np.arange(0, F, max(1, F // args.plain_sample))[:args.plain_sample]
     plain_s, plain_ps, same = 0.0, 0, True
-    warm = E.ParticleFilter(E.MODEL_UNICYCLE, params[0], particles_per_subfilter=cfg["particles_per_subfilter"],
-                            num_subfilters=1, pipeline=E.PIPELINE_SPLIT,
-                            **{k: v for k, v in cfg.items() if k != "particles_per_subfilter"})
-    warm.step(inputs[0, 0])  # loads the kernels once; every sampled filter below starts fresh
-    warm.close()
+    rest = {k: v for k, v in cfg.items() if k not in ("particles_per_subfilter", "particles_per_thread")}
+    for mf, e in sorted(set(shapes)):  # load each kernel once; every sampled filter below starts fresh
+        warm = E.ParticleFilter(E.MODEL_UNICYCLE, params[0], particles_per_subfilter=mf, particles_per_thread=e,
+                                num_subfilters=1, pipeline=E.PIPELINE_SPLIT, **rest)
+        warm.step(inputs[0, 0])
+        warm.close()
     for i in sample:
         n = int(counts[i])
-        f = E.ParticleFilter(E.MODEL_UNICYCLE, params[i], particles_per_subfilter=cfg["particles_per_subfilter"],
-                             num_subfilters=n // cfg["particles_per_subfilter"], pipeline=E.PIPELINE_SPLIT,
-                             stream_offset=int(np.sum(counts[:i] // cfg["particles_per_subfilter"])),
-                             **{k: v for k, v in cfg.items() if k != "particles_per_subfilter"})
+        mf, e = shapes[i]
+        f = E.ParticleFilter(E.MODEL_UNICYCLE, params[i], particles_per_subfilter=mf, particles_per_thread=e,
+                             num_subfilters=n // mf, pipeline=E.PIPELINE_SPLIT, stream_offset=int(offsets[i]),
+                             **rest)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for k in range(steps):
@@ -350,7 +358,10 @@ def run_batched(E, torch, args, local):
                                "%d steps in one graph launch" % (F, P, steps),
                    "filters": F, "particles": P, "subfilters": info["total_subfilters"],
                    "particles_per_subfilter": cfg["particles_per_subfilter"],
-                   "particles_per_thread": cfg["particles_per_thread"], "exchange_period": cfg["exchange_period"],
+                   "subfilter_sizes": {str(mf): int(sum(1 for s in shapes if s[0] == mf))
+                                       for mf in sorted({s[0] for s in shapes})},
+                   "particles_per_thread": cfg["particles_per_thread"],
+                   "threads_per_particle": cfg["threads_per_particle"], "exchange_period": cfg["exchange_period"],
                    "l2": "working set %.1f GB > L2" % (info["device_bytes"] / 1e9)},
         "roofline": {"bound": "hbm", "achieved": ALG_BYTES * P * steps / (run_ms * 1e-3) / 1e9, "unit": "GB/s"},
         "e2e": {"value": P * e2e_steps / (lat.sum() * 1e-3), "unit": "particle-steps/s",
@@ -364,12 +375,10 @@ def run_batched(E, torch, args, local):
         "rmse_xy": {"mean": float(rmse_f.mean()), "p99": float(np.percentile(rmse_f, 99))},
         "autotune": {"seconds": tune_s, "slice": "%d filters x 16 steps" % len(sl),
                      "candidates": [{"m": r["particles_per_subfilter"], "ppt": r["particles_per_thread"],
-                                     "period": r["exchange_period"], "ms_per_step": r["ms_per_step"],
-                                     "rmse": r["rmse"], "accepted": r["accepted"]}
+                                     "tpp": r["threads_per_particle"], "period": r["exchange_period"],
+                                     "ms_per_step": r["ms_per_step"], "rmse": r["rmse"], "accepted": r["accepted"]}
                                     for r in table if r["status"] == 0],
-                     "not_runnable": len([r for r in table if r["status"] != 0]),
-                     "not_runnable_why": "m not dividing every count (512, 1024) or particles per thread "
-                                         "not built for m"},
+                     "not_runnable": len([r for r in table if r["status"] != 0])},
         "gpu_launches": 3 * steps,
     }
 

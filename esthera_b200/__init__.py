@@ -38,7 +38,8 @@ class PFConfig(C.Structure):
                 ("resampling_freq", C.c_float), ("seed", C.c_uint32), ("rng", C.c_int32),
                 ("mtgp_streams", C.c_int32), ("mtgp_mask", C.c_uint32), ("log_weights", C.c_int32),
                 ("pipeline", C.c_int32), ("particles_per_thread", C.c_int32), ("device", C.c_int32),
-                ("stream_offset", C.c_int32), ("exchange_period", C.c_int32), ("ess_fraction", C.c_float)]
+                ("stream_offset", C.c_int32), ("exchange_period", C.c_int32), ("ess_fraction", C.c_float),
+                ("threads_per_particle", C.c_int32)]
 
 
 class StepInput(C.Structure):
@@ -169,7 +170,8 @@ def _declare(L):
         "pf_batch_get_sorted": (C.c_int, [P, C.c_int32, fp, fp]),
         "pf_batch_filter_shape": (C.c_int, [P, C.c_int32, ip, ip]),
         "pf_batch_autotune": (C.c_int, [C.POINTER(PFConfig), C.c_int, C.c_int32, ip, P, C.c_size_t, P, fp, C.c_int32,
-                                        C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32, C.c_float,
+                                        C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32, ip, C.c_int32,
+                                        C.c_float,
                                         C.POINTER(TuneEntry), C.c_int32, ip, C.POINTER(PFConfig)]),
         "pf_server_create": (C.c_int, [C.POINTER(PFConfig), C.c_int64, C.c_int32, C.POINTER(P)]),
         "pf_server_destroy": (C.c_int, [P]),
@@ -775,12 +777,13 @@ def serve_load(filter_config=None, load=None, **load_kw):
 
 class TuneEntry(C.Structure):
     _fields_ = [("particles_per_subfilter", C.c_int32), ("particles_per_thread", C.c_int32),
-                ("exchange_period", C.c_int32), ("status", C.c_int32), ("ms_per_step", C.c_float),
+                ("threads_per_particle", C.c_int32), ("exchange_period", C.c_int32), ("status", C.c_int32),
+                ("ms_per_step", C.c_float),
                 ("accepted", C.c_int32), ("particle_steps_per_s", C.c_double), ("rmse", C.c_double)]
 
 
 def batch_autotune(model, params, counts, inputs, truth=None, m_list=(128, 256, 512, 1024), ppt_list=(1, 2, 4),
-                   period_list=(1, 2, 4), burn_in=0, rmse_tol=0.01, **cfg):
+                   period_list=(1, 2, 4), burn_in=0, rmse_tol=0.01, tpp_list=(1,), **cfg):
     """pf_batch_autotune over host inputs [F][steps] (and truth [F][steps][S]):
     returns (best pf_config, [candidate dicts])."""
     base = default_config(**cfg)
@@ -791,14 +794,15 @@ def batch_autotune(model, params, counts, inputs, truth=None, m_list=(128, 256, 
     inp = np.ascontiguousarray(inputs, STEP_INPUT_DTYPE)
     steps = inp.shape[1]
     tr = None if truth is None else _f32(truth)
-    ml, pl, ql = (np.ascontiguousarray(x, np.int32) for x in (m_list, ppt_list, period_list))
-    cap = len(ml) * len(pl) * len(ql)
+    ml, pl, tl, ql = (np.ascontiguousarray(x, np.int32) for x in (m_list, ppt_list, tpp_list, period_list))
+    cap = len(ml) * len(pl) * len(tl) * len(ql)
     table = (TuneEntry * cap)()
     n = C.c_int32()
     best = PFConfig()
     check(lib().pf_batch_autotune(C.byref(base), model, F, _iptr(counts), C.cast(arr, C.c_void_p), C.sizeof(ptype),
                                   inp.ctypes.data_as(C.c_void_p), None if tr is None else _fptr(tr), steps, burn_in,
-                                  _iptr(ml), len(ml), _iptr(pl), len(pl), _iptr(ql), len(ql), rmse_tol, table, cap,
+                                  _iptr(ml), len(ml), _iptr(pl), len(pl), _iptr(tl), len(tl), _iptr(ql), len(ql),
+                                  rmse_tol, table, cap,
                                   C.byref(n), C.byref(best)))
     rows = [{k: getattr(table[i], k) for k, _ in TuneEntry._fields_} for i in range(n.value)]
     return best, rows

@@ -227,6 +227,7 @@ struct pf_filter {
     ModelInfo mi;
     ModelOps ops;
     int M, E, N, t, dx, dy, streams, na, pipe;
+    int tp = 1;  // threads per particle of the sampling kernel
     StepState X{};
     uint32_t angle_mask;
     int64_t T, rtotal, draws, nbm;
@@ -398,6 +399,12 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
     *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M);
     if (!me_supported(M, *E))
         return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", *E, M);
+    if (c->threads_per_particle < 0 || c->threads_per_particle > 2)
+        return fail(PF_ERR_INVALID, "threads_per_particle must be 1 or 2");
+    if (c->threads_per_particle == 2 &&
+        (c->rng != PF_RNG_SUBFILTER || c->pipeline == PF_PIPELINE_PHASED || 2 * M / *E > 1024))
+        return fail(PF_ERR_UNSUPPORTED, "two threads per particle run the split pipeline with per-sub-filter "
+                                        "streams and 2 m / ppt <= 1024 threads");
     (void)model;
     (void)mi;
     return PF_OK;
@@ -527,7 +534,9 @@ extern "C" pf_status pf_create(const pf_config* cfg, pf_model_id model, const vo
     memcpy(&f->mp, params, params_size);
     f->mi = mi;
     f->ops = model_ops(model);
-    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER && cfg->exchange_period <= 1)
+    f->tp = cfg->threads_per_particle == 2 ? 2 : 1;
+    f->pipe = (cfg->pipeline == PF_PIPELINE_FUSED && cfg->rng == PF_RNG_SUBFILTER && cfg->exchange_period <= 1 &&
+               f->tp == 1)
                   ? PF_PIPELINE_FUSED
                   : (cfg->pipeline == PF_PIPELINE_PHASED ? PF_PIPELINE_PHASED : PF_PIPELINE_SPLIT);
     f->angle_mask = angle_mask_of(model);
@@ -763,7 +772,7 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
             CU(mark("a2a_merge"));
         }
     } else if (f->pipe == PF_PIPELINE_SPLIT) {
-        CU(f->ops.sample_sort(M, E, c.rng == PF_RNG_SUBFILTER, N, st, desc, nullptr, in));
+        CU(f->ops.sample_sort(M, E, f->tp, c.rng == PF_RNG_SUBFILTER, N, st, desc, nullptr, in));
         CU(mark("sample_sort"));
         if (c.exchange == PF_EXCHANGE_ALL2ALL && f->t > 0) {
             CU(launch_a2a_merge(1, desc, st));
@@ -1422,7 +1431,7 @@ extern "C" pf_status pf_shard_sample(pf_filter* f, const pf_step_input* in)
     *f->h_in = *in;
     CU(cudaMemcpyAsync(f->d_in, f->h_in, sizeof(pf_step_input), cudaMemcpyHostToDevice, f->stream));
     InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
-    CU(f->ops.sample_sort(f->M, f->E, true, f->N, f->stream, f->d_desc, nullptr, ir));
+    CU(f->ops.sample_sort(f->M, f->E, f->tp, true, f->N, f->stream, f->d_desc, nullptr, ir));
     CU(launch_shard_pack(f->d_desc, f->halo_out, f->mi.S, f->dx * f->t, f->stream));
     CU(cudaEventRecord(f->ev_sampled, f->stream));
     return PF_OK;

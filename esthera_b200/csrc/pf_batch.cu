@@ -56,7 +56,7 @@ struct pf_batch {
     std::vector<int32_t> mf;                      // each filter's sub-filter size
     std::vector<int64_t> part_off, ru_off;
     struct Group {
-        int M, E, NS, map_off;  // one sub-filter size: its ppt, sub-filters and first map entry
+        int M, E, TP, NS, map_off;  // one sub-filter size: ppt, threads per particle, sub-filters, first map entry
     };
     std::vector<Group> groups;
     std::vector<ModelParams> mp;
@@ -187,7 +187,7 @@ static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRe
 {
     for (const pf_batch::Group& g : B->groups) {
         const int2* map = B->map + g.map_off;
-        CU(B->ops.sample_sort(g.M, g.E, true, g.NS, B->stream, desc, map, in));
+        CU(B->ops.sample_sort(g.M, g.E, g.TP, true, g.NS, B->stream, desc, map, in));
         // a programmatic dependent of the sampling kernel when that pays (starts in its last wave, waits for
         // the grid)
         const int virt = dependent_launch_pays(g.NS, g.M, g.E, B->mi.S, B->cfg.device) ? 3 : 1;
@@ -231,6 +231,11 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         return fail(PF_ERR_INVALID, "ess_fraction must be in [0, 1]");
     if (cfg->stream_offset < 0 || cfg->exchange_period < 0)
         return fail(PF_ERR_INVALID, "stream_offset and exchange_period must be >= 0");
+    if (cfg->threads_per_particle < 0 || cfg->threads_per_particle > 2)
+        return fail(PF_ERR_INVALID, "threads_per_particle must be 1 or 2");
+    if (cfg->threads_per_particle == 2 && 2 * M / E > 1024)
+        return fail(PF_ERR_UNSUPPORTED, "two threads per particle need 2 m / ppt <= 1024 threads (m=%d, ppt=%d)", M,
+                    E);
     int64_t P = 0, NS = 0;
     std::vector<int32_t> mf(num_filters);
     for (int f = 0; f < num_filters; ++f) {
@@ -314,7 +319,9 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         const int ec = c == M ? E : (cfg->particles_per_thread > 0 && me_supported(c, cfg->particles_per_thread)
                                          ? cfg->particles_per_thread
                                          : default_ppt(c));
-        B->groups.push_back(pf_batch::Group{c, ec, ns, 0});
+        // two threads per particle where the sampling kernel's CTA stays within 1024 threads
+        const int tp = cfg->threads_per_particle == 2 && 2 * c / ec <= 1024 ? 2 : 1;
+        B->groups.push_back(pf_batch::Group{c, ec, tp, ns, 0});
     }
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -592,7 +599,8 @@ extern "C" pf_status pf_batch_get_sorted(pf_batch* B, int32_t filter, float* soa
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner: times every (m, particles per thread, exchange period) candidate
+// Autotuner: times every (m, particles per thread, threads per particle,
+// exchange period) candidate
 // on the caller's inputs and picks the fastest whose tracking error stays
 // within a tolerance of the every-step-exchange candidates.
 // ---------------------------------------------------------------------------
@@ -642,15 +650,18 @@ extern "C" pf_status pf_batch_autotune(const pf_config* base, pf_model_id model,
                                        const int32_t* num_particles, const void* params, size_t params_size,
                                        const pf_step_input* inputs, const float* truth, int32_t steps,
                                        int32_t burn_in, const int32_t* m_list, int32_t n_m, const int32_t* ppt_list,
-                                       int32_t n_ppt, const int32_t* period_list, int32_t n_period, float rmse_tol,
+                                       int32_t n_ppt, const int32_t* tpp_list, int32_t n_tpp,
+                                       const int32_t* period_list, int32_t n_period, float rmse_tol,
                                        pf_tune_entry* table, int32_t table_cap, int32_t* n_table, pf_config* best)
 {
-    if (!base || !num_particles || !params || !inputs || !m_list || !ppt_list || !period_list || !table ||
-        !n_table || !best)
+    if (!base || !num_particles || !params || !inputs || !m_list || !ppt_list || !tpp_list || !period_list ||
+        !table || !n_table || !best)
         return fail(PF_ERR_INVALID, "null argument");
-    if (num_filters < 1 || steps < 1 || burn_in < 0 || burn_in >= steps || n_m < 1 || n_ppt < 1 || n_period < 1)
+    if (num_filters < 1 || steps < 1 || burn_in < 0 || burn_in >= steps || n_m < 1 || n_ppt < 1 || n_tpp < 1 ||
+        n_period < 1)
         return fail(PF_ERR_INVALID, "bad tuning shape");
-    if ((int64_t)n_m * n_ppt * n_period > table_cap) return fail(PF_ERR_INVALID, "table too small for the candidates");
+    if ((int64_t)n_m * n_ppt * n_tpp * n_period > table_cap)
+        return fail(PF_ERR_INVALID, "table too small for the candidates");
     ModelInfo mi;
     if (!model_info(model, &mi)) return fail(PF_ERR_INVALID, "unknown model %d", (int)model);
     pf_status s = require_gpu(base->device);
@@ -675,46 +686,50 @@ extern "C" pf_status pf_batch_autotune(const pf_config* base, pf_model_id model,
     int n = 0;
     for (int im = 0; im < n_m; ++im)
         for (int ip = 0; ip < n_ppt; ++ip)
-            for (int iq = 0; iq < n_period; ++iq) {
-                pf_tune_entry& t = table[n++];
-                memset(&t, 0, sizeof(t));
-                t.particles_per_subfilter = m_list[im];
-                t.particles_per_thread = ppt_list[ip];
-                t.exchange_period = period_list[iq];
-                t.rmse = NAN;
-                pf_config c = *base;
-                c.particles_per_subfilter = m_list[im];
-                c.particles_per_thread = ppt_list[ip];
-                c.exchange_period = period_list[iq];
-                pf_batch* B = nullptr;
-                t.status = pf_batch_create(&c, model, num_filters, num_particles, params, params_size, &B);
-                if (t.status != PF_OK) continue;
-                // first run captures the graph; the timed run replays it from the initial states
-                pf_status r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
-                if (r == PF_OK) r = pf_batch_synchronize(B);
-                if (r == PF_OK) r = pf_batch_set_initial_states(B, init.data());
-                cudaError_t e = cudaSuccess;
-                if (r == PF_OK) e = cudaEventRecord(ev.a, B->stream);
-                if (r == PF_OK && e == cudaSuccess)
-                    r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
-                if (r == PF_OK && e == cudaSuccess) e = cudaEventRecord(ev.b, B->stream);
-                if (r == PF_OK && e == cudaSuccess) e = cudaEventSynchronize(ev.b);
-                float ms = 0.0f;
-                if (r == PF_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev.a, ev.b);
-                if (r == PF_OK && e == cudaSuccess)
-                    e = cudaMemcpy(est.data(), dest.p, nio * sizeof(pf_estimate), cudaMemcpyDeviceToHost);
-                pf_batch_destroy(B);
-                if (r != PF_OK || e != cudaSuccess) {
-                    if (e != cudaSuccess) return fail(PF_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
-                    t.status = r;
-                    continue;
+            for (int it = 0; it < n_tpp; ++it)
+                for (int iq = 0; iq < n_period; ++iq) {
+                    pf_tune_entry& t = table[n++];
+                    memset(&t, 0, sizeof(t));
+                    t.particles_per_subfilter = m_list[im];
+                    t.particles_per_thread = ppt_list[ip];
+                    t.threads_per_particle = tpp_list[it];
+                    t.exchange_period = period_list[iq];
+                    t.rmse = NAN;
+                    pf_config c = *base;
+                    c.particles_per_subfilter = m_list[im];
+                    c.particles_per_thread = ppt_list[ip];
+                    c.threads_per_particle = tpp_list[it];
+                    c.exchange_period = period_list[iq];
+                    pf_batch* B = nullptr;
+                    t.status = pf_batch_create(&c, model, num_filters, num_particles, params, params_size, &B);
+                    if (t.status != PF_OK) continue;
+                    // first run captures the graph; the timed run replays it from the initial states
+                    pf_status r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
+                    if (r == PF_OK) r = pf_batch_synchronize(B);
+                    if (r == PF_OK) r = pf_batch_set_initial_states(B, init.data());
+                    cudaError_t e = cudaSuccess;
+                    if (r == PF_OK) e = cudaEventRecord(ev.a, B->stream);
+                    if (r == PF_OK && e == cudaSuccess)
+                        r = pf_batch_submit(B, (const pf_step_input*)din.p, (pf_estimate*)dest.p, steps, steps);
+                    if (r == PF_OK && e == cudaSuccess) e = cudaEventRecord(ev.b, B->stream);
+                    if (r == PF_OK && e == cudaSuccess) e = cudaEventSynchronize(ev.b);
+                    float ms = 0.0f;
+                    if (r == PF_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev.a, ev.b);
+                    if (r == PF_OK && e == cudaSuccess)
+                        e = cudaMemcpy(est.data(), dest.p, nio * sizeof(pf_estimate), cudaMemcpyDeviceToHost);
+                    pf_batch_destroy(B);
+                    if (r != PF_OK || e != cudaSuccess) {
+                        if (e != cudaSuccess) return fail(PF_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+                        t.status = r;
+                        continue;
+                    }
+                    t.ms_per_step = ms / (float)steps;
+                    int64_t P = 0;
+                    for (int f = 0; f < num_filters; ++f) P += num_particles[f];
+                    t.particle_steps_per_s = (double)P * steps / (ms * 1e-3);
+                    if (truth)
+                        t.rmse = tracking_rmse(est, truth, num_filters, steps, burn_in, mi.S, angle_mask_of(model));
                 }
-                t.ms_per_step = ms / (float)steps;
-                int64_t P = 0;
-                for (int f = 0; f < num_filters; ++f) P += num_particles[f];
-                t.particle_steps_per_s = (double)P * steps / (ms * 1e-3);
-                if (truth) t.rmse = tracking_rmse(est, truth, num_filters, steps, burn_in, mi.S, angle_mask_of(model));
-            }
     *n_table = n;
     // reference error: mean over the runnable every-step-exchange candidates
     double ref = 0.0;
@@ -737,6 +752,7 @@ extern "C" pf_status pf_batch_autotune(const pf_config* base, pf_model_id model,
     *best = *base;
     best->particles_per_subfilter = table[pick].particles_per_subfilter;
     best->particles_per_thread = table[pick].particles_per_thread;
+    best->threads_per_particle = table[pick].threads_per_particle;
     best->exchange_period = table[pick].exchange_period;
     return PF_OK;
 }

@@ -291,10 +291,13 @@ __device__ __forceinline__ float pf_sqrt(float d2) { return d2 * rsqrtf(fmaxf(d2
 // Strides below E are register pairs, strides below 32E are warp shuffles,
 // longer strides go through shared memory (sk/si hold M entries).  `tid` is
 // the thread's rank within the sub-filter (the lane when a warp owns one).
+// TP = 2: two adjacent lanes hold the same E keys (two threads per particle);
+// the pair runs the network together (lane masks doubled) and only the
+// `writer` lane stores to shared memory.
 // ---------------------------------------------------------------------------
-template <int M, int E>
+template <int M, int E, int TP = 1>
 __device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si,
-                                                  int tid = threadIdx.x)
+                                                  int tid = threadIdx.x, bool writer = true)
 {
 #pragma unroll
     for (int size = 2; size <= M; size <<= 1) {
@@ -316,13 +319,13 @@ __device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], f
                         }
                     }
                 }
-            } else if (stride < 32 * E) {
+            } else if (stride < (32 / TP) * E) {
                 const int lm = stride / E;
                 const bool upper = (tid & lm) != 0;
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const float ok = __shfl_xor_sync(kFull, k[e], lm);
-                    const int oi = __shfl_xor_sync(kFull, ix[e], lm);
+                    const float ok = __shfl_xor_sync(kFull, k[e], lm * TP);
+                    const int oi = __shfl_xor_sync(kFull, ix[e], lm * TP);
                     const int p = E * tid + e;
                     const bool ddd = (p & size) != 0;
                     const float lo = upper ? ok : k[e];
@@ -334,10 +337,12 @@ __device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], f
                 }
             } else {
                 __syncthreads();
+                if (writer) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    sk[E * tid + e] = k[e];
-                    si[E * tid + e] = ix[e];
+                    for (int e = 0; e < E; ++e) {
+                        sk[E * tid + e] = k[e];
+                        si[E * tid + e] = ix[e];
+                    }
                 }
                 __syncthreads();
 #pragma unroll
@@ -373,12 +378,14 @@ __device__ __forceinline__ void bitonic_sort_desc(float (&k)[E], int (&ix)[E], f
 // branch) sorts the original (key, index) pairs with bitonic_sort_desc, which
 // keeps the reference network's tie order.  Same contract as
 // bitonic_sort_desc for a CTA owning one sub-filter (tid = threadIdx.x);
-// returns true when the CTA fell back to the full network.
+// returns true when the CTA fell back to the full network.  TP as for
+// bitonic_sort_desc (the pair's lanes hold the same keys).
 // ---------------------------------------------------------------------------
-template <int M, int E>
+template <int M, int E, int TP = 1>
 __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], float* sk, int* si)
 {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x / TP;
+    const bool writer = threadIdx.x % TP == 0;
     float v[E];
     bool nan = false;
 #pragma unroll
@@ -401,19 +408,21 @@ __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], floa
                         v[e + stride] = asc ? hi : lo;
                     }
                 }
-            } else if (stride < 32 * E) {
+            } else if (stride < (32 / TP) * E) {
                 const int lm = stride / E;
                 // p & size and the thread's side of the pair are the same for all e here
                 const bool keep_max = (((E * tid) & size) != 0) == ((tid & lm) != 0);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const float o = __shfl_xor_sync(kFull, v[e], lm);
+                    const float o = __shfl_xor_sync(kFull, v[e], lm * TP);
                     v[e] = keep_max ? fmaxf(v[e], o) : fminf(v[e], o);
                 }
             } else {
                 __syncthreads();
+                if (writer) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+                    for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+                }
                 __syncthreads();
                 const bool keep_max = (((E * tid) & size) != 0) == (((E * tid) & stride) != 0);
 #pragma unroll
@@ -425,15 +434,17 @@ __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], floa
         }
     }
     __syncthreads();
+    if (writer) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+        for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
+    }
     __syncthreads();
     bool tie = nan;
 #pragma unroll
     for (int e = 0; e + 1 < E; ++e) tie |= v[e] == v[e + 1];
     if (E * tid + E < M) tie |= v[E - 1] == sk[E * tid + E];
     if (__syncthreads_or(tie)) {
-        bitonic_sort_desc<M, E>(k, ix, sk, si);
+        bitonic_sort_desc<M, E, TP>(k, ix, sk, si, tid, writer);
         return true;
     }
     // sorted position of each original key = the number of keys above it
@@ -443,7 +454,7 @@ __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], floa
 #pragma unroll
         for (int step = M / 2; step > 0; step >>= 1)
             if (sk[pos + step - 1] > k[e]) pos += step;
-        si[pos] = E * tid + e;
+        if (writer) si[pos] = E * tid + e;
     }
     __syncthreads();
 #pragma unroll
@@ -982,6 +993,39 @@ struct Unicycle {
         }
         return -0.5f * acc;
     }
+    // Two threads per particle (lane pair h = 0, 1): both lanes propagate the
+    // particle (identical arithmetic), each sums the landmarks j = h, h + 2,
+    // ..., and the pair adds the two sums in lane order.
+    __device__ static __forceinline__ float step_pair(const Consts& c, float* s, const float* n, int h, float* sn,
+                                                      float* cs)
+    {
+        float st, ct;
+        __sincosf(s[2], &st, &ct);
+        const float nx = fmaf(c.sq0, n[0], fmaf(c.A, ct, fmaf(-c.B, st, s[0])));
+        const float ny = fmaf(c.sq1, n[1], fmaf(c.A, st, fmaf(c.B, ct, s[1])));
+        const float nt = wrap_pi(fmaf(c.sq2, n[2], s[2] + c.wd));
+        s[0] = nx;
+        s[1] = ny;
+        s[2] = nt;
+        float s2, c2;
+        __sincosf(nt, &s2, &c2);
+        sn[0] = s2;
+        cs[0] = c2;
+        float acc = 0.0f;
+#pragma unroll 1
+        for (int j = h; j < c.L; j += 2) {
+            const float dx = c.lx[j] - nx, dy = c.ly[j] - ny;
+            const float r = pf_sqrt(fmaf(dx, dx, dy * dy));
+            const float er = (c.rm[j] - r) * c.isr;
+            const float cp = fmaf(c2, c.cb[j], -(s2 * c.sb[j]));
+            const float sp = fmaf(s2, c.cb[j], c2 * c.sb[j]);
+            const float eb = pf_atan2(fmaf(sp, dx, -(cp * dy)), fmaf(cp, dx, sp * dy)) * c.isb;
+            acc = fmaf(er, er, acc);
+            acc = fmaf(eb, eb, acc);
+        }
+        const float o = __shfl_xor_sync(kFull, acc, 1);
+        return -0.5f * (h ? o + acc : acc + o);
+    }
     // E particles at once: the same per-particle arithmetic as step() in the
     // same order (bit-identical results), with the landmark loop outside the
     // particle loop so each landmark's constants are read once per thread and
@@ -1100,6 +1144,95 @@ struct DhArm {
         acc = fmaf(d4, d4, acc);
         acc = fmaf(d5, d5, acc);
         return -0.5f * acc;
+    }
+    // Two threads per particle (lane pair h = 0, 1): both lanes advance all
+    // joints (identical arithmetic); lane h chains the transforms of joints
+    // 3h .. 3h+2 from the identity, the pair swaps chains and joint sines, and
+    // both form the whole chain T = T_0 T_1 (position p_0 + R_0 p_1); lane 0
+    // weighs the position and yaw, lane 1 pitch and roll, and the pair adds
+    // the two sums in lane order.
+    __device__ static __forceinline__ float step_pair(const Consts& c, float* s, const float* n, int h, float* sn,
+                                                      float* cs)
+    {
+        float q[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            q[i] = wrap_pi(fmaf(s[6 + i], c.dt, s[i]));
+            s[i] = q[i];
+            s[6 + i] = fmaf(c.sqd, n[i], s[6 + i]);
+        }
+        float R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, p[3] = {0, 0, 0};
+        float msn[3], mcs[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int i = 3 * h + k;
+            const float qi = h ? q[3 + k] : q[k];
+            float sq, cq;
+            __sincosf(qi, &sq, &cq);
+            msn[k] = sq;
+            mcs[k] = cq;
+            const float ca = c.ca[i], sa = c.sa[i];
+            const float a00 = cq, a01 = -(sq * ca), a02 = sq * sa;
+            const float a10 = sq, a11 = cq * ca, a12 = -(cq * sa);
+            const float a21 = sa, a22 = ca;
+            const float t0 = c.a[i] * cq, t1 = c.a[i] * sq, t2 = c.d[i];
+            float N[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                N[3 * r + 0] = fmaf(R[3 * r + 1], a10, R[3 * r + 0] * a00);
+                N[3 * r + 1] = fmaf(R[3 * r + 2], a21, fmaf(R[3 * r + 1], a11, R[3 * r + 0] * a01));
+                N[3 * r + 2] = fmaf(R[3 * r + 2], a22, fmaf(R[3 * r + 1], a12, R[3 * r + 0] * a02));
+                p[r] = fmaf(R[3 * r + 2], t2, fmaf(R[3 * r + 1], t1, fmaf(R[3 * r + 0], t0, p[r])));
+            }
+#pragma unroll
+            for (int j = 0; j < 9; ++j) R[j] = N[j];
+        }
+        float Ro[9], po[3];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) Ro[j] = __shfl_xor_sync(kFull, R[j], 1);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) po[j] = __shfl_xor_sync(kFull, p[j], 1);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float os = __shfl_xor_sync(kFull, msn[k], 1), oc = __shfl_xor_sync(kFull, mcs[k], 1);
+            sn[k] = h ? os : msn[k];
+            cs[k] = h ? oc : mcs[k];
+            sn[3 + k] = h ? msn[k] : os;
+            cs[3 + k] = h ? mcs[k] : oc;
+        }
+        const float* A = h ? Ro : R;  // joints 0..2
+        const float* B = h ? R : Ro;  // joints 3..5
+        const float* pa = h ? po : p;
+        const float* pb = h ? p : po;
+        float W[9], P[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int col = 0; col < 3; ++col)
+                W[3 * r + col] = fmaf(A[3 * r + 2], B[6 + col], fmaf(A[3 * r + 1], B[3 + col], A[3 * r] * B[col]));
+            P[r] = fmaf(A[3 * r + 2], pb[2], fmaf(A[3 * r + 1], pb[1], fmaf(A[3 * r], pb[0], pa[r])));
+        }
+        float acc;
+        if (h == 0) {
+            const float yaw = pf_atan2(W[3], W[0]);
+            const float e0 = (c.z[0] - P[0]) * c.isp, e1 = (c.z[1] - P[1]) * c.isp, e2 = (c.z[2] - P[2]) * c.isp;
+            float d3 = c.z[3] - yaw;
+            d3 = fmaf(-kTwoPi, rintf(d3 * kInvTwoPi), d3) * c.isa;
+            acc = e0 * e0;
+            acc = fmaf(e1, e1, acc);
+            acc = fmaf(e2, e2, acc);
+            acc = fmaf(d3, d3, acc);
+        } else {
+            const float pitch = pf_atan2(-W[6], pf_sqrt(fmaf(W[7], W[7], W[8] * W[8])));
+            const float roll = pf_atan2(W[7], W[8]);
+            float d4 = c.z[4] - pitch, d5 = c.z[5] - roll;
+            d4 = fmaf(-kTwoPi, rintf(d4 * kInvTwoPi), d4) * c.isa;
+            d5 = fmaf(-kTwoPi, rintf(d5 * kInvTwoPi), d5) * c.isa;
+            acc = d4 * d4;
+            acc = fmaf(d5, d5, acc);
+        }
+        const float o = __shfl_xor_sync(kFull, acc, 1);
+        return -0.5f * (h ? o + acc : acc + o);
     }
 };
 
@@ -1310,6 +1443,36 @@ struct Beacon {
         }
         return fmaf(-c.h, acc, c.lnorm);
     }
+    // Two threads per particle (lane pair h = 0, 1): both lanes propagate the
+    // particle (identical arithmetic), each sums the beacons j = h, h + 2, ...,
+    // and the pair adds the two sums in lane order.
+    __device__ static __forceinline__ float step_pair(const Consts& c, float* s, const float* n, int h, float* sn,
+                                                      float* cs)
+    {
+        const float v = fmaf(c.nv, n[0], c.v);
+        const float w = fmaf(c.nw, n[1], c.w);
+        const float g = c.ng * n[2];
+        const float ha = w * c.hdt;
+        const float k = v * c.dt * sinc(ha);
+        float sm, cm;
+        __sincosf(s[2] + ha, &sm, &cm);
+        const float nx = fmaf(k, cm, s[0]);
+        const float ny = fmaf(k, sm, s[1]);
+        const float nt = wrap_pi(fmaf(g, c.dt, fmaf(w, c.dt, s[2])));
+        s[0] = nx;
+        s[1] = ny;
+        s[2] = nt;
+        __sincosf(nt, &sn[0], &cs[0]);
+        float acc = 0.0f;
+#pragma unroll 1
+        for (int j = h; j < c.L; j += 2) {
+            const float dx = nx - c.bx[j], dy = ny - c.by[j];
+            const float e = pf_sqrt(fmaf(dx, dx, fmaf(dy, dy, c.bz2[j]))) - c.z[j];
+            acc = fmaf(e, e, acc);
+        }
+        const float o = __shfl_xor_sync(kFull, acc, 1);
+        return fmaf(-c.h, h ? o + acc : acc + o, c.lnorm);
+    }
     // E particles at once: step()'s per-particle arithmetic in the same order
     // (bit-identical results), the beacon loop outside the particle loop so
     // each beacon's constants are read once per thread and the E range
@@ -1387,6 +1550,33 @@ __device__ __forceinline__ void model_step_batch(const typename Mdl::Consts& c, 
     }
 }
 
+// Two threads per particle (TP = 2, lane pair h = lane & 1, both lanes
+// holding the same E particles): models with step_pair split each particle's
+// work between the pair; others run model_step_batch on both lanes, which
+// compute identical results.
+template <class Mdl, class = void>
+struct HasStepPair : std::false_type {};
+template <class Mdl>
+struct HasStepPair<Mdl, std::void_t<decltype(&Mdl::step_pair)>> : std::true_type {};
+
+template <class Mdl, int E, int TP, class Noise>
+__device__ __forceinline__ void model_step_tp(const typename Mdl::Consts& c, float (&s)[E][Mdl::S], Noise noise,
+                                              int h, float (&sn)[E][Mdl::NA > 0 ? Mdl::NA : 1],
+                                              float (&cs)[E][Mdl::NA > 0 ? Mdl::NA : 1], float (&ll)[E])
+{
+    if constexpr (TP == 2 && HasStepPair<Mdl>::value) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            float n[Mdl::K];
+#pragma unroll
+            for (int v = 0; v < Mdl::K; ++v) n[v] = noise(e, v);
+            ll[e] = Mdl::step_pair(c, s[e], n, h, sn[e], cs[e]);
+        }
+    } else {
+        model_step_batch<Mdl, E>(c, s, noise, sn, cs, ll);
+    }
+}
+
 // Models whose weights are continuous functions of a state that every step
 // perturbs in every variable the weight depends on: two particles share a key
 // only by coincidence, so their sub-filters sort with rank_sort_desc.  The
@@ -1401,13 +1591,13 @@ template <>
 struct RareTies<Beacon> : std::true_type {};
 
 // The sampling kernels' sort of one sub-filter per CTA (see rank_sort_desc).
-template <class Mdl, int M, int E>
+template <class Mdl, int M, int E, int TP = 1>
 __device__ __forceinline__ void sort_subfilter(float (&k)[E], int (&ix)[E], float* sk, int* si)
 {
     if constexpr (RareTies<Mdl>::value) {
-        rank_sort_desc<M, E>(k, ix, sk, si);
+        rank_sort_desc<M, E, TP>(k, ix, sk, si);
     } else {
-        bitonic_sort_desc<M, E>(k, ix, sk, si);
+        bitonic_sort_desc<M, E, TP>(k, ix, sk, si, threadIdx.x / TP, threadIdx.x % TP == 0);
     }
 }
 

@@ -47,7 +47,7 @@ int angle_count_of(int model);
 
 // Launch dispatch over the model template.
 struct ModelOps {
-    cudaError_t (*sample_sort)(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
+    cudaError_t (*sample_sort)(int, int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
     cudaError_t (*sample_weight)(int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
     cudaError_t (*block_sort)(int, int, int, cudaStream_t, const FilterDesc*, const int2*);
     cudaError_t (*exchange_resample)(int, int, int, int, cudaStream_t, const FilterDesc*, const int2*, InputRef,

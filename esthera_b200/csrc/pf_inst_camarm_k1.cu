@@ -3,7 +3,7 @@
 #include "pf_launch_impl.cuh"
 #include "pf_host.cuh"
 namespace pfdev {
-template cudaError_t Launch<CamArm>::sample_sort(int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
+template cudaError_t Launch<CamArm>::sample_sort(int, int, int, bool, int, cudaStream_t, const FilterDesc*, const int2*, InputRef);
 }  // namespace pfdev
 // the model registers itself here (once for the library)
 PF_REGISTER_MODEL(pfdev::CamArm, PF_MODEL_CAMARM, pf_camarm_params, "camarm");

@@ -105,6 +105,9 @@ __device__ __forceinline__ void wait_prerequisites() { asm volatile("griddepcont
 // 4 particles per thread runs 53 us capped at 56 registers against 59 us at
 // the compiler's own 83.  The arms' states (9-12 variables, forward
 // kinematics) need ~128 registers per thread; capping them lower spills.
+// The sampling kernel with two threads per particle asks for 4 warps fewer
+// (its CTAs are twice as large, so the rounding up of whole CTAs would
+// otherwise cut its registers below the one-thread kernel's).
 #ifndef PF_K1_WARPS_SMALL
 #define PF_K1_WARPS_SMALL 36
 #endif
@@ -230,17 +233,18 @@ __device__ __forceinline__ void normals_from_raw(const float* nz, int tid, float
 // k_sample_sort's dynamic shared memory: the MTGP32 ring (FR), one region
 // holding in turn the normals, the state stage of the sorted gather and the
 // estimate partials' per-thread sums, then the sort keys + indices.
-template <class Mdl, int M, bool FR>
+template <class Mdl, int M, bool FR, int TP = 1>
 constexpr size_t k1_stage_bytes()
 {
     const size_t nz = FR ? (size_t)(2 * ((Mdl::K * M + 1) / 2)) * 4 : 0;
-    const size_t stage = (size_t)Mdl::S * M * 4;
+    size_t stage = (size_t)Mdl::S * M * 4;
+    if (TP > 1 && stage < (size_t)TP * M * 8) stage = (size_t)TP * M * 8;  // a row of partials per thread
     return nz > stage ? nz : stage;
 }
-template <class Mdl, int M, bool FR>
+template <class Mdl, int M, bool FR, int TP = 1>
 constexpr size_t k1_smem()
 {
-    return (FR ? sizeof(MtgpSmem) : 0) + k1_stage_bytes<Mdl, M, FR>() + (size_t)M * 8;
+    return (FR ? sizeof(MtgpSmem) : 0) + k1_stage_bytes<Mdl, M, FR, TP>() + (size_t)M * 8;
 }
 
 // Estimate partials of one sub-filter from particles in any order:
@@ -251,12 +255,14 @@ constexpr size_t k1_smem()
 // bytes, free for this call; chunks of values when they do not all fit): P
 // consecutive lanes per value (P the largest power of two with NV * P <= NT,
 // at most 32) each add NT / P rows in order, then an xor-shuffle tree over
-// the P lanes.  A fixed order: deterministic for a given (M, E).
+// the P lanes.  A fixed order: deterministic for a given (M, E).  A thread
+// with counts = false (the second lane of a particle pair) adds zeros.
 template <class Mdl, int E, int NT, size_t ACC_BYTES>
 __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float lmax, const float (&okey)[E],
                                                const float (&st)[E][Mdl::S],
                                                const float (&sn)[E][Mdl::NA > 0 ? Mdl::NA : 1],
-                                               const float (&cs)[E][Mdl::NA > 0 ? Mdl::NA : 1], double* acc)
+                                               const float (&cs)[E][Mdl::NA > 0 ? Mdl::NA : 1], double* acc,
+                                               bool counts = true)
 {
     constexpr int S = Mdl::S, NA = Mdl::NA, NV = 1 + S + NA;
     constexpr int CH = (int)(ACC_BYTES / (8 * NT)) < NV ? (int)(ACC_BYTES / (8 * NT)) : NV;  // values per chunk
@@ -297,7 +303,7 @@ __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float
                         a += w[e] * (double)cs[e][i - 1 - S];
                     }
                 }
-                acc[c * NT + tid] = a;
+                acc[c * NT + tid] = counts ? a : 0.0;
             }
         }
         __syncthreads();
@@ -317,12 +323,15 @@ __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float
 // ---------------------------------------------------------------------------
 // Fused propagate + weight + sort.  FR: generate this sub-filter's MTGP32
 // stream in the kernel; otherwise read reference-layout normals from rbuf.
+// TP = 2: two threads per particle -- lanes 2g and 2g+1 both hold particles
+// E g .. E g + E - 1, split each particle's model work (model_step_tp), run the
+// sort together, and lane 2g alone writes (its partials carry the particles).
 // ---------------------------------------------------------------------------
-template <class Mdl, int M, int E, bool FR>
-__global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S))) k_sample_sort(const FilterDesc* __restrict__ descs,
+template <class Mdl, int M, int E, bool FR, int TP = 1>
+__global__ void __launch_bounds__(TP * M / E, pf_min_blocks(TP * M / E, pf_k1_warps(Mdl::S) - (TP - 1) * 4)) k_sample_sort(const FilterDesc* __restrict__ descs,
                                                        const int2* __restrict__ cta_map, InputRef in)
 {
-    constexpr int NT = M / E, S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
+    constexpr int NT = TP * M / E, S = Mdl::S, K = Mdl::K, NA = Mdl::NA;
     constexpr int NANG = NA > 0 ? NA : 1;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ typename Mdl::Consts cst;
@@ -333,8 +342,10 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     allow_dependents();
     const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
+    const int vt = tid / TP, h = tid % TP;  // the thread's E particles, its half of them
+    const bool writer = h == 0;
     const int64_t T = D.T;
-    const int64_t base = (int64_t)b * M + E * tid;
+    const int64_t base = (int64_t)b * M + E * vt;
 
     unsigned char* p = smem;
     MtgpSmem* ms = nullptr;
@@ -344,7 +355,7 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     }
     float* nz = reinterpret_cast<float*>(p);     // normals (FR), later the state stage, then the partials
     float* stage = nz;
-    p += k1_stage_bytes<Mdl, M, FR>();
+    p += k1_stage_bytes<Mdl, M, FR, TP>();
     float* sk = reinterpret_cast<float*>(p);
     int* si = reinterpret_cast<int*>(p + (size_t)M * 4);
 
@@ -377,17 +388,18 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
         float ll[E];
         if constexpr (FR && raw_normals<Mdl, E>()) {
             float z[E][K];
-            normals_from_raw<Mdl, M, E>(nz, tid, z);
-            model_step_batch<Mdl, E>(cst, st, [&](int e, int v) { return z[e][v]; }, sn, cs, ll);
+            normals_from_raw<Mdl, M, E>(nz, vt, z);
+            model_step_tp<Mdl, E, TP>(cst, st, [&](int e, int v) { return z[e][v]; }, h, sn, cs, ll);
         } else {
-            model_step_batch<Mdl, E>(
+            model_step_tp<Mdl, E, TP>(
                 cst, st,
-                [&](int e, int v) { return FR ? nz[v * M + E * tid + e] : D.rbuf[v * T + base + e]; }, sn, cs, ll);
+                [&](int e, int v) { return FR ? nz[v * M + E * vt + e] : D.rbuf[v * T + base + e]; }, h, sn, cs,
+                ll);
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) okey[e] = D.log_weights ? ll[e] : __expf(ll[e]);
     }
-    if (D.inplace) {
+    if (D.inplace && writer) {
 #pragma unroll
         for (int v = 0; v < S; ++v) {
             float o[E];
@@ -401,15 +413,17 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         k[e] = okey[e];
-        ix[e] = E * tid + e;
+        ix[e] = E * vt + e;
     }
-    sort_subfilter<Mdl, M, E>(k, ix, sk, si);
-    stv<E>(D.tkey + base, k);
+    sort_subfilter<Mdl, M, E, TP>(k, ix, sk, si);
+    if (writer) stv<E>(D.tkey + base, k);
     __syncthreads();  // normals consumed, sort buffers free: stage the state
+    if (writer) {
 #pragma unroll
-    for (int v = 0; v < S; ++v)
+        for (int v = 0; v < S; ++v)
 #pragma unroll
-        for (int e = 0; e < E; ++e) stage[v * M + E * tid + e] = st[e][v];
+            for (int e = 0; e < E; ++e) stage[v * M + E * vt + e] = st[e][v];
+    }
     if (tid == 0) {
         D.winner[b] = k[0];
         s_lmax = k[0];
@@ -417,13 +431,14 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k1_warps(Mdl::S
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < S; ++v) {
+        if (v % TP != h) continue;  // a pair's lanes gather alternate variables
         float o[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) o[e] = stage[v * M + ix[e]];
         stv<E>(D.tmp + v * T + base, o);
     }
-    write_partials<Mdl, E, NT, k1_stage_bytes<Mdl, M, FR>()>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn,
-                                                              cs, reinterpret_cast<double*>(stage));
+    write_partials<Mdl, E, NT, k1_stage_bytes<Mdl, M, FR, TP>()>(D, b, D.log_weights ? s_lmax : 0.0f, okey, st, sn,
+                                                                  cs, reinterpret_cast<double*>(stage), writer);
 }
 
 // ---------------------------------------------------------------------------

@@ -35,7 +35,8 @@ struct Launch {
         for (int a = 0; a < Mdl::NA; ++a) m |= 1u << Mdl::angle_var(a);
         return m;
     }
-    static cudaError_t sample_sort(int M, int E, bool fr, int grid, cudaStream_t st, const FilterDesc* d,
+    // tp: threads per particle (1, or 2 with fr)
+    static cudaError_t sample_sort(int M, int E, int tp, bool fr, int grid, cudaStream_t st, const FilterDesc* d,
                                    const int2* map, InputRef in);
     static cudaError_t sample_weight(int M, int E, int grid, cudaStream_t st, const FilterDesc* d, const int2* map,
                                      InputRef in);

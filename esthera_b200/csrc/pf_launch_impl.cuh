@@ -9,28 +9,32 @@ namespace pfdev {
 
 #if defined(PF_PART_K1)
 template <class Mdl>
-cudaError_t Launch<Mdl>::sample_sort(int M, int E, bool fr, int grid, cudaStream_t st, const FilterDesc* d,
+cudaError_t Launch<Mdl>::sample_sort(int M, int E, int tp, bool fr, int grid, cudaStream_t st, const FilterDesc* d,
                                      const int2* map, InputRef in)
 {
+#define PF_K1_ONE(m, e, FR, TP)                                                             \
+    {                                                                                       \
+        auto fn = k_sample_sort<Mdl, m, e, FR, TP>;                                         \
+        constexpr size_t sm = k1_smem<Mdl, m, FR, TP>();                                    \
+        cudaError_t r = allow_smem(fn, sm);                                                 \
+        if (r != cudaSuccess) return r;                                                     \
+        fn<<<grid, TP * m / e, sm, st>>>(d, map, in);                                       \
+        return cudaGetLastError();                                                          \
+    }
 #define PF_K1(m, e)                                                                         \
     if (M == m && E == e) {                                                                 \
-        if (fr) {                                                                           \
-            auto fn = k_sample_sort<Mdl, m, e, true>;                                       \
-            constexpr size_t sm = k1_smem<Mdl, m, true>();                                  \
-            cudaError_t r = allow_smem(fn, sm);                                             \
-            if (r != cudaSuccess) return r;                                                 \
-            fn<<<grid, m / e, sm, st>>>(d, map, in);                                        \
-        } else {                                                                            \
-            auto fn = k_sample_sort<Mdl, m, e, false>;                                      \
-            constexpr size_t sm = k1_smem<Mdl, m, false>();                                 \
-            cudaError_t r = allow_smem(fn, sm);                                             \
-            if (r != cudaSuccess) return r;                                                 \
-            fn<<<grid, m / e, sm, st>>>(d, map, in);                                        \
+        if (tp == 2) {                                                                      \
+            if constexpr (2 * m / e <= 1024) {                                              \
+                if (fr) PF_K1_ONE(m, e, true, 2)                                            \
+            }                                                                               \
+            return cudaErrorInvalidValue;                                                   \
         }                                                                                   \
-        return cudaGetLastError();                                                          \
+        if (fr) PF_K1_ONE(m, e, true, 1)                                                    \
+        PF_K1_ONE(m, e, false, 1)                                                           \
     }
     PF_ME_LIST(PF_K1)
 #undef PF_K1
+#undef PF_K1_ONE
     return cudaErrorInvalidValue;
 }
 #endif

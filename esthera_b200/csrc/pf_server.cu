@@ -569,7 +569,7 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
         CU(cudaGetLastError());
         const ModelOps ops = model_ops(m);
         InputRef ir{s->d_slot_in, 1, nullptr, 0, 0};
-        CU(ops.sample_sort(M, E, true, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir));
+        CU(ops.sample_sort(M, E, 1, true, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir));
         ModelInfo mi;
         model_info(m, &mi);
         const int virt = dependent_launch_pays((int)ctas[m], M, E, mi.S, s->device) ? 3 : 1;

@@ -113,6 +113,11 @@ typedef struct {
                                         otherwise it keeps its propagated particles; 0: always (the
                                         reference's ADAPTIVE_RESAMPLING test sum p^2 <= thr,
                                         resampling-valias.cl:273-284, is ess_fraction = 1 / (thr m)) */
+    int32_t threads_per_particle;    /* 0 or 1: one thread per particle; 2: two adjacent threads share each
+                                        particle's propagate + weight (the unicycle and beacon models split
+                                        their measurement sums, the DH arm its forward-kinematics chain; other
+                                        models compute it on both) and sort together.  Split pipeline with
+                                        PF_RNG_SUBFILTER, 2 m / ppt <= 1024 */
 } pf_config;
 
 /* One step's inputs.  control/meas are interpreted by the model:
@@ -366,19 +371,21 @@ pf_status pf_batch_filter_shape(pf_batch* b, int32_t filter, int32_t* particles_
 pf_status pf_batch_get_sorted(pf_batch* b, int32_t filter, float* soa, float* keys);
 
 /* Autotuner for batched filters (project-written; no reference counterpart).
- * Every candidate (m from m_list x particles per thread from ppt_list x exchange
- * period from period_list) runs `steps` steps of the whole batch on `inputs`
+ * Every candidate (m from m_list x particles per thread from ppt_list x threads
+ * per particle from tpp_list x exchange period from period_list) runs `steps` steps of the whole batch on `inputs`
  * (host, [F][steps]) twice -- the first run captures the CUDA graph, the second
  * is timed with CUDA events -- and, when `truth` ([F][steps][S], host) is given,
  * its tracking RMSE over steps >= burn_in is computed (angles wrapped).  A
  * candidate is accepted when its RMSE is within (1 + rmse_tol) of the mean
  * RMSE of the period-1 candidates (without truth: period-1 candidates only);
- * *best = base with the fastest accepted candidate's m, ppt and period.
- * Candidates that cannot run (m not dividing every count, ppt not built for m)
- * keep their pf_status in the table. */
+ * *best = base with the fastest accepted candidate's m, ppt, threads per
+ * particle and period.  Candidates that cannot run (no sub-filter size
+ * dividing some count, ppt not built for m) keep their pf_status in the
+ * table. */
 typedef struct {
     int32_t particles_per_subfilter;
     int32_t particles_per_thread;
+    int32_t threads_per_particle;
     int32_t exchange_period;
     int32_t status;
     float ms_per_step;
@@ -390,7 +397,8 @@ pf_status pf_batch_autotune(const pf_config* base, pf_model_id model, int32_t nu
                             const int32_t* num_particles, const void* params, size_t params_size,
                             const pf_step_input* inputs, const float* truth, int32_t steps, int32_t burn_in,
                             const int32_t* m_list, int32_t n_m, const int32_t* ppt_list, int32_t n_ppt,
-                            const int32_t* period_list, int32_t n_period, float rmse_tol,
+                            const int32_t* tpp_list, int32_t n_tpp, const int32_t* period_list, int32_t n_period,
+                            float rmse_tol,
                             pf_tune_entry* table, int32_t table_cap, int32_t* n_table, pf_config* best);
 
 /* ---- serving: many resident filters, updates batched as they arrive ----

@@ -179,14 +179,16 @@ def test_batch_autotune(gpu):
     steps = 12
     params, inputs, truth = batch_setup(E, counts, steps)
     best, rows = E.batch_autotune(UNI, params, counts, inputs, truth, m_list=(128, 256, 512, 1024), ppt_list=(2, 4),
-                                  period_list=(1, 2), burn_in=2, rmse_tol=0.5, num_transfer=1, exchange=1)
-    assert len(rows) == 4 * 2 * 2
+                                  tpp_list=(1, 2), period_list=(1, 2), burn_in=2, rmse_tol=0.5, num_transfer=1,
+                                  exchange=1)
+    assert len(rows) == 4 * 2 * 2 * 2
     for r in rows:  # m = 512 / 1024 cap each filter's sub-filters at a size dividing its count
         assert r["status"] == E.PF_OK and r["ms_per_step"] > 0 and np.isfinite(r["rmse"])
     ok = [r for r in rows if r["accepted"]]
     pick = max(ok, key=lambda r: r["particle_steps_per_s"])
-    assert (best.particles_per_subfilter, best.particles_per_thread, best.exchange_period) == (
-        pick["particles_per_subfilter"], pick["particles_per_thread"], pick["exchange_period"])
+    assert (best.particles_per_subfilter, best.particles_per_thread, best.threads_per_particle,
+            best.exchange_period) == (pick["particles_per_subfilter"], pick["particles_per_thread"],
+                                      pick["threads_per_particle"], pick["exchange_period"])
 
 
 @pytest.mark.gpu
