@@ -41,6 +41,14 @@
  *                  float (&sn)[E][NA or 1], float (&cs)[E][NA or 1], float (&ll)[E]);
  *       E particles at once with step()'s arithmetic (noise(e, v) is
  *       particle e's v-th normal), when interleaving them pays.
+ *   optional: __device__ static float step_pair(const Consts& c, float* s,
+ *                                               const float* n, int h,
+ *                                               float* sn, float* cs);
+ *       two threads per particle (pf_config.threads_per_particle = 2): the
+ *       lanes 2g + h (h = 0, 1) of a pair call it for the same particle; both
+ *       must leave identical s / sn / cs and return identical log-likelihoods,
+ *       exchanging partial results with __shfl_xor_sync(0xffffffff, x, 1)
+ *       (every lane of the warp takes part).  Without it both lanes run step.
  *
  * The parameter struct: standard layout, at most 256 bytes, with a member
  * float init_state[S] (the state pf_set_initial_state and creation use).

@@ -207,3 +207,34 @@ def test_batch_normalisation_vs_fp64(gpu):
         mx = kk.max()
         ln = mx + np.log(np.sum(np.exp(kk - mx)))
         assert abs(est[f]["log_norm"] - ln) <= 1e-6 * max(1.0, abs(ln)), (f, est[f]["log_norm"], ln)
+
+
+@pytest.mark.gpu
+def test_batch_rmse_vs_fp64_oracle(gpu, O):
+    """Tracking error of batched filters against the oracle's FP64 run of the
+    same filters (same streams: each filter's oracle starts at its batch
+    stream offset): the mean RMSE over the filters agrees within 5 % + 0.005.
+    The batched results equal the plain path's bit for bit, so the plain path
+    has the same error."""
+    E = gpu
+    counts = [2048, 4096, 8192, 2048, 4096, 8192]
+    steps = 60
+    params, inputs, truth = batch_setup(E, counts, steps, seed0=21)
+    cfg = dict(num_transfer=2, exchange=1, resampler=1, particles_per_thread=4)
+    B = E.FilterBatch(UNI, params, counts, particles_per_subfilter=256, **cfg)
+    est = np.stack([B.step(inputs[:, k]) for k in range(steps)], axis=1)  # [F, steps]
+    seed = B.config.seed
+    g, o = [], []
+    for f, n in enumerate(counts):
+        mf, ppt = B.filter_shape(f)
+        md = O.model_from_params(UNI, params[f])
+        of = O.Filter(md, mf, n // mf, 2, O.EXCH_RING, 1, O.RNG_SUBFILTER, 96, ppt, 1, 1.0, seed, 0,
+                      np.array(params[f].init_state[:3], np.float32))
+        of.set_stream_offset(B.filter_info(f)["stream_offset"])
+        om = np.array([of.step(inputs[f, k]["control"], inputs[f, k]["meas"])[0].mean[:2] for k in range(steps)])
+        of.close()
+        gm = np.array([e["mean"][:2] for e in est[f]])
+        g.append(np.sqrt(np.mean(np.sum((gm[10:] - truth[f, 10:, :2]) ** 2, axis=1))))
+        o.append(np.sqrt(np.mean(np.sum((om[10:] - truth[f, 10:, :2]) ** 2, axis=1))))
+    g, o = float(np.mean(g)), float(np.mean(o))
+    assert abs(g - o) <= 0.05 * o + 0.005, (g, o)
