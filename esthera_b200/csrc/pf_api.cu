@@ -784,7 +784,8 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
         // a programmatic dependent of the sampling kernel when that pays (its
         // CTAs start during the sampling kernel's last wave and wait there)
         const int virt = dependent_launch_pays(N, M, E, f->mi.S, c.device) ? 3 : 1;
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, late ? nullptr : ctr_inc, virt));
+        CU(f->ops.exchange_resample(M, E, c.resampler, N + estimate_ctas(N), st, desc, nullptr, in,
+                                    late ? nullptr : ctr_inc, virt));
         CU(mark("exchange_resample"));
         if (late) CU(launch_counter_inc(ctr_inc, st));
     } else {
@@ -801,7 +802,7 @@ static pf_status enqueue_step(pf_filter* f, const FilterDesc* desc, InputRef in,
             CU(f->ops.exchange_inplace(N, nx < 1024 ? ((nx + 31) / 32) * 32 : 1024, st, desc, nullptr));
             CU(mark("exchange"));
         }
-        CU(f->ops.exchange_resample(M, E, c.resampler, N, st, desc, nullptr, in, ctr_inc, 0));
+        CU(f->ops.exchange_resample(M, E, c.resampler, N + estimate_ctas(N), st, desc, nullptr, in, ctr_inc, 0));
         CU(mark("resample"));
     }
     if (f->timing) f->nphase = np - 1;
@@ -1490,7 +1491,8 @@ extern "C" pf_status pf_shard_resample(pf_filter* f)
     TRYS(need_shard(f));
     CU(cudaSetDevice(f->cfg.device));
     InputRef ir{f->d_in, 0, nullptr, 0, f->steps_done};
-    CU(f->ops.exchange_resample(f->M, f->E, f->cfg.resampler, f->N, f->stream, f->d_desc, nullptr, ir, nullptr, 1));
+    CU(f->ops.exchange_resample(f->M, f->E, f->cfg.resampler, f->N + estimate_ctas(f->N), f->stream, f->d_desc,
+                                nullptr, ir, nullptr, 1));
     const int ng = (f->N + 31) / 32;
     CU(launch_shard_rows(f->d_desc, ng, f->rows, f->states, f->mi.S, 2 + f->mi.S + f->na, f->stream));
     CU(cudaMemcpyAsync(f->h_est, f->d_est, sizeof(pf_estimate) + sizeof(int32_t), cudaMemcpyDeviceToHost, f->stream));

@@ -32,6 +32,7 @@ __global__ void k_batch_fill(const FilterDesc* __restrict__ descs, const int2* _
 {
     int f, b;
     cta_target(map, f, b);
+    if (b < 0) return;  // an estimate entry
     const FilterDesc& D = descs[f];
     for (int v = 0; v < S; ++v) {
         const float x = init[(int64_t)f * S + v];
@@ -52,11 +53,14 @@ struct pf_batch {
     int F = 0, M = 0, E = 0, S = 0, t = 0;  // M, E: the configured (largest) sub-filter size and its ppt
     int64_t P = 0;   // particles in all filters
     int NS = 0;      // sub-filters in all filters
+    int map_len = 0;  // CTA-map entries: sub-filters and estimate CTAs
     std::vector<int32_t> nsub, sub_off, grp_off;  // grp_off: first estimate group (32 sub-filters) of a filter
     std::vector<int32_t> mf;                      // each filter's sub-filter size
     std::vector<int64_t> part_off, ru_off;
     struct Group {
-        int M, E, TP, NS, map_off;  // one sub-filter size: ppt, threads per particle, sub-filters, first map entry
+        // one sub-filter size: ppt, threads per particle, sub-filters, estimate
+        // CTAs (one per 32 sub-filters of each filter), first map entry
+        int M, E, TP, NS, NE, map_off;
     };
     std::vector<Group> groups;
     std::vector<ModelParams> mp;
@@ -186,12 +190,13 @@ static pf_status batch_status(int32_t st)
 static pf_status enqueue_batch_step(pf_batch* B, const FilterDesc* desc, InputRef in, int32_t* ctr_inc)
 {
     for (const pf_batch::Group& g : B->groups) {
-        const int2* map = B->map + g.map_off;
-        CU(B->ops.sample_sort(g.M, g.E, g.TP, true, g.NS, B->stream, desc, map, in));
+        const int2* map = B->map + g.map_off;  // the estimate CTAs, then the sub-filters
+        CU(B->ops.sample_sort(g.M, g.E, g.TP, true, g.NS, B->stream, desc, map + g.NE, in));
         // a programmatic dependent of the sampling kernel when that pays (starts in its last wave, waits for
         // the grid)
         const int virt = dependent_launch_pays(g.NS, g.M, g.E, B->mi.S, B->cfg.device) ? 3 : 1;
-        CU(B->ops.exchange_resample(g.M, g.E, B->cfg.resampler, g.NS, B->stream, desc, map, in, nullptr, virt));
+        CU(B->ops.exchange_resample(g.M, g.E, B->cfg.resampler, g.NE + g.NS, B->stream, desc, map, in, nullptr,
+                                    virt));
     }
     if (ctr_inc) CU(launch_counter_inc(ctr_inc, B->stream));
     return PF_OK;
@@ -312,16 +317,19 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     }
     // one group of launches per sub-filter size, the largest first
     for (int c = M; c >= 32; c >>= 1) {
-        int ns = 0;
+        int ns = 0, ne = 0;
         for (int f = 0; f < num_filters; ++f)
-            if (mf[f] == c) ns += B->nsub[f];
+            if (mf[f] == c) {
+                ns += B->nsub[f];
+                ne += estimate_ctas(B->nsub[f]);
+            }
         if (!ns) continue;
         const int ec = c == M ? E : (cfg->particles_per_thread > 0 && me_supported(c, cfg->particles_per_thread)
                                          ? cfg->particles_per_thread
                                          : default_ppt(c));
         // two threads per particle where the sampling kernel's CTA stays within 1024 threads
         const int tp = cfg->threads_per_particle == 2 && 2 * c / ec <= 1024 ? 2 : 1;
-        B->groups.push_back(pf_batch::Group{c, ec, tp, ns, 0});
+        B->groups.push_back(pf_batch::Group{c, ec, tp, ns, ne, 0});
     }
     cudaError_t e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -346,7 +354,7 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     TRY(balloc(B, &B->gpart, (size_t)go * kPartStride));
     TRY(balloc(B, &B->est_ctr, (size_t)num_filters));
     TRY(balloc(B, &B->ctr, 1));
-    TRY(balloc(B, &B->map, (size_t)NS));
+    TRY(balloc(B, &B->map, (size_t)NS + go));
     TRY(balloc(B, &B->d_desc, 2 * (size_t)num_filters));
     TRY(balloc(B, &B->d_in, (size_t)num_filters));
     TRY(balloc(B, &B->d_est, (size_t)num_filters + 1));  // + the kernels' status word
@@ -357,21 +365,21 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         return fail(PF_ERR_NOMEM, "cudaMallocHost failed");
     }
     {
-        // per sub-filter size, group leaders (sub-filters 0, 32, 64, ... of each
-        // filter) first: the resampling kernel's CTAs that combine the
-        // estimates run in its first wave
+        // per sub-filter size, the estimate CTAs (filter, -1 - group) first --
+        // they combine each group of 32 sub-filters' partials in the
+        // resampling kernel's first wave -- then every sub-filter
         std::vector<int2> map;
-        map.reserve((size_t)NS);
+        map.reserve((size_t)NS + go);
         for (pf_batch::Group& g : B->groups) {
             g.map_off = (int)map.size();
             for (int f = 0; f < num_filters; ++f)
                 if (mf[f] == g.M)
-                    for (int b = 0; b < B->nsub[f]; b += 32) map.push_back(make_int2(f, b));
+                    for (int q = 0; q < estimate_ctas(B->nsub[f]); ++q) map.push_back(make_int2(f, -1 - q));
             for (int f = 0; f < num_filters; ++f)
                 if (mf[f] == g.M)
-                    for (int b = 0; b < B->nsub[f]; ++b)
-                        if (b & 31) map.push_back(make_int2(f, b));
+                    for (int b = 0; b < B->nsub[f]; ++b) map.push_back(make_int2(f, b));
         }
+        B->map_len = (int)map.size();
         if (cudaMemcpy(B->map, map.data(), map.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
             launch_mtgp_init(B->mtgp, (int)NS, cfg->stream_offset, cfg->seed, B->stream) != cudaSuccess ||
             cudaStreamSynchronize(B->stream) != cudaSuccess) {
@@ -416,7 +424,7 @@ extern "C" pf_status pf_batch_set_initial_states(pf_batch* B, const float* state
     CU(cudaMalloc(&d, sizeof(float) * B->S * B->F));
     cudaError_t e = cudaMemcpy(d, states, sizeof(float) * B->S * B->F, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        k_batch_fill<<<B->NS, 256, 0, B->stream>>>(B->d_desc, B->map, d, B->S);
+        k_batch_fill<<<B->map_len, 256, 0, B->stream>>>(B->d_desc, B->map, d, B->S);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);

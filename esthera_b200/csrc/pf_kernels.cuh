@@ -190,18 +190,19 @@ __device__ __forceinline__ void cta_target(const int2* __restrict__ cta_map, int
     }
 }
 
-// The resampling kernel's CTA order puts the first sub-filter of every group of
-// 32 (the CTAs that combine the estimate partials, the last of them also the
-// global estimate) ahead of the rest, so the estimate runs in the first wave
-// instead of delaying a CTA of the last one.  Without a CTA map: CTA i < ng
-// takes sub-filter 32 i, CTA ng + j takes the j-th of the others.  Maps built
-// by the batch and the server list the group leaders first in the same way.
-__device__ __forceinline__ int leaders_first(int i, int N)
+// The resampling kernel's grid: one estimate CTA per group of 32 sub-filters
+// first (it combines the group's partial rows; the last of them, by ticket,
+// the global estimate), then one CTA per sub-filter, so the estimate runs in
+// short CTAs of the first wave instead of lengthening resampling CTAs.
+// Without a CTA map CTA i < ng is group i's estimate CTA and CTA ng + j
+// resamples sub-filter j; maps built by the batch and the server list
+// (filter, -1 - g) entries first in the same way (the sampling kernel is
+// given the map past them).  Returns the sub-filter, or -1 - g.
+__host__ __device__ constexpr int estimate_ctas(int N) { return (N + 31) >> 5; }
+__device__ __forceinline__ int resample_cta(int i, int N)
 {
-    const int ng = (N + 31) >> 5;
-    if (i < ng) return i << 5;
-    const int j = i - ng;
-    return j + j / 31 + 1;
+    const int ng = estimate_ctas(N);
+    return i < ng ? -1 - i : i - ng;
 }
 
 __device__ __forceinline__ const pf_step_input* input_of(const InputRef& in, int f)
@@ -559,22 +560,26 @@ __global__ void __launch_bounds__(M / E) k_block_sort(const FilterDesc* __restri
 __device__ __forceinline__ int64_t exchange_source(const FilterDesc& D, int b, int x)
 {
     const int M = D.M, N = D.N, t = D.t;
-    if (D.exchange == PF_EXCHANGE_RING) return (int64_t)((b - 1 + N) % N) * M + x;
+    if (D.exchange == PF_EXCHANGE_RING) return (int64_t)(b == 0 ? N - 1 : b - 1) * M + x;
     if (D.exchange == PF_EXCHANGE_ALL2ALL) return D.a2a[x];
-    const int k = x / t, j = x - k * t;
+    // the torus width dx is a power of two: shifts and masks, no divisions
+    const int k = x >= 2 * t ? (x >= 3 * t ? 3 : 2) : (x >= t ? 1 : 0);
+    const int j = x - k * t;
     const int dx = D.dx, dy = D.shard ? D.gdy : D.dy;
+    const int sh = __ffs(dx) - 1, mk = dx - 1;
     const int bg = b + D.b0;
-    const int cx = bg % dx, cy = bg / dx;
+    const int cx = bg & mk, cy = bg >> sh;
     int from;
-    if (k == 0) from = cy * dx + (cx + 1) % dx;            // right neighbour sent "left"
-    else if (k == 1) from = cy * dx + (cx - 1 + dx) % dx;  // left neighbour sent "right"
-    else if (k == 2) from = ((cy + 1) % dy) * dx + cx;     // bottom neighbour sent "top"
-    else from = ((cy - 1 + dy) % dy) * dx + cx;            // top neighbour sent "bottom"
+    if (k == 0) from = (cy << sh) + ((cx + 1) & mk);            // right neighbour sent "left"
+    else if (k == 1) from = (cy << sh) + ((cx - 1) & mk);       // left neighbour sent "right"
+    else if (k == 2) from = ((cy + 1 == dy ? 0 : cy + 1) << sh) + cx;  // bottom neighbour sent "top"
+    else from = ((cy == 0 ? dy - 1 : cy - 1) << sh) + cx;       // top neighbour sent "bottom"
     if (D.shard) {
         // a row of this shard, or the halo row above (block 0) / below (block 1):
         // halo slots are returned as -(1 + index into a block's rows)
-        const int fy = from / dx, fx = from - fy * dx, rows = N / dx;
-        const int ry = (fy - D.r0 + dy) % dy;
+        const int fy = from >> sh, fx = from & mk, rows = N >> sh;
+        int ry = fy - D.r0;
+        if (ry < 0) ry += dy;
         if (ry < rows) return (int64_t)(from - D.b0) * M + j;
         const int h = ry == dy - 1 ? 0 : 1;
         return -(1 + ((int64_t)(h * dx + fx) * t + j));
@@ -782,13 +787,16 @@ __device__ __forceinline__ void estimate_final(const FilterDesc& D, int lane, in
     estimate_write<S>(D, lane, ng, NV, gm, bk, bi, best_src, E, step_no);
 }
 
+// Group g's estimate row from its 32 sub-filters' partial rows (one warp);
+// the last group to finish (ticket) combines every group row into the
+// filter's estimate.
 template <int S>
-__device__ __forceinline__ void estimate_groups(const FilterDesc& D, int b, const InputRef& in, int32_t* step_ctr)
+__device__ __forceinline__ void estimate_group(const FilterDesc& D, int g, const InputRef& in, int32_t* step_ctr)
 {
-    if ((b & 31) != 0 || threadIdx.x >= 32) return;
+    if (threadIdx.x >= 32) return;
     constexpr int NVMAX = 2 + 2 * S;
     const int lane = threadIdx.x;
-    const int g = b >> 5, ng = (D.N + 31) >> 5;
+    const int b = g << 5, ng = (D.N + 31) >> 5;
     const int NV = 2 + S + D.na;
     const int sb = b + lane;
     const bool valid = sb < D.N;
@@ -1158,14 +1166,17 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
         b = c.y;
     } else {
         f = 0;
-        b = leaders_first(blockIdx.x, descs[0].N);
+        b = resample_cta(blockIdx.x, descs[0].N);
     }
     __shared__ FilterDesc sdesc;
     __shared__ uint64_t mbar;
     const FilterDesc& D = load_desc(sdesc, descs + f);
     const int tid = threadIdx.x;
     wait_prerequisites();
-    estimate_groups<S>(D, b, in, step_ctr);
+    if (b < 0) {
+        estimate_group<S>(D, -1 - b, in, step_ctr);
+        return;
+    }
     const int64_t T = D.T;
     const int64_t base = (int64_t)b * M + E * tid;
     const float* U = D.rng_fused ? D.ru + (int64_t)b * D.ru_stride : D.rbuf + D.nnorm;

@@ -34,8 +34,8 @@ namespace {
 
 struct Pending {         // one update in a batch (host -> device)
     int32_t slot;
-    int32_t first_lead;  // position of the slot's group leaders in its model's CTA map
-    int32_t first_rest;  // position of its other sub-filters, after all groups' leaders
+    int32_t first_lead;  // position of the slot's estimate CTAs in its model's CTA map
+    int32_t first_rest;  // position of its sub-filters, after all estimate CTAs
 };
 
 // One block per batched update: copy its input into the slot's input entry
@@ -50,10 +50,8 @@ __global__ void k_srv_expand(const Pending* __restrict__ pend, const pf_step_inp
     if (i >= n) return;
     const Pending p = pend[i];
     const int N = descs[p.slot].N;
-    for (int b = threadIdx.x; b < N; b += blockDim.x) {
-        const int at = (b & 31) == 0 ? p.first_lead + (b >> 5) : p.first_rest + b - (b >> 5) - 1;
-        map[at] = make_int2(p.slot, b);
-    }
+    for (int b = threadIdx.x; b < N; b += blockDim.x) map[p.first_rest + b] = make_int2(p.slot, b);
+    for (int q = threadIdx.x; q < estimate_ctas(N); q += blockDim.x) map[p.first_lead + q] = make_int2(p.slot, -1 - q);
     const uint32_t* src = reinterpret_cast<const uint32_t*>(in + i);
     uint32_t* dst = reinterpret_cast<uint32_t*>(slot_in + p.slot);
     for (int w = threadIdx.x; w < (int)(sizeof(pf_step_input) / 4); w += blockDim.x) dst[w] = src[w];
@@ -399,7 +397,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
         return fail(PF_ERR_ADMISSION, "filter needs %zu bytes, %lld of %lld in use", L.total, (long long)s->used,
                     (long long)s->budget);
     CU(cudaSetDevice(s->device));
-    pf_status st = ensure_map(s, s->resident_sub + N);
+    pf_status st = ensure_map(s, s->resident_sub + N + estimate_ctas(N));
     if (st != PF_OK) return st;
     void* mem = nullptr;
     cudaError_t e = cudaMallocAsync(&mem, L.total, s->pool, s->stream);
@@ -475,7 +473,7 @@ extern "C" pf_status pf_server_open(pf_server* s, pf_model_id model, const void*
     s->used += (int64_t)L.total;
     s->n_open++;
     s->resident_T += D.T;
-    s->resident_sub += N;
+    s->resident_sub += N + estimate_ctas(N);  // map entries: sub-filters and estimate CTAs
     *id = slot;
     return PF_OK;
 }
@@ -490,7 +488,7 @@ extern "C" pf_status pf_server_close(pf_server* s, int32_t id)
     s->used -= (int64_t)sl.bytes;
     s->n_open--;
     s->resident_T -= sl.T;
-    s->resident_sub -= sl.N;
+    s->resident_sub -= sl.N + estimate_ctas(sl.N);
     s->queued -= (int64_t)sl.queue.size();
     sl = Slot();
     s->free_slots.push_back(id);
@@ -518,7 +516,7 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
     if (s->busy) return PF_OK;  // one batch in flight at a time
     CU(cudaSetDevice(s->device));
     int n = 0;
-    int64_t ctas[PF_NUM_MODELS] = {};
+    int64_t ctas[PF_NUM_MODELS] = {}, ests[PF_NUM_MODELS] = {};
     s->batch_slots.clear();
     s->batch_tags.clear();
     // group the batch by model so each model's kernels see one contiguous CTA map
@@ -536,16 +534,16 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
             sl.queue.pop_front();
             s->queued--;
             sl.in_flight = true;
-            leads += (sl.N + 31) / 32;
+            leads += estimate_ctas(sl.N);
             ctas[m] += sl.N;
             ++n;
         }
         s->ready[m].clear();
-        int64_t rest = leads;  // the other sub-filters follow all of the group's leaders
+        ests[m] = leads;
+        int64_t rest = leads;  // the sub-filters follow all of the model's estimate CTAs
         for (int q = first; q < n; ++q) {
             s->h_pend[q].first_rest = (int32_t)rest;
-            const int N = s->slots[s->h_pend[q].slot].N;
-            rest += N - (N + 31) / 32;
+            rest += s->slots[s->h_pend[q].slot].N;
         }
     }
     if (n == 0) return PF_OK;
@@ -569,11 +567,12 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
         CU(cudaGetLastError());
         const ModelOps ops = model_ops(m);
         InputRef ir{s->d_slot_in, 1, nullptr, 0, 0};
-        CU(ops.sample_sort(M, E, 1, true, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir));
+        CU(ops.sample_sort(M, E, 1, true, (int)ctas[m], ms, s->d_desc, s->d_map[m] + ests[m], ir));
         ModelInfo mi;
         model_info(m, &mi);
         const int virt = dependent_launch_pays((int)ctas[m], M, E, mi.S, s->device) ? 3 : 1;
-        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)ctas[m], ms, s->d_desc, s->d_map[m], ir, nullptr, virt));
+        CU(ops.exchange_resample(M, E, s->cfg.resampler, (int)(ests[m] + ctas[m]), ms, s->d_desc, s->d_map[m], ir,
+                                 nullptr, virt));
         CU(cudaEventRecord(s->join[m], ms));
         used[m] = true;
         first += cnt;

@@ -69,7 +69,7 @@ __device__ __forceinline__ void estimate_last_done(const FilterDesc& D, const St
         go[NV + 1] = (double)wi;
         X.grp_ctr[g] = 0;
     }
-    // second level: the same combination as estimate_groups
+    // second level: the same combination as estimate_group
     __syncwarp();
     __threadfence();
     last = 0;
