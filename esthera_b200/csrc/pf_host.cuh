@@ -91,6 +91,9 @@ ModelEntry model_entry(int id, const char* name, size_t init_offset)
     static_assert(Mdl::S >= 1 && Mdl::S <= PF_MAX_STATE && Mdl::K >= 1 && Mdl::NA >= 0 && Mdl::NA <= Mdl::S,
                   "model sizes out of range");
     static_assert(Mdl::C <= PF_MAX_CONTROL && Mdl::Z <= PF_MAX_MEAS, "control / measurement larger than pf_step_input");
+    static_assert(2 + Mdl::S + Mdl::NA + 2 <= pfdev::kPartStride,
+                  "a sub-filter's estimate row (key max, weight sum, S state sums, NA cosine sums, winner key and "
+                  "index) must fit kPartStride doubles: S + NA <= 28");
     uint32_t mask = 0;
     for (int a = 0; a < Mdl::NA; ++a) mask |= 1u << Mdl::angle_var(a);
     return {id, name, {Mdl::S, Mdl::K, Mdl::C, Mdl::Z, sizeof(Params)}, ops_of<Mdl>(), mask, Mdl::NA, init_offset};

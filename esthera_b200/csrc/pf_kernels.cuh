@@ -637,6 +637,65 @@ __global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const i
 }
 
 // ---------------------------------------------------------------------------
+// One warp: the sum over rows r < nr (<= 32) of sc_r * rows[r * kPartStride
+// + j] for every value j < NV (sc_r held by lane r), returned in lane j.  P =
+// 4, 2 or 1 lanes per value (as many as fit 32 / NV): lane (q, j) adds rows
+// q, q + P, q + 2P, ... in that order, loading them eight at a time (all of
+// them independent loads of contiguous rows), then an xor tree over the P
+// lanes.  A fixed order for a given NV.
+__device__ __forceinline__ double weighted_rows(const double* __restrict__ rows, int nr, double sc, int NV, int lane)
+{
+    const int P = NV <= 8 ? 4 : (NV <= 16 ? 2 : 1);
+    const int W = 32 / P, j = lane & (W - 1), q = lane / W;
+    const bool on = j < NV;
+    double a = 0.0;
+    for (int k0 = 0; k0 < W; k0 += 8) {
+        double v[8], w[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int r = q + P * (k0 + i);
+            w[i] = __shfl_sync(kFull, sc, r & 31);
+            v[i] = (on && r < nr) ? __ldcg(rows + (int64_t)r * kPartStride + j) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a += w[i] * v[i];
+    }
+    for (int o = W; o < 32; o <<= 1) a += __shfl_xor_sync(kFull, a, o);
+    return a;
+}
+
+// A group's row from its nr (<= 32) sub-filters' partial rows, one warp:
+// [0] the group's key maximum, [1 .. NV) the sums scaled to it, [NV] the
+// first-maximum winner's key, [NV + 1] its index (idx0 + the sub-filter).
+__device__ __forceinline__ void group_row(const FilterDesc& D, const double* __restrict__ part,
+                                          const float* __restrict__ winner, int nr, int NV, int idx0, int lane,
+                                          double* __restrict__ go)
+{
+    const bool valid = lane < nr;
+    const double l = valid ? __ldcg(part + (int64_t)lane * kPartStride) : -INFINITY;
+    double gl = l;
+    float wk = valid ? __ldcg(winner + lane) : -INFINITY;
+    int wi = valid ? lane : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
+        const float ok = __shfl_xor_sync(kFull, wk, o);
+        const int oi = __shfl_xor_sync(kFull, wi, o);
+        if (ok > wk || (ok == wk && oi < wi)) {
+            wk = ok;
+            wi = oi;
+        }
+    }
+    const double sc = valid ? (D.log_weights ? exp(l - gl) : 1.0) : 0.0;
+    const double a = weighted_rows(part, nr, sc, NV, lane);
+    if (lane >= 1 && lane < NV) go[lane] = a;
+    if (lane == 0) {
+        go[0] = D.log_weights ? gl : 0.0;
+        go[NV] = (double)wk;
+        go[NV + 1] = (double)(wi + idx0);
+    }
+}
+
 // Global winner (first maximum, thrust::max_element semantics,
 // pf_generic_soa.cu:1014-1017) + FP64 posterior mean, reduced in two fixed-order
 // levels inside the resampling kernel: warp 0 of the CTA of sub-filter 32g
@@ -648,83 +707,28 @@ __global__ void k_exchange_inplace(const FilterDesc* __restrict__ descs, const i
 // the global maximum gm and the winner (bk, bi) are known): the FP64 sums of
 // the NV values, then the fields written by different lanes at once -- lane v
 // the mean (or circular mean) of variable v, lane 16 + v the winner's
-// variable v from best_src, lane 0 the rest.  Each sum keeps one order: a
-// lane's groups ascending, then the xor-shuffle tree.
+// variable v from best_src, lane 0 the rest.  Each sum keeps one order: the
+// groups ascending in chunks of 32, the chunks' sums in order.
 template <int S>
 __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, int ng, int NV, double gm, float bk,
                                                int bi, const float* __restrict__ best_src, pf_estimate& E,
                                                int32_t step_no)
 {
     __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
-    constexpr int NVMAX = 2 + 2 * S;
     const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
     // the winner's state first: its load overlaps the sums
     const int bv = lane - PF_MAX_STATE;
     const float best_v = (bv >= 0 && bv < S) ? __ldcg(best_src + bv * D.T + (int64_t)best * D.M) : 0.0f;
-    const bool batched = S <= 3 && ng <= 64;
-    if (batched) {
-        // small states: every group row of the lane (groups lane, lane + 32)
-        // in one batch of loads; the same sums, in the same order, as the
-        // general loop below
-        double acc[NVMAX];
-#pragma unroll
-        for (int j = 0; j < NVMAX; ++j) acc[j] = 0.0;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int q = lane + 32 * r;
-            if (q < ng) {
-                const double* gq = D.gpart + (int64_t)q * kPartStride;
-                double v[NVMAX];
-#pragma unroll
-                for (int j = 0; j < NVMAX; ++j) v[j] = j < NV ? __ldcg(gq + j) : 0.0;
-                const double sq = D.log_weights ? exp(v[0] - gm) : 1.0;
-#pragma unroll
-                for (int j = 1; j < NVMAX; ++j)
-                    if (j < NV) acc[j] += sq * v[j];
-            }
-        }
-#pragma unroll
-        for (int j = 1; j < NVMAX; ++j) {
-            if (j < NV) {
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(kFull, acc[j], o);
-                if (lane == 0) s_acc[j] = acc[j];
-            }
-        }
+    // lane j sums value j over the groups, 32 rows at a time (weighted_rows)
+    double acc = 0.0;
+    for (int c = 0; c < ng; c += 32) {
+        const int nr = min(32, ng - c);
+        const double* rows = D.gpart + (int64_t)c * kPartStride;
+        const double sq =
+            lane < nr ? (D.log_weights ? exp(__ldcg(rows + (int64_t)lane * kPartStride) - gm) : 1.0) : 0.0;
+        acc += weighted_rows(rows, nr, sq, NV, lane);
     }
-    double sqv[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int q = lane + 32 * r;
-        sqv[r] = (!batched && q < ng) ? (D.log_weights ? exp(__ldcg(D.gpart + (int64_t)q * kPartStride) - gm) : 1.0)
-                                      : 0.0;
-    }
-    for (int j0 = 1; j0 < NV && !batched; j0 += 4) {
-        double a4[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int q = lane + 32 * r;
-            if (q < ng) {
-                const double* gq = D.gpart + (int64_t)q * kPartStride;
-#pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (j0 + c < NV) a4[c] += sqv[r] * __ldcg(gq + j0 + c);
-            }
-        }
-        for (int q = lane + 128; q < ng; q += 32) {
-            const double* gq = D.gpart + (int64_t)q * kPartStride;
-            const double sq = D.log_weights ? exp(__ldcg(gq) - gm) : 1.0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (j0 + c < NV) a4[c] += sq * __ldcg(gq + j0 + c);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) a4[c] += __shfl_xor_sync(kFull, a4[c], o);
-            if (lane == 0 && j0 + c < NV) s_acc[j0 + c] = a4[c];
-        }
-    }
+    if (lane >= 1 && lane < NV) s_acc[lane] = acc;
     __syncwarp();
     const double W = s_acc[1];
     if (lane < PF_MAX_STATE) {
@@ -794,48 +798,12 @@ template <int S>
 __device__ __forceinline__ void estimate_group(const FilterDesc& D, int g, const InputRef& in, int32_t* step_ctr)
 {
     if (threadIdx.x >= 32) return;
-    constexpr int NVMAX = 2 + 2 * S;
     const int lane = threadIdx.x;
     const int b = g << 5, ng = (D.N + 31) >> 5;
     const int NV = 2 + S + D.na;
-    const int sb = b + lane;
-    const bool valid = sb < D.N;
-    const double* pp = D.part + (int64_t)(valid ? sb : b) * kPartStride;
-    // small states: the lane's whole partial row in one batch of loads (one
-    // round trip); large states read each value where it is used
-    constexpr int NROW = S <= 3 ? NVMAX : 1;
-    double row[NROW];
-#pragma unroll
-    for (int j = 0; j < NROW; ++j) row[j] = (valid && j < NV) ? pp[j] : 0.0;
-    double gl = valid ? (S <= 3 ? row[0] : pp[0]) : -INFINITY;
-    float wk = valid ? D.winner[sb] : -INFINITY;
-    int wi = valid ? sb : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
-        const float ok = __shfl_xor_sync(kFull, wk, o);
-        const int oi = __shfl_xor_sync(kFull, wi, o);
-        if (ok > wk || (ok == wk && oi < wi)) {
-            wk = ok;
-            wi = oi;
-        }
-    }
-    const double sc = valid ? (D.log_weights ? exp((S <= 3 ? row[0] : pp[0]) - gl) : 1.0) : 0.0;
-    double* go = D.gpart + (int64_t)g * kPartStride;
-#pragma unroll
-    for (int j = 1; j < NVMAX; ++j) {
-        if (j < NV) {
-            double v = valid ? sc * (S <= 3 ? row[j < NROW ? j : 0] : pp[j]) : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-            if (lane == 0) go[j] = v;
-        }
-    }
-    if (lane == 0) {
-        go[0] = D.log_weights ? gl : 0.0;
-        go[NV] = (double)wk;
-        go[NV + 1] = (double)(wi + D.b0);  // the filter-wide index (a shard's sub-filters start at b0)
-    }
+    // winners as filter-wide indices (a shard's sub-filters start at b0)
+    group_row(D, D.part + (int64_t)b * kPartStride, D.winner + b, min(32, D.N - b), NV, b + D.b0, lane,
+              D.gpart + (int64_t)g * kPartStride);
     if (D.shard) return;  // the shards' group rows are combined across shards (pf_shard_estimate)
     __syncwarp();
     __threadfence();

@@ -34,41 +34,10 @@ __device__ __forceinline__ void estimate_last_done(const FilterDesc& D, const St
     last = __shfl_sync(kFull, last, 0);
     if (!last) return;
     __threadfence();
-    constexpr int NVMAX = 2 + 2 * S;
     const int NV = 2 + S + D.na;
-    const int sb = 32 * g + lane;
-    const bool valid = sb < D.N;
-    const double* pp = D.part + (int64_t)(valid ? sb : 32 * g) * kPartStride;
-    double gl = valid ? __ldcg(pp) : -INFINITY;
-    float wk = valid ? __ldcg(D.winner + sb) : -INFINITY;
-    int wi = valid ? sb : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
-        const float ok = __shfl_xor_sync(kFull, wk, o);
-        const int oi = __shfl_xor_sync(kFull, wi, o);
-        if (ok > wk || (ok == wk && oi < wi)) {
-            wk = ok;
-            wi = oi;
-        }
-    }
-    const double sc = valid ? (D.log_weights ? exp(__ldcg(pp) - gl) : 1.0) : 0.0;
-    double* go = D.gpart + (int64_t)g * kPartStride;
-#pragma unroll
-    for (int j = 1; j < NVMAX; ++j) {
-        if (j < NV) {
-            double v = valid ? sc * __ldcg(pp + j) : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-            if (lane == 0) go[j] = v;
-        }
-    }
-    if (lane == 0) {
-        go[0] = D.log_weights ? gl : 0.0;
-        go[NV] = (double)wk;
-        go[NV + 1] = (double)wi;
-        X.grp_ctr[g] = 0;
-    }
+    group_row(D, D.part + (int64_t)(32 * g) * kPartStride, D.winner + 32 * g, gsize, NV, 32 * g, lane,
+              D.gpart + (int64_t)g * kPartStride);
+    if (lane == 0) X.grp_ctr[g] = 0;
     // second level: the same combination as estimate_group
     __syncwarp();
     __threadfence();

@@ -21,7 +21,8 @@
  *   static constexpr int S, K, NA, C, Z;
  *       state floats (1..PF_MAX_STATE), standard normals drawn per particle
  *       and step (>= 1), angular state variables (0..S; their posterior mean
- *       is circular), control and measurement floats read from pf_step_input.
+ *       is circular; S + NA <= 28), control and measurement floats read from
+ *       pf_step_input.
  *   __host__ __device__ static constexpr int angle_var(int a);
  *       the state index of the a-th angular variable.
  *   struct Consts { ... };
