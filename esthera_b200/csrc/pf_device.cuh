@@ -393,30 +393,35 @@ __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], floa
         v[e] = k[e];
         nan |= k[e] != k[e];
     }
+    // the keys alone through a bitonic network in its mirrored form: the first
+    // stage of each merge pairs p with p ^ (size - 1), the later ones p with
+    // p ^ stride, and every comparator leaves the larger key at the lower
+    // position (no direction bit per block)
 #pragma unroll
     for (int size = 2; size <= M; size <<= 1) {
 #pragma unroll
         for (int stride = size / 2; stride > 0; stride >>= 1) {
+            const bool first = stride == size / 2;
             if (stride < E) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    if ((e & stride) == 0) {
-                        // descending where (p & size) == 0: the larger key first
-                        const bool asc = ((E * tid + e) & size) != 0;
-                        const float hi = fmaxf(v[e], v[e + stride]), lo = fminf(v[e], v[e + stride]);
-                        v[e] = asc ? lo : hi;
-                        v[e + stride] = asc ? hi : lo;
+                    const int pe = first ? (e ^ (size - 1)) : (e ^ stride);
+                    if (e < pe) {
+                        const float hi = fmaxf(v[e], v[pe]), lo = fminf(v[e], v[pe]);
+                        v[e] = hi;
+                        v[pe] = lo;
                     }
                 }
             } else if (stride < (32 / TP) * E) {
-                const int lm = stride / E;
-                // p & size and the thread's side of the pair are the same for all e here
-                const bool keep_max = (((E * tid) & size) != 0) == ((tid & lm) != 0);
+                // partner thread tid ^ lm (first stage: tid ^ (size / E - 1),
+                // element E - 1 - e); the lower thread of the pair keeps the maxima
+                const int lm = first ? size / E - 1 : stride / E;
+                const bool keep_max = (tid & (stride / E)) == 0;
+                float o[E];
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const float o = __shfl_xor_sync(kFull, v[e], lm * TP);
-                    v[e] = keep_max ? fmaxf(v[e], o) : fminf(v[e], o);
-                }
+                for (int e = 0; e < E; ++e) o[e] = __shfl_xor_sync(kFull, v[first ? E - 1 - e : e], lm * TP);
+#pragma unroll
+                for (int e = 0; e < E; ++e) v[e] = keep_max ? fmaxf(v[e], o[e]) : fminf(v[e], o[e]);
             } else {
                 __syncthreads();
                 if (writer) {
@@ -424,10 +429,11 @@ __device__ __forceinline__ bool rank_sort_desc(float (&k)[E], int (&ix)[E], floa
                     for (int e = 0; e < E; ++e) sk[E * tid + e] = v[e];
                 }
                 __syncthreads();
-                const bool keep_max = (((E * tid) & size) != 0) == (((E * tid) & stride) != 0);
+                const bool keep_max = ((E * tid) & stride) == 0;
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const float o = sk[(E * tid + e) ^ stride];
+                    const int p = E * tid + e;
+                    const float o = sk[first ? p ^ (size - 1) : p ^ stride];
                     v[e] = keep_max ? fmaxf(v[e], o) : fminf(v[e], o);
                 }
             }
