@@ -664,30 +664,73 @@ __device__ __forceinline__ double weighted_rows(const double* __restrict__ rows,
     return a;
 }
 
+// The same sums in the same order for rows of more than 8 values, loaded
+// sixteen at a time, the first batch issued before scale() -- which computes
+// lane r's factor sc_r and whose own loads and reductions then overlap the
+// rows in flight (rows of up to 8 values keep weighted_rows: their kernels'
+// registers hold no more).
+template <class Scale>
+__device__ __forceinline__ double weighted_rows_late(const double* __restrict__ rows, int nr, int NV, int lane,
+                                                     Scale scale)
+{
+    constexpr int B = 16;
+    const int P = NV <= 8 ? 4 : (NV <= 16 ? 2 : 1);
+    const int W = 32 / P, j = lane & (W - 1), q = lane / W;
+    const bool on = j < NV;
+    double a = 0.0, sc = 0.0;
+    for (int k0 = 0; k0 < W; k0 += B) {
+        double v[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            const int r = q + P * (k0 + i);
+            v[i] = (k0 + i < W && on && r < nr) ? __ldcg(rows + (int64_t)r * kPartStride + j) : 0.0;
+        }
+        if (k0 == 0) sc = scale();
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            if (k0 + i < W) {  // warp-uniform
+                const double w = __shfl_sync(kFull, sc, (q + P * (k0 + i)) & 31);
+                a += w * v[i];
+            }
+        }
+    }
+    for (int o = W; o < 32; o <<= 1) a += __shfl_xor_sync(kFull, a, o);
+    return a;
+}
+
 // A group's row from its nr (<= 32) sub-filters' partial rows, one warp:
 // [0] the group's key maximum, [1 .. NV) the sums scaled to it, [NV] the
 // first-maximum winner's key, [NV + 1] its index (idx0 + the sub-filter).
+template <int S>
 __device__ __forceinline__ void group_row(const FilterDesc& D, const double* __restrict__ part,
                                           const float* __restrict__ winner, int nr, int NV, int idx0, int lane,
                                           double* __restrict__ go)
 {
     const bool valid = lane < nr;
     const double l = valid ? __ldcg(part + (int64_t)lane * kPartStride) : -INFINITY;
+    const float lw = valid ? __ldcg(winner + lane) : -INFINITY;
     double gl = l;
-    float wk = valid ? __ldcg(winner + lane) : -INFINITY;
+    float wk = lw;
     int wi = valid ? lane : 0x7fffffff;
+    auto reduce = [&] {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
-        const float ok = __shfl_xor_sync(kFull, wk, o);
-        const int oi = __shfl_xor_sync(kFull, wi, o);
-        if (ok > wk || (ok == wk && oi < wi)) {
-            wk = ok;
-            wi = oi;
+        for (int o = 16; o > 0; o >>= 1) {
+            gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
+            const float ok = __shfl_xor_sync(kFull, wk, o);
+            const int oi = __shfl_xor_sync(kFull, wi, o);
+            if (ok > wk || (ok == wk && oi < wi)) {
+                wk = ok;
+                wi = oi;
+            }
         }
+        return valid ? (D.log_weights ? exp(l - gl) : 1.0) : 0.0;
+    };
+    double a;
+    if constexpr (2 + 2 * S <= 8) {
+        a = weighted_rows(part, nr, reduce(), NV, lane);
+    } else {
+        a = weighted_rows_late(part, nr, NV, lane, reduce);
     }
-    const double sc = valid ? (D.log_weights ? exp(l - gl) : 1.0) : 0.0;
-    const double a = weighted_rows(part, nr, sc, NV, lane);
     if (lane >= 1 && lane < NV) go[lane] = a;
     if (lane == 0) {
         go[0] = D.log_weights ? gl : 0.0;
@@ -724,9 +767,13 @@ __device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, in
     for (int c = 0; c < ng; c += 32) {
         const int nr = min(32, ng - c);
         const double* rows = D.gpart + (int64_t)c * kPartStride;
-        const double sq =
-            lane < nr ? (D.log_weights ? exp(__ldcg(rows + (int64_t)lane * kPartStride) - gm) : 1.0) : 0.0;
-        acc += weighted_rows(rows, nr, sq, NV, lane);
+        const double l = lane < nr ? __ldcg(rows + (int64_t)lane * kPartStride) : 0.0;
+        auto scale = [&] { return lane < nr ? (D.log_weights ? exp(l - gm) : 1.0) : 0.0; };
+        if constexpr (2 + 2 * S <= 8) {
+            acc += weighted_rows(rows, nr, scale(), NV, lane);
+        } else {
+            acc += weighted_rows_late(rows, nr, NV, lane, scale);
+        }
     }
     if (lane >= 1 && lane < NV) s_acc[lane] = acc;
     __syncwarp();
@@ -802,7 +849,7 @@ __device__ __forceinline__ void estimate_group(const FilterDesc& D, int g, const
     const int b = g << 5, ng = (D.N + 31) >> 5;
     const int NV = 2 + S + D.na;
     // winners as filter-wide indices (a shard's sub-filters start at b0)
-    group_row(D, D.part + (int64_t)b * kPartStride, D.winner + b, min(32, D.N - b), NV, b + D.b0, lane,
+    group_row<S>(D, D.part + (int64_t)b * kPartStride, D.winner + b, min(32, D.N - b), NV, b + D.b0, lane,
               D.gpart + (int64_t)g * kPartStride);
     if (D.shard) return;  // the shards' group rows are combined across shards (pf_shard_estimate)
     __syncwarp();
@@ -1012,25 +1059,43 @@ __device__ __forceinline__ int resample_from(const FilterDesc& D, int b, const f
             }
         }
     } else {
-        // large states: straight into shared memory (cp.async), the
-        // exchanged slots overwritten by their owner once its copies landed
-        cp_async_floats<E>(kb + E * tid, src_key + base);
+        // large states: straight into shared memory (cp.async).  A thread
+        // owning exchanged slots copies slot by slot, each from its source --
+        // its own row, a neighbour's sorted copy or a shard's halo block -- so
+        // the neighbours' values arrive with the rows, in one round trip
+        if (!xch) {
+            cp_async_floats<E>(kb + E * tid, src_key + base);
 #pragma unroll
-        for (int v = 0; v < S; ++v) cp_async_floats<E>(tile + v * M + E * tid, src_tmp + v * T + base);
-        cp_async_wait();
-        if (dec_u - 1.0f > D.freq) return PF_RS_KEPT;
-        if (xch) {
+            for (int v = 0; v < S; ++v) cp_async_floats<E>(tile + v * M + E * tid, src_tmp + v * T + base);
+        } else {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int x = M - 1 - (E * tid + e);
+                const float* ks = src_key + base + e;
+                const float* vs = src_tmp + base + e;
+                int64_t vstride = T;
                 if (x < nx) {
-                    float xv[S];
-                    exchange_fetch<S>(D, src_key, src_tmp, T, exchange_source(D, b, x), kb[E * tid + e], xv);
-#pragma unroll
-                    for (int v = 0; v < S; ++v) tile[v * M + E * tid + e] = xv[v];
+                    const int64_t g = exchange_source(D, b, x);
+                    if (g >= 0) {
+                        ks = src_key + g;
+                        vs = src_tmp + g;
+                    } else {  // a shard's halo block: key row, then the state rows
+                        const int64_t i = -(g + 1);
+                        const int P = D.dx * D.t;
+                        const int h = (int)(i / P);
+                        const float* blk = D.halo + (int64_t)h * (1 + S) * P + (i - (int64_t)h * P);
+                        ks = blk;
+                        vs = blk + P;
+                        vstride = P;
+                    }
                 }
+                cp_async_floats<1>(kb + E * tid + e, ks);
+#pragma unroll
+                for (int v = 0; v < S; ++v) cp_async_floats<1>(tile + v * M + E * tid + e, vs + v * vstride);
             }
         }
+        cp_async_wait();
+        if (dec_u - 1.0f > D.freq) return PF_RS_KEPT;
     }
     // this thread's own slots (copied, or patched by this thread) are readable
     // already; the barrier orders every slot's patch before the reads below

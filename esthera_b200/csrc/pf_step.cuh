@@ -35,7 +35,7 @@ __device__ __forceinline__ void estimate_last_done(const FilterDesc& D, const St
     if (!last) return;
     __threadfence();
     const int NV = 2 + S + D.na;
-    group_row(D, D.part + (int64_t)(32 * g) * kPartStride, D.winner + 32 * g, gsize, NV, 32 * g, lane,
+    group_row<S>(D, D.part + (int64_t)(32 * g) * kPartStride, D.winner + 32 * g, gsize, NV, 32 * g, lane,
               D.gpart + (int64_t)g * kPartStride);
     if (lane == 0) X.grp_ctr[g] = 0;
     // second level: the same combination as estimate_group
