@@ -550,6 +550,10 @@ def main():
         for name, ms in f.last_step_timing():
             phase_ms.setdefault(name, []).append(ms)
     f.set_timing(False)
+    # one untimed submit / collect: it captures the step graph over the pinned
+    # rings (set-up done once per filter, like the device run's warm-up)
+    f.submit(E.step_input(inputs[0]))
+    f.collect()
     f.set_initial_state(np.array(p.init_state[:E.model_info(W["model"])[0]], np.float32))
 
     # end to end through the public API, pipelined: pf_step_submit (host input
