@@ -415,7 +415,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=200)
     ap.add_argument("--phase-steps", type=int, default=100, help="steps of the per-kernel timing pass")
-    ap.add_argument("--ppt", type=int, default=4, help="particles per thread (split pipeline)")
+    ap.add_argument("--ppt", type=int, default=0,
+                    help="particles per thread (split pipeline; 0: the library's default for the model and m)")
     ap.add_argument("--pipeline", default="split", choices=["fused", "split"])
     ap.add_argument("--workload", default="plain", choices=["plain", "arm", "beacon", "batched", "served"])
     ap.add_argument("--serve-rate", type=float, default=2000.0)

@@ -141,7 +141,7 @@ bool pfhost::dependent_launch_pays(int grid, int M, int E, int S, int device)
         }
         sms[device].store(n, std::memory_order_relaxed);
     }
-    return grid > n * pf_min_blocks(M / E, pf_k1_warps(S));
+    return grid > n * pf_min_blocks(M / E, pf_k1_warps(S, E));
 }
 
 extern "C" pf_status pf_model_info(pf_model_id model, int32_t* S, int32_t* K, int32_t* C, int32_t* Z)
@@ -341,11 +341,11 @@ extern "C" pf_status pf_config_default(pf_config* c)
     return PF_OK;
 }
 
-int pfhost::default_ppt(int M)
+int pfhost::default_ppt(int M, int S)
 {
     if (M <= 32) return 1;
     if (M <= 64) return 2;
-    return 4;
+    return S > 3 ? 2 : 4;  // large states: two particles per thread (pf_k1_warps)
 }
 
 void pfhost::torus_dims(int N, int* dx, int* dy)
@@ -396,7 +396,7 @@ static pf_status validate(const pf_config* c, int model, const ModelInfo& mi, in
         return fail(PF_ERR_INVALID, "the phased pipeline uses the reference RNG layout (rng = PF_RNG_REFLAYOUT)");
     if (c->pipeline != PF_PIPELINE_FUSED && c->pipeline != PF_PIPELINE_PHASED && c->pipeline != PF_PIPELINE_SPLIT)
         return fail(PF_ERR_INVALID, "unknown pipeline");
-    *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M);
+    *E = c->particles_per_thread > 0 ? c->particles_per_thread : default_ppt(M, mi.S);
     if (!me_supported(M, *E))
         return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", *E, M);
     if (c->threads_per_particle < 0 || c->threads_per_particle > 2)
@@ -1184,7 +1184,7 @@ extern "C" pf_status pfk_boxmuller(float* data, int64_t n)
     return PF_OK;
 }
 
-static int pick_ppt(int m, int ppt) { return ppt > 0 ? ppt : default_ppt(m); }
+static int pick_ppt(int m, int ppt) { return ppt > 0 ? ppt : default_ppt(m, 1); }
 
 extern "C" pf_status pfk_bitonic_sort(float* keys, int32_t* idx, int32_t m, int32_t nsub, int32_t ppt)
 {

@@ -216,7 +216,7 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
     const int M = cfg->particles_per_subfilter;
     if (M < 32 || M > 1024 || (M & (M - 1)))
         return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
-    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M);
+    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M, mi.S);
     if (!me_supported(M, E)) return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E, M);
     if (cfg->rng != PF_RNG_SUBFILTER) return fail(PF_ERR_UNSUPPORTED, "batched filters use per-sub-filter streams");
     if (cfg->pipeline == PF_PIPELINE_PHASED)
@@ -326,7 +326,7 @@ extern "C" pf_status pf_batch_create(const pf_config* cfg, pf_model_id model, in
         if (!ns) continue;
         const int ec = c == M ? E : (cfg->particles_per_thread > 0 && me_supported(c, cfg->particles_per_thread)
                                          ? cfg->particles_per_thread
-                                         : default_ppt(c));
+                                         : default_ppt(c, mi.S));
         // two threads per particle where the sampling kernel's CTA stays within 1024 threads
         const int tp = cfg->threads_per_particle == 2 && 2 * c / ec <= 1024 ? 2 : 1;
         B->groups.push_back(pf_batch::Group{c, ec, tp, ns, ne, 0});

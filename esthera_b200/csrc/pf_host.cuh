@@ -26,8 +26,9 @@ pf_status require_gpu(int device);
 
 // Particles per thread when a configuration leaves it at 0 (the same for
 // single filters, batches and the server: the same configuration gives the
-// same bits everywhere): 1 for m = 32, 2 for m = 64, else 4.
-int default_ppt(int M);
+// same bits everywhere): 1 for m = 32, 2 for m = 64, else 4 for states of up
+// to 3 variables and 2 for larger states (S is the model's state size).
+int default_ppt(int M, int S);
 
 struct ModelInfo {
     int S, K, C, Z;

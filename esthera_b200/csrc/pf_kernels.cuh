@@ -124,7 +124,17 @@ __host__ __device__ constexpr int pf_min_blocks(int threads, int warps)
 {
     return (warps * 32 + threads - 1) / threads > 32 ? 32 : (warps * 32 + threads - 1) / threads;
 }
-__host__ __device__ constexpr int pf_k1_warps(int S) { return S <= 3 ? PF_K1_WARPS_SMALL : PF_K1_WARPS_LARGE; }
+// Large states with 2 or fewer particles per thread hold half the registers a
+// thread of 4 needs: their budget is 32 warps (64 registers; the DH arm's
+// sampling kernel at m = 256 runs 26.4 us against 29.6 us at 128 registers
+// and 28.8 us with 4 particles per thread).
+#ifndef PF_K1_WARPS_LARGE_E2
+#define PF_K1_WARPS_LARGE_E2 32
+#endif
+__host__ __device__ constexpr int pf_k1_warps(int S, int E = 4)
+{
+    return S <= 3 ? PF_K1_WARPS_SMALL : (E <= 2 ? PF_K1_WARPS_LARGE_E2 : PF_K1_WARPS_LARGE);
+}
 __host__ __device__ constexpr int pf_k2_warps(int S) { return S <= 3 ? PF_K2_WARPS_SMALL : PF_K2_WARPS_LARGE; }
 
 struct InputRef {
@@ -329,7 +339,7 @@ __device__ __forceinline__ void write_partials(const FilterDesc& D, int b, float
 // sort together, and lane 2g alone writes (its partials carry the particles).
 // ---------------------------------------------------------------------------
 template <class Mdl, int M, int E, bool FR, int TP = 1>
-__global__ void __launch_bounds__(TP * M / E, pf_min_blocks(TP * M / E, pf_k1_warps(Mdl::S) - (TP - 1) * 4)) k_sample_sort(const FilterDesc* __restrict__ descs,
+__global__ void __launch_bounds__(TP * M / E, pf_min_blocks(TP * M / E, pf_k1_warps(Mdl::S, E) - (TP - 1) * 4)) k_sample_sort(const FilterDesc* __restrict__ descs,
                                                        const int2* __restrict__ cta_map, InputRef in)
 {
     constexpr int NT = TP * M / E, S = Mdl::S, K = Mdl::K, NA = Mdl::NA;

@@ -132,7 +132,7 @@ struct pf_server {
     int device = 0;
     int64_t budget = 0, used = 0;
     int max_filters = 0;
-    int E = 2;
+    int E[PF_NUM_MODELS] = {};  // particles per thread of each model's kernels
     int64_t nbm[PF_NUM_MODELS] = {}, draws[PF_NUM_MODELS] = {};
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
@@ -205,8 +205,14 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     const int M = cfg->particles_per_subfilter;
     if (M < 32 || M > 1024 || (M & (M - 1)))
         return fail(PF_ERR_UNSUPPORTED, "particles per sub-filter must be a power of two in [32, 1024], got %d", M);
-    const int E = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M);
-    if (!me_supported(M, E)) return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E, M);
+    int E[PF_NUM_MODELS];
+    for (int m = 0; m < PF_NUM_MODELS; ++m) {
+        ModelInfo mi;
+        model_info(m, &mi);
+        E[m] = cfg->particles_per_thread > 0 ? cfg->particles_per_thread : default_ppt(M, mi.S);
+        if (!me_supported(M, E[m]))
+            return fail(PF_ERR_UNSUPPORTED, "particles per thread %d not built for m=%d", E[m], M);
+    }
     if (cfg->exchange != PF_EXCHANGE_NONE && cfg->exchange != PF_EXCHANGE_RING)
         return fail(PF_ERR_UNSUPPORTED, "served filters exchange by ring (or not at all)");
     if (cfg->exchange == PF_EXCHANGE_RING && (cfg->num_transfer < 0 || 2 * cfg->num_transfer > M))
@@ -225,7 +231,7 @@ extern "C" pf_status pf_server_create(const pf_config* cfg, int64_t hbm_budget, 
     s->device = cfg->device;
     s->budget = hbm_budget;
     s->max_filters = max_filters;
-    s->E = E;
+    for (int m = 0; m < PF_NUM_MODELS; ++m) s->E[m] = E[m];
     for (int m = 0; m < PF_NUM_MODELS; ++m) {
         ModelInfo mi;
         model_info(m, &mi);
@@ -547,7 +553,7 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
         }
     }
     if (n == 0) return PF_OK;
-    const int M = s->cfg.particles_per_subfilter, E = s->E;
+    const int M = s->cfg.particles_per_subfilter;
     cudaStream_t st = s->stream;
     CU(cudaMemcpyAsync(s->d_pend, s->h_pend, sizeof(Pending) * n, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(s->d_in, s->h_in, sizeof(pf_step_input) * n, cudaMemcpyHostToDevice, st));
@@ -566,6 +572,7 @@ extern "C" pf_status pf_server_launch(pf_server* s, int32_t* n_launched)
                                           s->d_map[m]);
         CU(cudaGetLastError());
         const ModelOps ops = model_ops(m);
+        const int E = s->E[m];
         InputRef ir{s->d_slot_in, 1, nullptr, 0, 0};
         CU(ops.sample_sort(M, E, 1, true, (int)ctas[m], ms, s->d_desc, s->d_map[m] + ests[m], ir));
         ModelInfo mi;

@@ -98,7 +98,8 @@ typedef struct {
     uint32_t mtgp_mask;              /* PF_MTGP_MASK_PARAMS or PF_MTGP_MASK_CUDA_REF */
     int32_t log_weights;             /* 1: FP32 max-subtracted log weights; 0: linear FP32 weights */
     int32_t pipeline;                /* pf_pipeline */
-    int32_t particles_per_thread;    /* 0 = pick (1 for m = 32, 2 for m = 64, else 4); built pairs
+    int32_t particles_per_thread;    /* 0 = pick (1 for m = 32, 2 for m = 64, else 4 for states of up to
+                                        3 variables and 2 for larger ones); built pairs
                                         (m, ppt): (32,1) (64,2) (128,2|4) (256,2|4|8) (512,2|4|16)
                                         (1024,2|4) */
     int32_t device;                  /* CUDA device ordinal */
