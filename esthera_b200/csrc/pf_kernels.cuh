@@ -708,192 +708,6 @@ __device__ __forceinline__ double weighted_rows_late(const double* __restrict__ 
     return a;
 }
 
-// A group's row from its nr (<= 32) sub-filters' partial rows, one warp:
-// [0] the group's key maximum, [1 .. NV) the sums scaled to it, [NV] the
-// first-maximum winner's key, [NV + 1] its index (idx0 + the sub-filter).
-template <int S>
-__device__ __forceinline__ void group_row(const FilterDesc& D, const double* __restrict__ part,
-                                          const float* __restrict__ winner, int nr, int NV, int idx0, int lane,
-                                          double* __restrict__ go)
-{
-    const bool valid = lane < nr;
-    const double l = valid ? __ldcg(part + (int64_t)lane * kPartStride) : -INFINITY;
-    const float lw = valid ? __ldcg(winner + lane) : -INFINITY;
-    double gl = l;
-    float wk = lw;
-    int wi = valid ? lane : 0x7fffffff;
-    auto reduce = [&] {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
-            const float ok = __shfl_xor_sync(kFull, wk, o);
-            const int oi = __shfl_xor_sync(kFull, wi, o);
-            if (ok > wk || (ok == wk && oi < wi)) {
-                wk = ok;
-                wi = oi;
-            }
-        }
-        return valid ? (D.log_weights ? exp(l - gl) : 1.0) : 0.0;
-    };
-    double a;
-    if constexpr (2 + 2 * S <= 8) {
-        a = weighted_rows(part, nr, reduce(), NV, lane);
-    } else {
-        a = weighted_rows_late(part, nr, NV, lane, reduce);
-    }
-    if (lane >= 1 && lane < NV) go[lane] = a;
-    if (lane == 0) {
-        go[0] = D.log_weights ? gl : 0.0;
-        go[NV] = (double)wk;
-        go[NV + 1] = (double)(wi + idx0);
-    }
-}
-
-// Global winner (first maximum, thrust::max_element semantics,
-// pf_generic_soa.cu:1014-1017) + FP64 posterior mean, reduced in two fixed-order
-// levels inside the resampling kernel: warp 0 of the CTA of sub-filter 32g
-// combines sub-filters 32g..32g+31 (all partials are final when that kernel
-// starts); the last group to finish (atomic ticket) combines the groups in
-// index order and writes the estimate.  Deterministic for a given N.
-// ---------------------------------------------------------------------------
-// The global estimate from the group partials gpart[0..ng) (one warp, after
-// the global maximum gm and the winner (bk, bi) are known): the FP64 sums of
-// the NV values, then the fields written by different lanes at once -- lane v
-// the mean (or circular mean) of variable v, lane 16 + v the winner's
-// variable v from best_src, lane 0 the rest.  Each sum keeps one order: the
-// groups ascending in chunks of 32, the chunks' sums in order.
-template <int S>
-__device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, int ng, int NV, double gm, float bk,
-                                               int bi, const float* __restrict__ best_src, pf_estimate& E,
-                                               int32_t step_no)
-{
-    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
-    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
-    // the winner's state first: its load overlaps the sums
-    const int bv = lane - PF_MAX_STATE;
-    const float best_v = (bv >= 0 && bv < S) ? __ldcg(best_src + bv * D.T + (int64_t)best * D.M) : 0.0f;
-    // lane j sums value j over the groups, 32 rows at a time (weighted_rows)
-    double acc = 0.0;
-    for (int c = 0; c < ng; c += 32) {
-        const int nr = min(32, ng - c);
-        const double* rows = D.gpart + (int64_t)c * kPartStride;
-        const double l = lane < nr ? __ldcg(rows + (int64_t)lane * kPartStride) : 0.0;
-        auto scale = [&] { return lane < nr ? (D.log_weights ? exp(l - gm) : 1.0) : 0.0; };
-        if constexpr (2 + 2 * S <= 8) {
-            acc += weighted_rows(rows, nr, scale(), NV, lane);
-        } else {
-            acc += weighted_rows_late(rows, nr, NV, lane, scale);
-        }
-    }
-    if (lane >= 1 && lane < NV) s_acc[lane] = acc;
-    __syncwarp();
-    const double W = s_acc[1];
-    if (lane < PF_MAX_STATE) {
-        const int v = lane;
-        double m = 0.0;
-        if (v < S) {
-            if ((D.angle_mask >> v) & 1u) {
-                const int a = __popc(D.angle_mask & ((1u << v) - 1u));
-                m = atan2(s_acc[2 + v], s_acc[2 + S + a]);
-            } else {
-                m = s_acc[2 + v] / W;
-            }
-        }
-        E.mean[v] = m;
-    } else {
-        E.best[bv] = best_v;
-    }
-    if (lane == 0) {
-        const double lg = D.log_weights ? gm : 0.0;
-        E.log_norm = lg + log(W);
-        E.best_key = bk;
-        E.best_subfilter = best;
-        E.step = step_no;
-        E.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
-    }
-    __syncwarp();
-}
-
-// The global estimate from the group partial rows gpart[0..ng) (one warp): the
-// global maximum, the first-maximum winner, then estimate_write (whose winner
-// state is read at best_src + v T + winner M).
-template <int S>
-__device__ __forceinline__ void estimate_final(const FilterDesc& D, int lane, int ng, int NV,
-                                               const float* __restrict__ best_src, pf_estimate& E, int32_t step_no)
-{
-    double gm = -INFINITY;
-    float bk = -INFINITY;
-    int bi = 0x7fffffff;
-#pragma unroll 2
-    for (int q = lane; q < ng; q += 32) {
-        const double* gq = D.gpart + (int64_t)q * kPartStride;
-        gm = fmax(gm, __ldcg(gq));
-        const float k = (float)__ldcg(gq + NV);
-        const int i = (int)__ldcg(gq + NV + 1);
-        if (k > bk || (k == bk && i < bi)) {
-            bk = k;
-            bi = i;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gm = fmax(gm, __shfl_xor_sync(kFull, gm, o));
-        const float ok = __shfl_xor_sync(kFull, bk, o);
-        const int oi = __shfl_xor_sync(kFull, bi, o);
-        if (ok > bk || (ok == bk && oi < bi)) {
-            bk = ok;
-            bi = oi;
-        }
-    }
-    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, best_src, E, step_no);
-}
-
-// Group g's estimate row from its 32 sub-filters' partial rows (one warp);
-// the last group to finish (ticket) combines every group row into the
-// filter's estimate.
-template <int S>
-__device__ __forceinline__ void estimate_group(const FilterDesc& D, int g, const InputRef& in, int32_t* step_ctr)
-{
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    const int b = g << 5, ng = (D.N + 31) >> 5;
-    const int NV = 2 + S + D.na;
-    // winners as filter-wide indices (a shard's sub-filters start at b0)
-    group_row<S>(D, D.part + (int64_t)b * kPartStride, D.winner + b, min(32, D.N - b), NV, b + D.b0, lane,
-              D.gpart + (int64_t)g * kPartStride);
-    if (D.shard) return;  // the shards' group rows are combined across shards (pf_shard_estimate)
-    __syncwarp();
-    __threadfence();
-    int last = 0;
-    if (lane == 0) last = atomicAdd(D.est_ctr, 1) == ng - 1;
-    last = __shfl_sync(kFull, last, 0);
-    if (!last) return;
-    __threadfence();
-    estimate_final<S>(D, lane, ng, NV, D.tmp, D.est[step_index(in)], in.ctr ? *in.ctr + 1 : 0);
-    if (lane == 0) {
-        *D.est_ctr = 0;
-        __threadfence();
-        if (step_ctr) *step_ctr += 1;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Exchange + resample + gather, one CTA per sub-filter.  `virt`: apply the
-// exchange virtually (read the neighbours' slots straight from tmp).
-// Resampling restates resampling (pf_generic_soa.cu:415-453) for
-// PF_RESAMPLE_REFERENCE, resampling_valias (resampling-valias.cl:214-300)
-// for PF_RESAMPLE_VOSE; PF_RESAMPLE_SYSTEMATIC uses the FP64 scan.
-// ---------------------------------------------------------------------------
-template <int S, int M, int E, int RES>
-constexpr size_t k2_smem()
-{
-    size_t s = (size_t)M * 4 + (size_t)S * M * 4;  // keys + state tile
-    if (RES == PF_RESAMPLE_SYSTEMATIC) s += 0;       // the scan stays in registers, the runs reuse the keys
-    else if (RES == PF_RESAMPLE_REFERENCE) s += (size_t)M * 4;
-    else s += (size_t)M * 16;  // prob, alias, work list, scratch
-    return s;
-}
-
 // E consecutive floats global -> shared without passing through registers
 // (cp.async; both addresses aligned to 4E bytes).  cp_async_wait() waits for
 // this thread's copies.
@@ -917,6 +731,320 @@ __device__ __forceinline__ void cp_async_floats(float* dst, const float* src)
 __device__ __forceinline__ void cp_async_wait()
 {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Rows r < nr of `src` (kPartStride doubles apart, 16-byte aligned), their
+// first nv (<= 32) values, into stage[r * rs + j], rs = nv rounded up to even:
+// one warp's cp.async copies of value pairs (16 bytes, through L2 only), lane
+// (q, p) copying pair p of rows q, q + 32 / W, ... (W the power of two >= the
+// pairs per row).  The caller waits (cp_async_wait + __syncwarp).
+__device__ __forceinline__ int staged_stride(int nv) { return (nv + 1) & ~1; }
+__device__ __forceinline__ void stage_rows(double* stage, const double* __restrict__ src, int nr, int nv, int lane)
+{
+    const int np = (nv + 1) >> 1, rs = 2 * np;
+    const int sh = np <= 4 ? 2 : (np <= 8 ? 3 : 4);
+    const int pr = lane & ((1 << sh) - 1);
+    if (pr >= np) return;
+    for (int r = lane >> sh; r < nr; r += 32 >> sh) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(stage + r * rs + 2 * pr);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d),
+                     "l"(src + (int64_t)r * kPartStride + 2 * pr)
+                     : "memory");
+    }
+}
+
+// weighted_rows over rows staged in shared memory (row r's value j at
+// rows[r * rs + j]): the same products added in the same order.
+__device__ __forceinline__ double weighted_rows_staged(const double* rows, int rs, int nr, double sc, int NV, int lane)
+{
+    const int P = NV <= 8 ? 4 : (NV <= 16 ? 2 : 1);
+    const int W = 32 / P, j = lane & (W - 1), q = lane / W;
+    const bool on = j < NV;
+    double a = 0.0;
+    for (int k = 0; k < W; ++k) {
+        const int r = q + P * k;
+        const double w = __shfl_sync(kFull, sc, r & 31);
+        const double v = (on && r < nr) ? rows[r * rs + j] : 0.0;
+        a += w * v;
+    }
+    for (int o = W; o < 32; o <<= 1) a += __shfl_xor_sync(kFull, a, o);
+    return a;
+}
+
+// A group's row from its nr (<= 32) sub-filters' partial rows, one warp:
+// [0] the group's key maximum, [1 .. NV) the sums scaled to it, [NV] the
+// first-maximum winner's key, [NV + 1] its index (idx0 + the sub-filter).
+// STAGED (`stage`: 32 rows of NV values in shared memory, `part` 16-byte
+// aligned): every row arrives in one round of copies before the maximum and
+// the sums; otherwise the maximum's values load first and the rows after.
+// The same result either way.
+template <int S, bool STAGED = false>
+__device__ __forceinline__ void group_row(const FilterDesc& D, const double* __restrict__ part,
+                                          const float* __restrict__ winner, int nr, int NV, int idx0, int lane,
+                                          double* __restrict__ go, double* stage = nullptr)
+{
+    const bool valid = lane < nr;
+    if constexpr (STAGED) stage_rows(stage, part, nr, NV, lane);
+    const float lw = valid ? __ldcg(winner + lane) : -INFINITY;
+    double l;
+    if constexpr (STAGED) {
+        cp_async_wait();
+        __syncwarp();
+        l = valid ? stage[lane * staged_stride(NV)] : -INFINITY;
+    } else {
+        l = valid ? __ldcg(part + (int64_t)lane * kPartStride) : -INFINITY;
+    }
+    double gl = l;
+    float wk = lw;
+    int wi = valid ? lane : 0x7fffffff;
+    auto reduce = [&] {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            gl = fmax(gl, __shfl_xor_sync(kFull, gl, o));
+            const float ok = __shfl_xor_sync(kFull, wk, o);
+            const int oi = __shfl_xor_sync(kFull, wi, o);
+            if (ok > wk || (ok == wk && oi < wi)) {
+                wk = ok;
+                wi = oi;
+            }
+        }
+        return valid ? (D.log_weights ? exp(l - gl) : 1.0) : 0.0;
+    };
+    double a;
+    if constexpr (STAGED) {
+        a = weighted_rows_staged(stage, staged_stride(NV), nr, reduce(), NV, lane);
+    } else if constexpr (2 + 2 * S <= 8) {
+        a = weighted_rows(part, nr, reduce(), NV, lane);
+    } else {
+        a = weighted_rows_late(part, nr, NV, lane, reduce);
+    }
+    if (lane >= 1 && lane < NV) go[lane] = a;
+    if (lane == 0) {
+        go[0] = D.log_weights ? gl : 0.0;
+        go[NV] = (double)wk;
+        go[NV + 1] = (double)(wi + idx0);
+    }
+}
+
+// Global winner (first maximum, thrust::max_element semantics,
+// pf_generic_soa.cu:1014-1017) + FP64 posterior mean, reduced in two fixed-order
+// levels inside the resampling kernel: warp 0 of the CTA of sub-filter 32g
+// combines sub-filters 32g..32g+31 (all partials are final when that kernel
+// starts); the last group to finish (atomic ticket) combines the groups in
+// index order and writes the estimate.  Deterministic for a given N.
+// ---------------------------------------------------------------------------
+// The estimate's fields from the sums `acc` (lane j < NV holds sum j), one
+// warp at once -- lane v the mean (or circular mean) of variable v, lane 16 +
+// v the winner's variable v (best_v), lane 0 the rest.
+template <int S>
+__device__ __forceinline__ void estimate_store(const FilterDesc& D, int lane, int NV, double gm, float bk, int best,
+                                               float best_v, double acc, pf_estimate& E, int32_t step_no)
+{
+    __shared__ double s_acc[2 + 2 * PF_MAX_STATE];
+    if (lane >= 1 && lane < NV) s_acc[lane] = acc;
+    __syncwarp();
+    const double W = s_acc[1];
+    if (lane < PF_MAX_STATE) {
+        const int v = lane;
+        double m = 0.0;
+        if (v < S) {
+            if ((D.angle_mask >> v) & 1u) {
+                const int a = __popc(D.angle_mask & ((1u << v) - 1u));
+                m = atan2(s_acc[2 + v], s_acc[2 + S + a]);
+            } else {
+                m = s_acc[2 + v] / W;
+            }
+        }
+        E.mean[v] = m;
+    } else {
+        E.best[lane - PF_MAX_STATE] = best_v;
+    }
+    if (lane == 0) {
+        const double lg = D.log_weights ? gm : 0.0;
+        E.log_norm = lg + log(W);
+        E.best_key = bk;
+        E.best_subfilter = best;
+        E.step = step_no;
+        E.flags = (isfinite(lg) && isfinite(W) && W > 0.0) ? 0 : 1;
+    }
+    __syncwarp();
+}
+
+// The global estimate from the group partials gpart[0..ng) (one warp, after
+// the global maximum gm and the winner (bk, bi) are known): the FP64 sums of
+// the NV values, then estimate_store with the winner's state from best_src.
+// Each sum keeps one order: the groups ascending in chunks of 32, the
+// chunks' sums in order.
+template <int S>
+__device__ __forceinline__ void estimate_write(const FilterDesc& D, int lane, int ng, int NV, double gm, float bk,
+                                               int bi, const float* __restrict__ best_src, pf_estimate& E,
+                                               int32_t step_no)
+{
+    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
+    // the winner's state first: its load overlaps the sums
+    const int bv = lane - PF_MAX_STATE;
+    const float best_v = (bv >= 0 && bv < S) ? __ldcg(best_src + bv * D.T + (int64_t)best * D.M) : 0.0f;
+    // lane j sums value j over the groups, 32 rows at a time (weighted_rows)
+    double acc = 0.0;
+    for (int c = 0; c < ng; c += 32) {
+        const int nr = min(32, ng - c);
+        const double* rows = D.gpart + (int64_t)c * kPartStride;
+        const double l = lane < nr ? __ldcg(rows + (int64_t)lane * kPartStride) : 0.0;
+        auto scale = [&] { return lane < nr ? (D.log_weights ? exp(l - gm) : 1.0) : 0.0; };
+        if constexpr (2 + 2 * S <= 8) {
+            acc += weighted_rows(rows, nr, scale(), NV, lane);
+        } else {
+            acc += weighted_rows_late(rows, nr, NV, lane, scale);
+        }
+    }
+    estimate_store<S>(D, lane, NV, gm, bk, best, best_v, acc, E, step_no);
+}
+
+// The winner and the maximum: lane q's own rows in ascending order, then an
+// xor tree (first maximum, lowest index on ties).
+__device__ __forceinline__ void winner_merge(double& gm, float& bk, int& bi, double g0, double gk, double gi)
+{
+    gm = fmax(gm, g0);
+    const float k = (float)gk;
+    const int i = (int)gi;
+    if (k > bk || (k == bk && i < bi)) {
+        bk = k;
+        bi = i;
+    }
+}
+__device__ __forceinline__ void winner_tree(double& gm, float& bk, int& bi)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gm = fmax(gm, __shfl_xor_sync(kFull, gm, o));
+        const float ok = __shfl_xor_sync(kFull, bk, o);
+        const int oi = __shfl_xor_sync(kFull, bi, o);
+        if (ok > bk || (ok == bk && oi < bi)) {
+            bk = ok;
+            bi = oi;
+        }
+    }
+}
+
+// The global estimate from the group partial rows gpart[0..ng) (one warp): the
+// global maximum, the first-maximum winner, then estimate_write (whose winner
+// state is read at best_src + v T + winner M).
+template <int S>
+__device__ __forceinline__ void estimate_final(const FilterDesc& D, int lane, int ng, int NV,
+                                               const float* __restrict__ best_src, pf_estimate& E, int32_t step_no)
+{
+    double gm = -INFINITY;
+    float bk = -INFINITY;
+    int bi = 0x7fffffff;
+#pragma unroll 2
+    for (int q = lane; q < ng; q += 32) {
+        const double* gq = D.gpart + (int64_t)q * kPartStride;
+        winner_merge(gm, bk, bi, __ldcg(gq), __ldcg(gq + NV), __ldcg(gq + NV + 1));
+    }
+    winner_tree(gm, bk, bi);
+    estimate_write<S>(D, lane, ng, NV, gm, bk, bi, best_src, E, step_no);
+}
+
+// estimate_final with the group rows staged in shared memory (`stage`: wr
+// rows of NV + 2 values, wr a multiple of 32; gpart 16-byte aligned): the
+// rows arrive in windows of wr, one round of copies each -- a single window,
+// copied once, for ng <= wr -- and give the same maximum, winner and sums in
+// the same order.
+template <int S>
+__device__ __forceinline__ void estimate_final_staged(const FilterDesc& D, int lane, int ng, int NV,
+                                                      const float* __restrict__ best_src, pf_estimate& E,
+                                                      int32_t step_no, double* stage, int wr)
+{
+    const int rs = staged_stride(NV + 2);
+    auto load_window = [&](int w0) {
+        __syncwarp();  // the previous window's reads are done
+        stage_rows(stage, D.gpart + (int64_t)w0 * kPartStride, min(wr, ng - w0), NV + 2, lane);
+        cp_async_wait();
+        __syncwarp();
+    };
+    double gm = -INFINITY;
+    float bk = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int w0 = 0; w0 < ng; w0 += wr) {
+        load_window(w0);
+        const int nr = min(wr, ng - w0);
+        for (int q = lane; q < nr; q += 32) {
+            const double* sq = stage + q * rs;
+            winner_merge(gm, bk, bi, sq[0], sq[NV], sq[NV + 1]);
+        }
+    }
+    winner_tree(gm, bk, bi);
+    const int best = (bi >= 0 && bi < D.N) ? bi : 0;  // NaN keys everywhere: report sub-filter 0
+    const int bv = lane - PF_MAX_STATE;
+    const float best_v = (bv >= 0 && bv < S) ? __ldcg(best_src + bv * D.T + (int64_t)best * D.M) : 0.0f;
+    double acc = 0.0;
+    for (int w0 = 0; w0 < ng; w0 += wr) {
+        if (ng > wr) load_window(w0);
+        const int nw = min(wr, ng - w0);
+        for (int c = 0; c < nw; c += 32) {
+            const int nr = min(32, nw - c);
+            const double* sr = stage + c * rs;
+            const double l = lane < nr ? sr[lane * rs] : 0.0;
+            acc += weighted_rows_staged(sr, rs, nr, lane < nr ? (D.log_weights ? exp(l - gm) : 1.0) : 0.0, NV, lane);
+        }
+    }
+    estimate_store<S>(D, lane, NV, gm, bk, best, best_v, acc, E, step_no);
+}
+
+// Group g's estimate row from its 32 sub-filters' partial rows (one warp);
+// the last group to finish (ticket) combines every group row into the
+// filter's estimate.  With CAP >= 32 kPartStride doubles of the kernel's
+// shared memory at `smem` (the partial rows are 256-byte aligned in every
+// allocation of this library) both levels read their rows staged there.
+template <int S, int CAP>
+__device__ __forceinline__ void estimate_group(const FilterDesc& D, int g, const InputRef& in, int32_t* step_ctr,
+                                               double* smem)
+{
+    constexpr bool STAGED = CAP >= 32 * kPartStride;
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const int b = g << 5, ng = (D.N + 31) >> 5;
+    const int NV = 2 + S + D.na;
+    // winners as filter-wide indices (a shard's sub-filters start at b0)
+    group_row<S, STAGED>(D, D.part + (int64_t)b * kPartStride, D.winner + b, min(32, D.N - b), NV, b + D.b0, lane,
+                         D.gpart + (int64_t)g * kPartStride, smem);
+    if (D.shard) return;  // the shards' group rows are combined across shards (pf_shard_estimate)
+    __syncwarp();
+    __threadfence();
+    int last = 0;
+    if (lane == 0) last = atomicAdd(D.est_ctr, 1) == ng - 1;
+    last = __shfl_sync(kFull, last, 0);
+    if (!last) return;
+    __threadfence();
+    const int32_t step_no = in.ctr ? *in.ctr + 1 : 0;
+    if constexpr (STAGED) {
+        const int wr = (CAP / staged_stride(NV + 2)) & ~31;
+        estimate_final_staged<S>(D, lane, ng, NV, D.tmp, D.est[step_index(in)], step_no, smem, wr);
+    } else {
+        estimate_final<S>(D, lane, ng, NV, D.tmp, D.est[step_index(in)], step_no);
+    }
+    if (lane == 0) {
+        *D.est_ctr = 0;
+        __threadfence();
+        if (step_ctr) *step_ctr += 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exchange + resample + gather, one CTA per sub-filter.  `virt`: apply the
+// exchange virtually (read the neighbours' slots straight from tmp).
+// Resampling restates resampling (pf_generic_soa.cu:415-453) for
+// PF_RESAMPLE_REFERENCE, resampling_valias (resampling-valias.cl:214-300)
+// for PF_RESAMPLE_VOSE; PF_RESAMPLE_SYSTEMATIC uses the FP64 scan.
+// ---------------------------------------------------------------------------
+template <int S, int M, int E, int RES>
+constexpr size_t k2_smem()
+{
+    size_t s = (size_t)M * 4 + (size_t)S * M * 4;  // keys + state tile
+    if (RES == PF_RESAMPLE_SYSTEMATIC) s += 0;       // the scan stays in registers, the runs reuse the keys
+    else if (RES == PF_RESAMPLE_REFERENCE) s += (size_t)M * 4;
+    else s += (size_t)M * 16;  // prob, alias, work list, scratch
+    return s;
 }
 
 // Bulk copies global -> shared through the TMA engine (cp.async.bulk, no
@@ -1217,7 +1345,8 @@ __global__ void __launch_bounds__(M / E, pf_min_blocks(M / E, pf_k2_warps(S))) k
     const int tid = threadIdx.x;
     wait_prerequisites();
     if (b < 0) {
-        estimate_group<S>(D, -1 - b, in, step_ctr);
+        constexpr int cap = (int)(k2_smem<S, M, E, RES>() / 8);  // doubles of dynamic shared memory
+        estimate_group<S, cap>(D, -1 - b, in, step_ctr, reinterpret_cast<double*>(smem));
         return;
     }
     const int64_t T = D.T;
