@@ -64,6 +64,33 @@ def test_fused_equals_split(gpu, m, ppt, res, exch, t):
         assert abs(x["log_norm"] - y["log_norm"]) <= 1e-12 * abs(x["log_norm"])
 
 
+@pytest.mark.parametrize("model,m,N,ppt", [(ARM, 256, 4096, 2), (UNI, 512, 16384, 4)])
+def test_fused_equals_split_many_groups(gpu, model, m, N, ppt):
+    """More groups of 32 sub-filters than the resampling kernel stages in one
+    round (the DH arm's 128 group rows against 64 per round at m = 256, the
+    unicycle's 512 against 256 at m = 512): the split pipeline's final combine
+    reads them in several windows, the single-kernel step's in chunks from
+    global memory; the estimates agree to the last bit of the FP64 sums."""
+    E = gpu
+    if model == UNI:
+        p, inputs, _ = uni_setup(steps=3)
+    else:
+        p = E.dharm_params(3)
+        inputs, _ = E.make_trace(ARM, p, 3, 3)
+    common = dict(particles_per_subfilter=m, num_subfilters=N, num_transfer=1, exchange=E.EXCHANGE_TORUS,
+                  resampler=E.RESAMPLE_SYSTEMATIC, particles_per_thread=ppt)
+    fa, ea = run(E, model, p, inputs, 3, pipeline=E.PIPELINE_SPLIT, **common)
+    fb, eb = run(E, model, p, inputs, 3, pipeline=E.PIPELINE_FUSED, **common)
+    assert fb.info()["pipeline"] == E.PIPELINE_FUSED and fa.info()["pipeline"] == E.PIPELINE_SPLIT
+    assert np.array_equal(fa.particles(), fb.particles())
+    for x, y in zip(ea, eb):
+        assert x["best_subfilter"] == y["best_subfilter"] and x["best_key"] == y["best_key"]
+        assert np.array_equal(x["best"], y["best"])
+        assert np.array_equal(x["mean"], y["mean"]) and x["log_norm"] == y["log_norm"]
+    fa.close()
+    fb.close()
+
+
 @pytest.mark.parametrize("rng_mode", [0, 1])
 @pytest.mark.parametrize("res", [0, 1, 2])
 def test_first_step_vs_oracle(gpu, O, rng_mode, res):
